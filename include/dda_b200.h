@@ -1,0 +1,148 @@
+/*
+ * dda_b200.h -- C ABI of the B200 discrete-dipole-approximation engine.
+ *
+ * Plain C: device pointers are `void*` / `const void*` to contiguous arrays,
+ * sizes are ints, streams are `cudaStream_t` passed as `void*` (NULL = the
+ * legacy default stream).  No call synchronises the device; calls that must
+ * observe device state (solver termination, cross sections) synchronise only
+ * on events of their own internal stream.  Every entry point returns an int
+ * status (DDA_OK on success); `dda_last_error()` gives the message of the
+ * last failure on the calling thread.
+ *
+ * Array conventions follow the reference engine (Toastlovesjam/preconDDA):
+ *   vectors (polarisation P, incident field E_inc, matvec in/out):
+ *       C-order (nx, ny, nz, 3) complex, component index fastest
+ *       (Gpbicgstab.py:937, :1172);
+ *   inverse polarisability inv_alpha: (nx, ny, nz) complex, 0 outside the
+ *       scatterer; the mask is inv_alpha != 0 (ddaforgit.py:1105-1108);
+ *   FFT'd interaction tensor ghat: reduced octant (Lx/2+1, Ly/2+1, Lz/2+1, 6)
+ *       of FFT(-G), components (xx, xy, xz, yy, yz, zz) fastest
+ *       (ddaforgit.py:1069-1077).  With Ln = 2 nn this is exactly the
+ *       reference's (nx+1, ny+1, nz+1, 6) array.
+ * dtype: DDA_C64 = complex64 (float2), DDA_C128 = complex128 (double2).
+ */
+#ifndef DDA_B200_H
+#define DDA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DDA_C64 0
+#define DDA_C128 1
+
+/* status codes */
+#define DDA_OK 0
+#define DDA_ERR_BAD_SHAPE 1
+#define DDA_ERR_OOM 2
+#define DDA_NOT_CONVERGED 3
+#define DDA_ERR_NAN 4
+#define DDA_ERR_TIMEOUT 5
+#define DDA_ERR_CUDA 6
+#define DDA_ERR_ARG 7
+
+/* matvec modes of dda_matvec */
+#define DDA_MV_AX 0            /* y = inv_alpha*x - mask*conv(x)          */
+#define DDA_MV_RESIDUAL 1      /* y = b - A.x  (b already masked)          */
+#define DDA_MV_CONV 2          /* y = conv(x), no mask (near field)        */
+#define DDA_MV_CONV_MASKED 3   /* y = mask*conv(x)                         */
+
+typedef struct dda_ctx dda_ctx;
+typedef struct dda_op dda_op;
+
+/* One right-hand side of a batched solve.  Instances of one batch share the
+ * box (nx,ny,nz), the FFT lengths and the dtype; ghat / inv_alpha may be
+ * shared between instances (many incidences of one geometry) or not (many
+ * geometries padded into one size bucket). */
+typedef struct dda_instance {
+  const void* ghat;        /* octant, dtype of the solve                  */
+  const void* inv_alpha;   /* (nx,ny,nz) complex, dtype of the solve      */
+  const void* e_inc;       /* (nx,ny,nz,3) complex, dtype of the solve    */
+  void* p_out;             /* (nx,ny,nz,3) complex, dtype of the solve    */
+} dda_instance;
+
+/* Per-instance result of a solve (reference return tuple, Gpbicgstab.py:1162-1201). */
+typedef struct dda_result {
+  int iters;               /* i+1 converged, max_iter not converged, -(i+1) NaN / stagnation */
+  int status;              /* DDA_OK, DDA_NOT_CONVERGED or DDA_ERR_NAN                       */
+  double lowest_rel;       /* lowest recursive residual norm / initial norm                  */
+  double first_rel;        /* residual norm after the first iteration / initial norm         */
+  double true_relres;      /* ||b - A.P|| / ||b|| where computed (mixed solve), else -1      */
+  int outer;               /* refinement sweeps (mixed solve), else 0                        */
+  int resets;              /* Krylov restarts taken                                          */
+} dda_result;
+
+int dda_version(void);
+const char* dda_last_error(void);
+/* Number of kernels this library has enqueued in the process so far
+ * (instrumentation for benchmarks; no reference counterpart). */
+long long dda_kernel_launches(void);
+
+/* Context: device binding, twiddle tables and solver workspaces. */
+int dda_ctx_create(int device, dda_ctx** out);
+void dda_ctx_destroy(dda_ctx* ctx);
+/* Frees cached solver workspaces (they are kept between solves). */
+int dda_ctx_trim(dda_ctx* ctx);
+
+/* 1 if L is a usable FFT length for the dtype (even, 2^a 3^b 5^c 7^d,
+ * small enough for one shared-memory tile), else 0. */
+int dda_fft_length_ok(int L, int dtype);
+
+/* Replaces generate_interaction_row (ddaforgit.py:1046-1080): builds
+ * scale * FFT(-G) on the (Lx,Ly,Lz) embedding of the (nx,ny,nz) box, cropped
+ * to the octant.  scale = 1 gives the reference's array.  Writes complex128 to
+ * out_c128 and/or complex64 to out_c64 (either may be NULL). */
+int dda_green_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d,
+                    double scale, void* out_c128, void* out_c64, void* stream);
+
+/* Operator A for one geometry: references caller-owned ghat (octant with the
+ * given scale, i.e. the kernel multiplies by gscale) and inv_alpha; owns the
+ * transform scratch.  Replaces the state prepared by prepare_interaction_matrices
+ * (ddaforgit.py:1085-1159) and setup_chunked_values (Gpbicgstab.py:832-876). */
+int dda_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* ghat,
+                  double gscale, const void* inv_alpha, dda_op** out);
+void dda_op_destroy(dda_op* op);
+
+/* Replaces interaction_mult (Gpbicgstab.py:828-830, mode DDA_MV_AX),
+ * fft_matvec (Gpbicgstab.py:742-772, DDA_MV_CONV_MASKED) and the product of
+ * E_field_solver (ExcitedField.py:129-195, DDA_MV_CONV).  b is read only by
+ * DDA_MV_RESIDUAL.  x and y must not alias. */
+int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void* stream);
+
+/* Replaces solve_gpbicgstab (Gpbicgstab.py:879-1201) with precon=False:
+ * solves A.P = E_inc*mask from P0 = 0 with the reference's GPBiCGSTAB
+ * recurrence, restarts (ratio), true-residual replacement and return codes.
+ * Blocks until the solve ends. */
+int dda_gpbicgstab(dda_op* op, const void* e_inc, double target, int max_iter, double ratio, void* p_out,
+                   dda_result* res, void* stream);
+
+/* Many right-hand sides / geometries in one batched solve (same box, L and
+ * dtype).  Converged instances retire while the others continue. */
+int dda_solve_batch(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                    const dda_instance* inst, int nb, double target, int max_iter, double ratio, dda_result* res,
+                    void* stream);
+
+/* Mixed precision: complex64 GPBiCGSTAB sweeps (relative target inner_tol)
+ * inside an FP64 iterative-refinement loop whose true residual
+ * E_inc*mask - A.P is an FP64 matvec; stops when it is <= tol * ||E_inc*mask||.
+ * inst64 / inst128 describe the same instances in both precisions
+ * (inst64[j].p_out and inst64[j].e_inc are scratch the engine may overwrite;
+ * inst128[j].p_out receives the FP64 solution). */
+int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                          const dda_instance* inst64, const dda_instance* inst128, int nb, double tol,
+                          double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
+                          void* stream);
+
+/* Extinction, absorption and scattering cross sections (Draine & Flatau
+ * 1994, not present in the reference) reduced in FP64:
+ *   out[0] = C_ext = 4 pi k/|E0|^2 sum Im(E_inc* . P)
+ *   out[1] = C_abs = 4 pi k/|E0|^2 sum [Im(P . conj(inv_alpha) P*) - 2/3 k^3 |P|^2]
+ *   out[2] = C_sca = C_ext - C_abs
+ * All three arrays have the given dtype; sites with inv_alpha == 0 are skipped. */
+int dda_cross_sections(dda_ctx* ctx, int dtype, long long nsite, const void* p, const void* e_inc,
+                       const void* inv_alpha, double k, double e0, double* out3, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DDA_B200_H */

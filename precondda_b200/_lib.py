@@ -1,0 +1,143 @@
+"""ctypes binding of libdda_b200.so (declared in include/dda_b200.h).
+
+The shared library is the engine; this module only loads it, declares the
+prototypes and turns status codes into Python exceptions.  There is no
+fallback: if the library is missing or the device cannot be used, every entry
+point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdda_b200.so")
+
+DDA_C64 = 0
+DDA_C128 = 1
+
+DDA_OK = 0
+DDA_ERR_BAD_SHAPE = 1
+DDA_ERR_OOM = 2
+DDA_NOT_CONVERGED = 3
+DDA_ERR_NAN = 4
+DDA_ERR_TIMEOUT = 5
+DDA_ERR_CUDA = 6
+DDA_ERR_ARG = 7
+
+MV_AX = 0
+MV_RESIDUAL = 1
+MV_CONV = 2
+MV_CONV_MASKED = 3
+
+# every symbol include/dda_b200.h declares
+EXPORTS = (
+    "dda_version", "dda_last_error", "dda_kernel_launches", "dda_ctx_create", "dda_ctx_destroy", "dda_ctx_trim",
+    "dda_fft_length_ok", "dda_green_build", "dda_op_create", "dda_op_destroy", "dda_matvec",
+    "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
+)
+
+
+class DDAError(RuntimeError):
+    """Failure reported by the engine's C ABI."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[dda status {code}] {msg}")
+        self.code = code
+
+
+class dda_instance(C.Structure):
+    _fields_ = [("ghat", C.c_void_p), ("inv_alpha", C.c_void_p), ("e_inc", C.c_void_p), ("p_out", C.c_void_p)]
+
+
+class dda_result(C.Structure):
+    _fields_ = [("iters", C.c_int), ("status", C.c_int), ("lowest_rel", C.c_double), ("first_rel", C.c_double),
+                ("true_relres", C.c_double), ("outer", C.c_int), ("resets", C.c_int)]
+
+
+_lib = None
+_lock = threading.Lock()
+
+
+def _declare(lib):
+    vp, i, d, ll = C.c_void_p, C.c_int, C.c_double, C.c_longlong
+    lib.dda_version.restype = i
+    lib.dda_last_error.restype = C.c_char_p
+    lib.dda_kernel_launches.restype = ll
+    lib.dda_ctx_create.argtypes = [i, C.POINTER(vp)]
+    lib.dda_ctx_destroy.argtypes = [vp]
+    lib.dda_ctx_destroy.restype = None
+    lib.dda_ctx_trim.argtypes = [vp]
+    lib.dda_fft_length_ok.argtypes = [i, i]
+    lib.dda_green_build.argtypes = [vp, i, i, i, i, i, i, d, d, d, vp, vp, vp]
+    lib.dda_op_create.argtypes = [vp, i, i, i, i, i, i, i, vp, d, vp, C.POINTER(vp)]
+    lib.dda_op_destroy.argtypes = [vp]
+    lib.dda_op_destroy.restype = None
+    lib.dda_matvec.argtypes = [vp, i, vp, vp, vp, vp]
+    lib.dda_gpbicgstab.argtypes = [vp, vp, d, i, d, vp, C.POINTER(dda_result), vp]
+    lib.dda_solve_batch.argtypes = [vp, i, i, i, i, i, i, i, d, C.POINTER(dda_instance), i, d, i, d,
+                                    C.POINTER(dda_result), vp]
+    lib.dda_solve_mixed_batch.argtypes = [vp, i, i, i, i, i, i, d, C.POINTER(dda_instance),
+                                          C.POINTER(dda_instance), i, d, d, i, i, d, C.POINTER(dda_result), vp]
+    lib.dda_cross_sections.argtypes = [vp, i, ll, vp, vp, vp, d, d, C.POINTER(d), vp]
+    return lib
+
+
+def lib():
+    """The loaded engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise ImportError(f"libdda_b200.so not found at {LIB_PATH}; build it with "
+                                      f"`python -m precondda_b200.build_lib` (or __graft_entry__.build())")
+                _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(rc: int) -> int:
+    """Raise DDAError for any status other than OK / NOT_CONVERGED / NAN."""
+    if rc in (DDA_OK, DDA_NOT_CONVERGED, DDA_ERR_NAN):
+        return rc
+    msg = lib().dda_last_error()
+    msg = msg.decode() if msg else ""
+    if rc == DDA_ERR_BAD_SHAPE:
+        raise ValueError(msg)
+    if rc == DDA_ERR_OOM:
+        raise MemoryError(msg)
+    raise DDAError(rc, msg)
+
+
+class Context:
+    """Engine context bound to one CUDA device (twiddles, workspaces)."""
+
+    def __init__(self, device: int):
+        self.device = device
+        h = C.c_void_p()
+        check(lib().dda_ctx_create(device, C.byref(h)))
+        self.handle = h
+
+    def trim(self):
+        check(lib().dda_ctx_trim(self.handle))
+
+    def __del__(self):
+        try:
+            if self.handle:
+                lib().dda_ctx_destroy(self.handle)
+        except Exception:
+            pass
+
+
+_ctxs: dict[int, Context] = {}
+
+
+def context(device: int) -> Context:
+    with _lock:
+        c = _ctxs.get(device)
+    if c is None:
+        c = Context(device)
+        with _lock:
+            _ctxs[device] = c
+    return c

@@ -1,0 +1,276 @@
+// extern "C" entry points of include/dda_b200.h.
+#include <cmath>
+#include <cstring>
+#include <new>
+
+#include "../../include/dda_b200.h"
+#include "dda_host.h"
+#include "reduce.cuh"
+#include "fft_sizes.h"
+
+using namespace dda;
+
+struct dda_ctx {
+  Ctx c;
+};
+
+struct dda_op {
+  dda_ctx* ctx = nullptr;
+  int dtype = 0;
+  Geo g{};
+  PassCfg pc{};
+  double gscale = 1.0;
+  const void* ghat = nullptr;
+  const void* inva = nullptr;
+  void* scratch = nullptr;
+  InstState* d_st = nullptr;
+};
+
+static int check_ctx(dda_ctx* ctx) {
+  if (!ctx) { set_error("null context"); return DDA_ERR_ARG; }
+  cudaError_t e = cudaSetDevice(ctx->c.device);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  return DDA_OK;
+}
+
+static int fft_cap(int dtype) { return dtype == DDA_C128 ? 12 * 256 : 24 * 256; }
+
+static bool length_ok(int L, int dtype) {
+  if (L < 2 || (L & 1)) return false;
+  if (3 * L > fft_cap(dtype)) return false;
+  return fft_size_compiled(L);
+}
+
+static int make_geo(int nx, int ny, int nz, int Lx, int Ly, int Lz, int dtype, Geo* g) {
+  if (nx < 1 || ny < 1 || nz < 1) { set_error("box dimensions must be >= 1"); return DDA_ERR_BAD_SHAPE; }
+  if (Lx < 2 * nx || Ly < 2 * ny || Lz < 2 * nz) {
+    set_error("FFT lengths must be >= twice the box dimensions");
+    return DDA_ERR_BAD_SHAPE;
+  }
+  if (!length_ok(Lx, dtype) || !length_ok(Ly, dtype) || !length_ok(Lz, dtype)) {
+    set_error("FFT lengths must be one of the compiled sizes (even, 2^a 3^b 5^c 7^d, <= 512)");
+    return DDA_ERR_BAD_SHAPE;
+  }
+  g->nx = nx; g->ny = ny; g->nz = nz;
+  g->Lx = Lx; g->Ly = Ly; g->Lz = Lz;
+  g->hx = Lx / 2 + 1; g->hy = Ly / 2 + 1; g->hz = Lz / 2 + 1;
+  g->nsite = (long long)nx * ny * nz;
+  return DDA_OK;
+}
+
+extern "C" {
+
+int dda_version(void) { return 100; }
+
+long long dda_kernel_launches(void) { return launch_count(); }
+
+const char* dda_last_error(void) { return get_error().c_str(); }
+
+int dda_ctx_create(int device, dda_ctx** out) {
+  if (!out) { set_error("null output pointer"); return DDA_ERR_ARG; }
+  *out = nullptr;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  dda_ctx* c = new (std::nothrow) dda_ctx();
+  if (!c) { set_error("host allocation failed"); return DDA_ERR_OOM; }
+  c->c.device = device;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+    c->c.num_sms = sms;
+  if ((e = cudaStreamCreateWithFlags(&c->c.stream, cudaStreamNonBlocking)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->c.ev[0], cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->c.ev[1], cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->c.ev_user, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->c.ev_done, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&c->c.xred, (size_t)4 * c->c.num_sms * 12 * sizeof(double))) != cudaSuccess ||
+      (e = cudaMalloc((void**)&c->c.xcnt, sizeof(unsigned))) != cudaSuccess ||
+      (e = cudaMalloc((void**)&c->c.xout, 4 * sizeof(double))) != cudaSuccess ||
+      (e = cudaMallocHost((void**)&c->c.xout_h, 4 * sizeof(double))) != cudaSuccess ||
+      (e = cudaMemset(c->c.xcnt, 0, sizeof(unsigned))) != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    delete c;
+    return DDA_ERR_CUDA;
+  }
+  *out = c;
+  return DDA_OK;
+}
+
+void dda_ctx_destroy(dda_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->c.device);
+  cudaStreamSynchronize(ctx->c.stream);
+  ctx->c.trim();
+  cudaEventDestroy(ctx->c.ev[0]); cudaEventDestroy(ctx->c.ev[1]);
+  cudaEventDestroy(ctx->c.ev_user); cudaEventDestroy(ctx->c.ev_done);
+  cudaStreamDestroy(ctx->c.stream);
+  cudaFree(ctx->c.xred); cudaFree(ctx->c.xcnt); cudaFree(ctx->c.xout); cudaFreeHost(ctx->c.xout_h);
+  delete ctx;
+}
+
+int dda_ctx_trim(dda_ctx* ctx) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  cudaStreamSynchronize(ctx->c.stream);
+  ctx->c.trim();
+  return DDA_OK;
+}
+
+int dda_fft_length_ok(int L, int dtype) { return length_ok(L, dtype) ? 1 : 0; }
+
+int dda_green_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d, double scale,
+                    void* out_c128, void* out_c64, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, DDA_C128, &g))) return rc;
+  if (!(k > 0) || !(d > 0)) { set_error("k and d must be positive"); return DDA_ERR_ARG; }
+  if (!out_c128 && !out_c64) { set_error("no output"); return DDA_ERR_ARG; }
+  return green_build(ctx->c, g, k, d, scale, out_c128, out_c64, (cudaStream_t)stream);
+}
+
+int dda_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* ghat,
+                  double gscale, const void* inv_alpha, dda_op** out) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!out || !ghat || !inv_alpha) { set_error("null argument"); return DDA_ERR_ARG; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  *out = nullptr;
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g))) return rc;
+  dda_op* op = new (std::nothrow) dda_op();
+  if (!op) { set_error("host allocation failed"); return DDA_ERR_OOM; }
+  op->ctx = ctx; op->dtype = dtype; op->g = g; op->gscale = gscale; op->ghat = ghat; op->inva = inv_alpha;
+  op->pc = make_pass_cfg(g, dtype == DDA_C128);
+  const size_t esz = dtype == DDA_C128 ? 16 : 8;
+  const size_t t1n = (size_t)g.nx * g.ny * g.Lz * 3, t2n = (size_t)g.nx * g.Ly * g.Lz * 3;
+  if (cudaMalloc(&op->scratch, (t1n + t2n) * esz) != cudaSuccess ||
+      cudaMalloc((void**)&op->d_st, sizeof(InstState)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(op->scratch);
+    delete op;
+    set_error("operator scratch: out of device memory");
+    return DDA_ERR_OOM;
+  }
+  *out = op;
+  return DDA_OK;
+}
+
+void dda_op_destroy(dda_op* op) {
+  if (!op) return;
+  cudaSetDevice(op->ctx->c.device);
+  cudaStreamSynchronize(op->ctx->c.stream);
+  cudaDeviceSynchronize();
+  cudaFree(op->scratch);
+  cudaFree(op->d_st);
+  delete op;
+}
+
+int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void* stream) {
+  if (!op) { set_error("null operator"); return DDA_ERR_ARG; }
+  int rc = check_ctx(op->ctx);
+  if (rc) return rc;
+  if (!x || !y || (mode == DDA_MV_RESIDUAL && !b)) { set_error("null vector"); return DDA_ERR_ARG; }
+  if (mode < 0 || mode > 3) { set_error("bad matvec mode"); return DDA_ERR_ARG; }
+  if (x == y) { set_error("x and y must not alias"); return DDA_ERR_ARG; }
+  InstState S;
+  std::memset(&S, 0, sizeof(S));
+  S.vec[V_R] = (void*)x;
+  S.vec[V_RHAT] = y;
+  S.vec[V_B] = (void*)b;
+  S.ghat = op->ghat;
+  S.inva = op->inva;
+  const size_t esz = op->dtype == DDA_C128 ? 16 : 8;
+  S.t1 = op->scratch;
+  S.t2 = (char*)op->scratch + (size_t)op->g.nx * op->g.ny * op->g.Lz * 3 * esz;
+  S.active = 1;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(op->d_st, &S, sizeof(S), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  if (op->dtype == DDA_C128)
+    e = launch_matvec<double>(op->ctx->c, op->g, op->pc, op->d_st, nullptr, 1, V_R, V_RHAT, mode, C_ALWAYS,
+                              op->gscale, s);
+  else
+    e = launch_matvec<float>(op->ctx->c, op->g, op->pc, op->d_st, nullptr, 1, V_R, V_RHAT, mode, C_ALWAYS,
+                             op->gscale, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  return DDA_OK;
+}
+
+int dda_gpbicgstab(dda_op* op, const void* e_inc, double target, int max_iter, double ratio, void* p_out,
+                   dda_result* res, void* stream) {
+  if (!op) { set_error("null operator"); return DDA_ERR_ARG; }
+  dda_instance in{op->ghat, op->inva, e_inc, p_out};
+  return dda_solve_batch(op->ctx, op->dtype, op->g.nx, op->g.ny, op->g.nz, op->g.Lx, op->g.Ly, op->g.Lz, op->gscale,
+                         &in, 1, target, max_iter, ratio, res, stream);
+}
+
+int dda_solve_batch(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                    const dda_instance* inst, int nb, double target, int max_iter, double ratio, dda_result* res,
+                    void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!inst || nb < 1) { set_error("no instances"); return DDA_ERR_ARG; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g))) return rc;
+  for (int j = 0; j < nb; ++j)
+    if (!inst[j].ghat || !inst[j].inv_alpha || !inst[j].e_inc || !inst[j].p_out) {
+      set_error("null instance pointer");
+      return DDA_ERR_ARG;
+    }
+  if (dtype == DDA_C128)
+    return solve_batch<double>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream);
+  return solve_batch<float>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream);
+}
+
+int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                          const dda_instance* inst64, const dda_instance* inst128, int nb, double tol,
+                          double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
+                          void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!inst64 || !inst128 || nb < 1) { set_error("no instances"); return DDA_ERR_ARG; }
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, DDA_C128, &g))) return rc;
+  for (int j = 0; j < nb; ++j)
+    if (!inst64[j].ghat || !inst64[j].inv_alpha || !inst128[j].ghat || !inst128[j].inv_alpha || !inst128[j].e_inc ||
+        !inst128[j].p_out) {
+      set_error("null instance pointer");
+      return DDA_ERR_ARG;
+    }
+  return solve_mixed(ctx->c, g, gscale, inst64, inst128, nb, tol, inner_tol, max_iter, max_outer, ratio, res,
+                     (cudaStream_t)stream);
+}
+
+int dda_cross_sections(dda_ctx* ctx, int dtype, long long nsite, const void* p, const void* e_inc,
+                       const void* inv_alpha, double k, double e0, double* out3, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!p || !e_inc || !inv_alpha || !out3 || nsite < 0) { set_error("null argument"); return DDA_ERR_ARG; }
+  if (!(e0 != 0.0)) { set_error("E0 must be non-zero"); return DDA_ERR_ARG; }
+  Ctx& c = ctx->c;
+  cudaStream_t s = c.stream;
+  cudaError_t e;
+  if ((e = cudaEventRecord(c.ev_user, (cudaStream_t)stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(s, c.ev_user, 0)) != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return DDA_ERR_CUDA;
+  }
+  long long want = (nsite + 255) / 256;
+  int RB = (int)std::max<long long>(1, std::min<long long>(want, 4LL * c.num_sms));
+  if (dtype == DDA_C128) launch_xsec<double>(p, e_inc, inv_alpha, nsite, k, c.xred, c.xcnt, RB, c.xout, s);
+  else launch_xsec<float>(p, e_inc, inv_alpha, nsite, k, c.xred, c.xcnt, RB, c.xout, s);
+  if ((e = cudaMemcpyAsync(c.xout_h, c.xout, 2 * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(s)) != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return DDA_ERR_CUDA;
+  }
+  const double* h = c.xout_h;
+  const double pref = 4.0 * M_PI * k / (std::fabs(e0) * std::fabs(e0));
+  out3[0] = pref * h[0];
+  out3[1] = pref * h[1];
+  out3[2] = out3[0] - out3[1];
+  return DDA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+// Common device helpers for the B200 DDA engine: complex arithmetic on
+// float2 / double2, the per-instance solver state, and launch constants.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dda {
+
+// ---------------------------------------------------------------------------
+// complex type traits: R = float -> float2 (complex64), double -> double2
+// ---------------------------------------------------------------------------
+template <typename R> struct CT;
+template <> struct CT<float> { typedef float2 T; };
+template <> struct CT<double> { typedef double2 T; };
+
+template <class C> __host__ __device__ __forceinline__ C mk(double re, double im) {
+  C c; c.x = (decltype(c.x))re; c.y = (decltype(c.y))im; return c;
+}
+template <class C> __device__ __forceinline__ C cadd(C a, C b) { C c; c.x = a.x + b.x; c.y = a.y + b.y; return c; }
+template <class C> __device__ __forceinline__ C csub(C a, C b) { C c; c.x = a.x - b.x; c.y = a.y - b.y; return c; }
+template <class C> __device__ __forceinline__ C cmul(C a, C b) {
+  C c; c.x = a.x * b.x - a.y * b.y; c.y = a.x * b.y + a.y * b.x; return c;
+}
+// conj(a) * b
+template <class C> __device__ __forceinline__ C cmulc(C a, C b) {
+  C c; c.x = a.x * b.x + a.y * b.y; c.y = a.x * b.y - a.y * b.x; return c;
+}
+template <class C, typename S> __device__ __forceinline__ C cscale(C a, S s) { C c; c.x = a.x * s; c.y = a.y * s; return c; }
+template <class C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+// multiply by -i
+template <class C> __device__ __forceinline__ C cmul_mi(C a) { C c; c.x = a.y; c.y = -a.x; return c; }
+template <class C> __device__ __forceinline__ C czero() { C c; c.x = 0; c.y = 0; return c; }
+
+// complex double helpers used by the scalar control logic
+__device__ __forceinline__ double2 zmul(double2 a, double2 b) { return cmul(a, b); }
+__device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
+  // plain complex division; scalars here are O(1) so no scaling is needed
+  double den = b.x * b.x + b.y * b.y;
+  double2 c; c.x = (a.x * b.x + a.y * b.y) / den; c.y = (a.y * b.x - a.x * b.y) / den; return c;
+}
+__device__ __forceinline__ double2 zsub(double2 a, double2 b) { return csub(a, b); }
+
+// convert complex between precisions
+template <class D, class S> __device__ __forceinline__ D ccvt(S s) {
+  D d; d.x = (decltype(d.x))s.x; d.y = (decltype(d.y))s.y; return d;
+}
+
+// ---------------------------------------------------------------------------
+// geometry of one batch bucket: box (nx,ny,nz) and FFT lengths (Lx,Ly,Lz)
+// ---------------------------------------------------------------------------
+struct Geo {
+  int nx, ny, nz;
+  int Lx, Ly, Lz;
+  int hx, hy, hz;     // octant extents L/2+1
+  long long nsite;    // nx*ny*nz
+};
+
+// Largest number of Stockham stages a length may need (L <= 4096).
+constexpr int kMaxStages = 12;
+
+
+// ---------------------------------------------------------------------------
+// Logical vectors of one GPBiCGSTAB instance.  Kernels address vectors by
+// these ids through InstState::vec, so the control logic can rotate buffers
+// (s <-> s_prev, current / best iterate) on the device without copies.
+// ---------------------------------------------------------------------------
+enum VecId {
+  V_R = 0, V_RHAT, V_P, V_V, V_T, V_S, V_SPREV, V_U, V_Z, V_W, V_Y,
+  V_X, V_B, V_TMP, V_XA, V_XB, V_XC, kNumVec
+};
+
+// control condition under which a (matvec / update) kernel does work
+enum Cond { C_ALWAYS = 0, C_ACTIVE = 1, C_TRUE_RES = 2, C_RESET_RES = 3, C_RESET = 4 };
+
+// solver status codes (mirrors the sign convention of the reference's
+// iteration return value)
+enum SolveStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NAN = 3, ST_STAGNATED = 4 };
+
+struct InstState {
+  // vector table (device pointers, element type given by the batch dtype)
+  void* vec[kNumVec];
+  const void* ghat;    // octant of FFT(-G)/(LxLyLz), (hx,hy,hz,6)
+  const void* inva;    // inverse polarizability per site (N complex)
+  void* t1;            // scratch (nx,ny,Lz,3)
+  void* t2;            // scratch (nx,Ly,Lz,3)
+  // scalars (complex double)
+  double2 rho1, rho0, alpha, beta, zeta, eta;
+  double initial_norm, lowest, current, prev_lowest, first, target, ratio;
+  double bnorm;        // ||b|| for reporting
+  int iter;            // current iteration index i
+  int max_iter;
+  int last_change;
+  int was_reset;
+  int reset_count;
+  int done;            // 1 once the reference's loop would have exited
+  int status;          // SolveStatus
+  int ret_iters;       // reference-style return code (iterations / -(i+1))
+  int flag_true_res;   // r := b - A x needed this iteration (i == 1)
+  int flag_reset;      // reset branch taken this iteration
+  int flag_reset_res;  // reset branch recomputes the true residual
+  int cur_x;           // which of XA/XB/XC holds the current iterate (0..2)
+  int best_x;          // which holds the best iterate (0..2), -1 = none yet
+  int active;          // 1 while the instance takes part in the batch
+  int pad_[3];
+};
+
+__device__ __forceinline__ bool cond_ok(const InstState& s, int cond) {
+  switch (cond) {
+    case C_ALWAYS: return true;
+    case C_ACTIVE: return s.active && !s.done;
+    case C_TRUE_RES: return s.active && !s.done && s.flag_true_res;
+    case C_RESET_RES: return s.active && !s.done && s.flag_reset && s.flag_reset_res;
+    case C_RESET: return s.active && !s.done;
+  }
+  return false;
+}
+
+}  // namespace dda

@@ -1,0 +1,137 @@
+// Host-side internal declarations of the B200 DDA engine (not part of the
+// public C ABI, which lives in include/dda_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dda_common.cuh"
+#include "../../include/dda_b200.h"
+
+namespace dda {
+
+void set_error(const std::string& msg);
+// Counts kernels this library enqueues (launches made while a stream is being
+// captured into a graph are counted when the graph is launched instead).
+void note_launch(cudaStream_t s, long long n);
+long long launch_count();
+const std::string& get_error();
+
+#define DDA_CUDA_OK(expr)                                                        \
+  do {                                                                           \
+    cudaError_t e_ = (expr);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      ::dda::set_error(std::string(#expr) + ": " + cudaGetErrorString(e_));      \
+      return DDA_ERR_CUDA;                                                       \
+    }                                                                            \
+  } while (0)
+
+// status codes shared with include/dda_b200.h
+enum {
+  DDA_OK_ = 0
+};
+
+// Twiddle tables per FFT length, in both precisions, resident on one device.
+struct TwTable {
+  void* d64 = nullptr;    // float2[L]
+  void* d128 = nullptr;   // double2[L]
+};
+
+struct BatchWs;
+
+struct Ctx {
+  int device = 0;
+  int num_sms = 148;
+  std::mutex mu;
+  std::map<int, TwTable> tw;
+  std::map<std::string, BatchWs*> ws;
+  cudaStream_t stream = nullptr;     // internal non-blocking stream
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  cudaEvent_t ev_user = nullptr, ev_done = nullptr;
+  // small reduction scratch for one-off reductions (cross sections)
+  double* xred = nullptr;      // [xrb * 12]
+  unsigned* xcnt = nullptr;
+  double* xout = nullptr;      // [4] device
+  double* xout_h = nullptr;    // [4] pinned
+  int xrb = 1;
+  // returns device twiddles for length L (builds on first use)
+  const void* twiddles(int L, bool dbl);
+  // cached solver workspace for (dtype, geometry, batch size)
+  BatchWs* workspace(int dtype, const Geo& g, int nb, bool full, int* err);
+  void trim();
+  ~Ctx();
+};
+
+// Launch geometry of the five matvec passes for one (Geo, dtype).
+struct PassCfg {
+  int NL, WS1;      // z passes: lines per tile, smem row stride
+  int Tz2, WS2;     // y passes: kz per tile
+  int Tz3, WS3;     // x pass
+  size_t smem1, smem2, smem3;
+  int ntz2, ntz3;
+  long long grid1, grid2, grid3;
+};
+
+PassCfg make_pass_cfg(const Geo& g, bool dbl);
+
+// Device memory of a batch of solver instances sharing one geometry.
+struct BatchWs {
+  int dtype = 0, nb = 0, nslot = 0, RB = 1;
+  bool full = true;
+  Geo g{};
+  PassCfg pc{};
+  size_t esz = 8, n3 = 0, t1n = 0, t2n = 0;
+  void* vecs = nullptr;          // nb * nslot * n3 complex
+  void* scratch = nullptr;       // nb * (t1n + t2n) complex
+  InstState* d_st = nullptr;
+  InstState* h_st[2] = {nullptr, nullptr};   // pinned status buffers
+  double* red = nullptr;
+  unsigned* cnt = nullptr;
+  double* d_out = nullptr;
+  double* h_out = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  double graph_gscale = 0.0;
+  long long graph_kernels = 0;
+  int alloc(Ctx& c, int dtype, const Geo& g, int nb, bool full);
+  void base_state(int j, InstState& S) const;
+  ~BatchWs();
+};
+
+enum MvMode { MV_AX = 0, MV_RESIDUAL = 1, MV_CONV = 2, MV_CONV_MASKED = 3 };
+
+// Enqueue the 5-pass matvec for a batch of instances that share Geo.
+// Instance slots: st[act ? act[j] : j], j < nb.
+template <typename R>
+cudaError_t launch_matvec(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
+                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s);
+
+// Batched GPBiCGSTAB kernels (krylov.cu); RB CTAs per instance.
+struct KrylovLaunch {
+  InstState* st; const int* act; int nb; double* red; unsigned* cnt; long long n3; int RB;
+};
+template <typename R> void launch_init(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_alpha(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_sy(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_zeta(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_uzrx(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_norm(const KrylovLaunch& k, cudaStream_t s);
+template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s);
+
+template <typename R>
+int solve_batch(Ctx& c, const Geo& g, double gscale, const struct dda_instance* inst, int nb, double target,
+                int max_iter, double ratio, struct dda_result* res, cudaStream_t user);
+int solve_mixed(Ctx& c, const Geo& g, double gscale, const struct dda_instance* i64,
+                const struct dda_instance* i128, int nb, double tol, double inner_tol, int max_iter, int max_outer,
+                double ratio, struct dda_result* res, cudaStream_t user);
+template <typename R>
+void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, double k, double* red, unsigned* cnt,
+                 int RB, double* out, cudaStream_t s);
+
+// Green's tensor build: FFT(-G) octant (hx,hy,hz,6) scaled by `scale`.
+// Writes complex128 to out128 (if non-null) and complex64 to out64 (if non-null).
+int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64,
+                cudaStream_t s);
+
+}  // namespace dda

@@ -1,0 +1,10 @@
+// complex64 instantiations of the matvec passes
+#include "matvec_impl.cuh"
+
+namespace dda {
+template <>
+cudaError_t launch_matvec<float>(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
+                                 int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
+  return launch_matvec_impl<float>(ctx, g, pc, st, act, nb, in_id, out_id, mode, cond, gscale, s);
+}
+}  // namespace dda

@@ -1,0 +1,374 @@
+// Host side of the engine: FFT plans and twiddles, solver workspaces, the
+// batched GPBiCGSTAB driver (graph-captured iterations, pipelined status
+// polling) and the mixed-precision iterative-refinement driver.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "../../include/dda_b200.h"
+#include "dda_host.h"
+#include "reduce.cuh"
+
+namespace dda {
+
+static thread_local std::string g_err;
+void set_error(const std::string& m) { g_err = m; }
+
+static std::atomic<long long> g_launches{0};
+void note_launch(cudaStream_t s, long long n) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+}
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+const std::string& get_error() { return g_err; }
+
+template <typename R> void launch_make_b(InstState*, int, long long, int, int, int, cudaStream_t);
+void launch_down(InstState*, int, const InstState*, int, int, long long, int, cudaStream_t);
+void launch_accum(InstState*, int, const InstState*, int, long long, int, cudaStream_t);
+template <typename R> void launch_norm2(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
+int grid_for(long long n, int nb, int num_sms);
+
+const void* Ctx::twiddles(int L, bool dbl) {
+  std::lock_guard<std::mutex> g(mu);
+  auto it = tw.find(L);
+  if (it == tw.end()) {
+    std::vector<double2> h(L);
+    std::vector<float2> hf(L);
+    const long double tau = 6.283185307179586476925286766559005768L;
+    for (int j = 0; j < L; ++j) {
+      const long double a = tau * (long double)j / (long double)L;
+      const double c = (double)cosl(a), s = (double)-sinl(a);
+      h[j] = make_double2(c, s);
+      hf[j] = make_float2((float)c, (float)s);
+    }
+    TwTable t;
+    if (cudaMalloc(&t.d128, L * sizeof(double2)) != cudaSuccess) return nullptr;
+    if (cudaMalloc(&t.d64, L * sizeof(float2)) != cudaSuccess) { cudaFree(t.d128); return nullptr; }
+    cudaMemcpy(t.d128, h.data(), L * sizeof(double2), cudaMemcpyHostToDevice);
+    cudaMemcpy(t.d64, hf.data(), L * sizeof(float2), cudaMemcpyHostToDevice);
+    it = tw.emplace(L, t).first;
+  }
+  return dbl ? it->second.d128 : it->second.d64;
+}
+
+Ctx::~Ctx() {
+  for (auto& kv : tw) { cudaFree(kv.second.d64); cudaFree(kv.second.d128); }
+}
+
+// ---------------------------------------------------------------------------
+// workspaces
+// ---------------------------------------------------------------------------
+static const int kFullSlots[] = {V_R, V_RHAT, V_P, V_V, V_T, V_S, V_SPREV, V_U, V_Z, V_W, V_Y, V_B, V_TMP,
+                                 V_XA, V_XB, V_XC};
+static const int kLightSlots[] = {V_R, V_B};
+
+BatchWs::~BatchWs() {
+  if (gexec) cudaGraphExecDestroy(gexec);
+  cudaFree(vecs); cudaFree(scratch); cudaFree(d_st); cudaFreeHost(h_st[0]); cudaFreeHost(h_st[1]);
+  cudaFree(red); cudaFree(cnt); cudaFree(d_out); cudaFreeHost(h_out);
+}
+
+int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
+  dtype = dtype_; g = g_; nb = nb_; full = full_;
+  esz = dtype == DDA_C128 ? 16 : 8;
+  n3 = (size_t)g.nsite * 3;
+  nslot = full ? (int)(sizeof(kFullSlots) / sizeof(int)) : (int)(sizeof(kLightSlots) / sizeof(int));
+  pc = make_pass_cfg(g, dtype == DDA_C128);
+  RB = grid_for((long long)n3, nb, c.num_sms);
+  t1n = (size_t)g.nx * g.ny * g.Lz * 3;
+  t2n = (size_t)g.nx * g.Ly * g.Lz * 3;
+  if (cudaMalloc(&vecs, (size_t)nb * nslot * n3 * esz) != cudaSuccess ||
+      cudaMalloc(&scratch, (size_t)nb * (t1n + t2n) * esz) != cudaSuccess ||
+      cudaMalloc((void**)&d_st, nb * sizeof(InstState)) != cudaSuccess ||
+      cudaMallocHost((void**)&h_st[0], nb * sizeof(InstState)) != cudaSuccess ||
+      cudaMallocHost((void**)&h_st[1], nb * sizeof(InstState)) != cudaSuccess ||
+      cudaMalloc((void**)&red, (size_t)nb * RB * KRED * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&cnt, nb * sizeof(unsigned)) != cudaSuccess ||
+      cudaMalloc((void**)&d_out, nb * sizeof(double)) != cudaSuccess ||
+      cudaMallocHost((void**)&h_out, nb * sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("solver workspace: out of device memory");
+    return DDA_ERR_OOM;
+  }
+  cudaMemset(cnt, 0, nb * sizeof(unsigned));
+  std::memset(h_st[0], 0, nb * sizeof(InstState));
+  return DDA_OK;
+}
+
+// base InstState of instance j: vector slots and scratch
+void BatchWs::base_state(int j, InstState& S) const {
+  std::memset(&S, 0, sizeof(S));
+  const int* slots = full ? kFullSlots : kLightSlots;
+  char* v0 = (char*)vecs + (size_t)j * nslot * n3 * esz;
+  for (int q = 0; q < nslot; ++q) S.vec[slots[q]] = v0 + (size_t)q * n3 * esz;
+  if (full) S.vec[V_X] = S.vec[V_XA];
+  char* sc = (char*)scratch + (size_t)j * (t1n + t2n) * esz;
+  S.t1 = sc;
+  S.t2 = sc + t1n * esz;
+  S.best_x = -1;
+}
+
+BatchWs* Ctx::workspace(int dtype, const Geo& g, int nb, bool full, int* err) {
+  char key[160];
+  snprintf(key, sizeof(key), "%d:%d,%d,%d:%d,%d,%d:%d:%d", dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, nb, full ? 1 : 0);
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = ws.find(key);
+  if (it != ws.end()) return it->second;
+  BatchWs* w = new BatchWs();
+  const int e = w->alloc(*this, dtype, g, nb, full);
+  if (e != DDA_OK) { delete w; *err = e; return nullptr; }
+  ws[key] = w;
+  return w;
+}
+
+void Ctx::trim() {
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& kv : ws) delete kv.second;
+  ws.clear();
+}
+
+// ---------------------------------------------------------------------------
+// one GPBiCGSTAB iteration for every instance of the workspace
+// ---------------------------------------------------------------------------
+template <typename R>
+static cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s) {
+  KrylovLaunch k{w.d_st, nullptr, w.nb, w.red, w.cnt, (long long)w.n3, w.RB};
+  cudaError_t e;
+  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
+  launch_alpha<R>(k, s);
+  launch_sy<R>(k, s);
+  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return e;
+  launch_zeta<R>(k, s);
+  launch_uzrx<R>(k, s);
+  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s)))
+    return e;
+  launch_norm<R>(k, s);
+  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s)))
+    return e;
+  launch_fin<R>(k, s);
+  return cudaGetLastError();
+}
+
+template <typename R>
+static int build_graph(Ctx& c, BatchWs& w, double gscale) {
+  if (w.gexec && w.graph_gscale == gscale) return DDA_OK;
+  if (w.gexec) { cudaGraphExecDestroy(w.gexec); w.gexec = nullptr; }
+  // make sure lazily created resources exist before capture
+  c.twiddles(w.g.Lx, sizeof(R) == 8); c.twiddles(w.g.Ly, sizeof(R) == 8); c.twiddles(w.g.Lz, sizeof(R) == 8);
+  cudaGraph_t graph;
+  DDA_CUDA_OK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = enqueue_iteration<R>(c, w, gscale, c.stream);
+  cudaError_t e2 = cudaStreamEndCapture(c.stream, &graph);
+  if (e != cudaSuccess || e2 != cudaSuccess) {
+    set_error(std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    return DDA_ERR_CUDA;
+  }
+  size_t nnodes = 0;
+  cudaGraphGetNodes(graph, nullptr, &nnodes);
+  w.graph_kernels = (long long)nnodes;
+  e = cudaGraphInstantiate(&w.gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { set_error(std::string("graph instantiate: ") + cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  w.graph_gscale = gscale;
+  return DDA_OK;
+}
+
+// Run iterations until every active instance is done.  Status is polled
+// through two pinned buffers so the GPU keeps iterating while the host checks.
+template <typename R>
+static int run_iterations(Ctx& c, BatchWs& w, double gscale, int chunk) {
+  int rc = build_graph<R>(c, w, gscale);
+  if (rc) return rc;
+  cudaStream_t s = c.stream;
+  auto enqueue_chunk = [&](int buf) -> cudaError_t {
+    for (int q = 0; q < chunk; ++q) {
+      cudaError_t e = cudaGraphLaunch(w.gexec, s);
+      if (e != cudaSuccess) return e;
+      note_launch(s, w.graph_kernels);
+    }
+    cudaError_t e = cudaMemcpyAsync(w.h_st[buf], w.d_st, w.nb * sizeof(InstState), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return e;
+    return cudaEventRecord(c.ev[buf], s);
+  };
+  DDA_CUDA_OK(enqueue_chunk(0));
+  DDA_CUDA_OK(enqueue_chunk(1));
+  for (int it = 0;; ++it) {
+    const int buf = it & 1;
+    DDA_CUDA_OK(cudaEventSynchronize(c.ev[buf]));
+    bool all = true;
+    for (int j = 0; j < w.nb; ++j) {
+      const InstState& S = w.h_st[buf][j];
+      if (S.active && !S.done) { all = false; break; }
+    }
+    if (all) break;
+    DDA_CUDA_OK(enqueue_chunk(buf));
+  }
+  DDA_CUDA_OK(cudaStreamSynchronize(s));
+  DDA_CUDA_OK(cudaMemcpy(w.h_st[0], w.d_st, w.nb * sizeof(InstState), cudaMemcpyDeviceToHost));
+  return DDA_OK;
+}
+
+static void fill_result(const InstState& S, dda_result& r) {
+  r.iters = S.ret_iters;
+  r.status = S.status == ST_CONVERGED ? DDA_OK : (S.status == ST_MAXITER ? DDA_NOT_CONVERGED : DDA_ERR_NAN);
+  r.lowest_rel = S.initial_norm > 0 ? S.lowest / S.initial_norm : NAN;
+  r.first_rel = S.initial_norm > 0 ? S.first / S.initial_norm : NAN;
+  r.true_relres = -1.0;
+  r.outer = 0;
+  r.resets = S.reset_count;
+}
+
+template <typename R>
+int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, int nb, double target, int max_iter,
+                double ratio, dda_result* res, cudaStream_t user) {
+  int err = DDA_OK;
+  const int dtype = sizeof(R) == 8 ? DDA_C128 : DDA_C64;
+  BatchWs* w = c.workspace(dtype, g, nb, true, &err);
+  if (!w) return err;
+  InstState* H = w->h_st[0];
+  for (int j = 0; j < nb; ++j) {
+    w->base_state(j, H[j]);
+    H[j].ghat = inst[j].ghat;
+    H[j].inva = inst[j].inv_alpha;
+    H[j].vec[V_TMP] = (void*)inst[j].e_inc;
+    H[j].target = target;
+    H[j].ratio = ratio;
+    H[j].max_iter = max_iter;
+    H[j].active = 1;
+  }
+  cudaStream_t s = c.stream;
+  DDA_CUDA_OK(cudaEventRecord(c.ev_user, user));
+  DDA_CUDA_OK(cudaStreamWaitEvent(s, c.ev_user, 0));
+  DDA_CUDA_OK(cudaMemcpyAsync(w->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+  launch_make_b<R>(w->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s);
+  KrylovLaunch k{w->d_st, nullptr, nb, w->red, w->cnt, (long long)w->n3, w->RB};
+  launch_init<R>(k, s);
+  DDA_CUDA_OK(cudaGetLastError());
+  int rc = run_iterations<R>(c, *w, gscale, 4);
+  if (rc) return rc;
+  const size_t bytes = w->n3 * w->esz;
+  for (int j = 0; j < nb; ++j) {
+    const InstState& S = w->h_st[0][j];
+    const void* src = nullptr;
+    if (S.status == ST_CONVERGED) src = S.vec[V_X];
+    else if (S.best_x >= 0) src = S.vec[V_XA + S.best_x];
+    if (src) DDA_CUDA_OK(cudaMemcpyAsync(inst[j].p_out, src, bytes, cudaMemcpyDeviceToDevice, s));
+    else DDA_CUDA_OK(cudaMemsetAsync(inst[j].p_out, 0, bytes, s));
+    if (res) fill_result(S, res[j]);
+  }
+  DDA_CUDA_OK(cudaEventRecord(c.ev_done, s));
+  DDA_CUDA_OK(cudaStreamWaitEvent(user, c.ev_done, 0));
+  return DDA_OK;
+}
+template int solve_batch<float>(Ctx&, const Geo&, double, const dda_instance*, int, double, int, double, dda_result*,
+                                cudaStream_t);
+template int solve_batch<double>(Ctx&, const Geo&, double, const dda_instance*, int, double, int, double,
+                                 dda_result*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// mixed precision: complex64 sweeps inside FP64 iterative refinement
+// ---------------------------------------------------------------------------
+int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, const dda_instance* i128, int nb,
+                double tol, double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
+                cudaStream_t user) {
+  int err = DDA_OK;
+  BatchWs* w64 = c.workspace(DDA_C64, g, nb, true, &err);
+  if (!w64) return err;
+  BatchWs* w128 = c.workspace(DDA_C128, g, nb, false, &err);
+  if (!w128) return err;
+  cudaStream_t s = c.stream;
+  DDA_CUDA_OK(cudaEventRecord(c.ev_user, user));
+  DDA_CUDA_OK(cudaStreamWaitEvent(s, c.ev_user, 0));
+  // FP64 side: b = mask*E, x = 0, r = b
+  InstState* H = w128->h_st[0];
+  const size_t bytes128 = w128->n3 * 16;
+  for (int j = 0; j < nb; ++j) {
+    w128->base_state(j, H[j]);
+    H[j].ghat = i128[j].ghat;
+    H[j].inva = i128[j].inv_alpha;
+    H[j].vec[V_TMP] = (void*)i128[j].e_inc;
+    H[j].vec[V_X] = i128[j].p_out;
+    H[j].active = 1;
+    DDA_CUDA_OK(cudaMemsetAsync(i128[j].p_out, 0, bytes128, s));
+  }
+  DDA_CUDA_OK(cudaMemcpyAsync(w128->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+  launch_make_b<double>(w128->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s);
+  launch_norm2<double>(w128->d_st, V_B, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s);
+  DDA_CUDA_OK(cudaMemcpyAsync(w128->h_out, w128->d_out, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+  DDA_CUDA_OK(cudaStreamSynchronize(s));
+  std::vector<double> bnorm(nb), relres(nb, 1.0);
+  std::vector<int> active(nb, 1), total(nb, 0), outer(nb, 0), resets(nb, 0), last_status(nb, ST_RUNNING);
+  std::vector<double> first_rel(nb, NAN), lowest_rel(nb, NAN);
+  for (int j = 0; j < nb; ++j) {
+    bnorm[j] = std::sqrt(w128->h_out[j]);
+    if (!(bnorm[j] > 0)) { active[j] = 0; relres[j] = 0.0; }
+  }
+  // residual r = b (x = 0)
+  for (int j = 0; j < nb; ++j)
+    DDA_CUDA_OK(cudaMemcpyAsync(H[j].vec[V_R], H[j].vec[V_B], bytes128, cudaMemcpyDeviceToDevice, s));
+  InstState* H64 = w64->h_st[0];
+  for (int sweep = 0; sweep < max_outer; ++sweep) {
+    int nact = 0;
+    for (int j = 0; j < nb; ++j) nact += active[j];
+    if (!nact) break;
+    for (int j = 0; j < nb; ++j) {
+      w64->base_state(j, H64[j]);
+      H64[j].ghat = i64[j].ghat;
+      H64[j].inva = i64[j].inv_alpha;
+      H64[j].target = inner_tol;
+      H64[j].ratio = ratio;
+      H64[j].max_iter = max_iter;
+      H64[j].active = active[j];
+      H[j].active = active[j];
+    }
+    DDA_CUDA_OK(cudaMemcpyAsync(w64->d_st, H64, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+    DDA_CUDA_OK(cudaMemcpyAsync(w128->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+    launch_down(w64->d_st, V_B, w128->d_st, V_R, nb, (long long)w64->n3, c.num_sms, s);
+    KrylovLaunch k{w64->d_st, nullptr, nb, w64->red, w64->cnt, (long long)w64->n3, w64->RB};
+    launch_init<float>(k, s);
+    int rc = run_iterations<float>(c, *w64, gscale, 4);
+    if (rc) return rc;
+    for (int j = 0; j < nb; ++j) {
+      if (!active[j]) continue;
+      const InstState& S = w64->h_st[0][j];
+      total[j] += S.ret_iters < 0 ? -S.ret_iters : S.ret_iters;
+      resets[j] += S.reset_count;
+      outer[j] += 1;
+      last_status[j] = S.status;
+      if (sweep == 0) {
+        first_rel[j] = S.initial_norm > 0 ? S.first / S.initial_norm : NAN;
+        lowest_rel[j] = S.initial_norm > 0 ? S.lowest / S.initial_norm : NAN;
+      }
+    }
+    launch_accum(w128->d_st, V_X, w64->d_st, nb, (long long)w64->n3, c.num_sms, s);
+    cudaError_t e = launch_matvec<double>(c, g, w128->pc, w128->d_st, nullptr, nb, V_X, V_R, MV_RESIDUAL, C_ACTIVE,
+                                          gscale, s);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+    launch_norm2<double>(w128->d_st, V_R, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s);
+    DDA_CUDA_OK(cudaMemcpyAsync(w128->h_out, w128->d_out, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DDA_CUDA_OK(cudaStreamSynchronize(s));
+    for (int j = 0; j < nb; ++j) {
+      if (!active[j]) continue;
+      relres[j] = std::sqrt(w128->h_out[j]) / bnorm[j];
+      if (relres[j] <= tol || std::isnan(relres[j])) active[j] = 0;
+    }
+  }
+  for (int j = 0; j < nb; ++j) {
+    if (!res) break;
+    dda_result& r = res[j];
+    r.iters = total[j];
+    r.status = (relres[j] <= tol) ? DDA_OK : (std::isnan(relres[j]) ? DDA_ERR_NAN : DDA_NOT_CONVERGED);
+    r.lowest_rel = lowest_rel[j];
+    r.first_rel = first_rel[j];
+    r.true_relres = relres[j];
+    r.outer = outer[j];
+    r.resets = resets[j];
+  }
+  DDA_CUDA_OK(cudaEventRecord(c.ev_done, s));
+  DDA_CUDA_OK(cudaStreamWaitEvent(user, c.ev_done, 0));
+  return DDA_OK;
+}
+
+}  // namespace dda

@@ -1,0 +1,157 @@
+// Small batched vector kernels around the solver: masked right-hand side,
+// precision conversion and accumulation for iterative refinement, norms, and
+// the FP64 cross-section reduction.
+#include "dda_host.h"
+#include "reduce.cuh"
+
+namespace dda {
+
+// b = mask * E  with mask = (inv_alpha != 0) (ddaforgit.py:1108; the
+// reference forms E_inc * mask at Gpbicgstab.py:935, :1064)
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_make_b(InstState* st, long long nsite, int src_id, int dst_id) {
+  typedef typename CT<R>::T C;
+  InstState& S = st[blockIdx.y];
+  if (!S.active) return;
+  const C* __restrict__ e = (const C*)S.vec[src_id];
+  const C* __restrict__ ia = (const C*)S.inva;
+  C* __restrict__ b = (C*)S.vec[dst_id];
+  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < nsite * 3; i += (long long)gridDim.x * KNT) {
+    const C a = ia[i / 3];
+    const bool m = (a.x != (R)0) || (a.y != (R)0);
+    b[i] = m ? e[i] : czero<C>();
+  }
+}
+
+// dst(c64).vec[did] = (complex64) src(c128).vec[sid]
+__global__ void __launch_bounds__(KNT) k_down(InstState* dst, int did, const InstState* src, int sid, long long n3) {
+  InstState& D = dst[blockIdx.y];
+  if (!D.active) return;
+  const double2* __restrict__ s = (const double2*)src[blockIdx.y].vec[sid];
+  float2* __restrict__ d = (float2*)D.vec[did];
+  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT)
+    d[i] = make_float2((float)s[i].x, (float)s[i].y);
+}
+
+// solution of a finished complex64 solve: the current iterate when it
+// converged, else the best one, else zero (Gpbicgstab.py:1162-1201)
+__device__ __forceinline__ const float2* sol64(const InstState& S) {
+  if (S.status == ST_CONVERGED) return (const float2*)S.vec[V_X];
+  if (S.best_x >= 0) return (const float2*)S.vec[V_XA + S.best_x];
+  return nullptr;
+}
+
+// x128 += solution(c64)
+__global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const InstState* st64, long long n3) {
+  const InstState& S = st64[blockIdx.y];
+  if (!st128[blockIdx.y].active) return;
+  const float2* __restrict__ e = sol64(S);
+  if (!e) return;
+  double2* __restrict__ x = (double2*)st128[blockIdx.y].vec[xid];
+  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT) {
+    const float2 v = e[i];
+    double2 a = x[i];
+    a.x += (double)v.x; a.y += (double)v.y;
+    x[i] = a;
+  }
+}
+
+// out[inst] = ||vec[id]||^2 (FP64, deterministic)
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_norm2(InstState* st, int id, long long n3, double* red, unsigned* cnt, int RB,
+                                               double* out) {
+  typedef typename CT<R>::T C;
+  const int inst = blockIdx.y;
+  InstState& S = st[inst];
+  if (!S.active) return;
+  const C* __restrict__ v = (const C*)S.vec[id];
+  double acc[1] = {0.0};
+  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+    const C a = v[i];
+    acc[0] += (double)a.x * a.x + (double)a.y * a.y;
+  }
+  double tot[1];
+  if (reduce_last<1>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) out[inst] = tot[0];
+}
+
+// cross sections (Draine & Flatau 1994): sums reduced in FP64
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_xsec(const typename CT<R>::T* __restrict__ P,
+                                              const typename CT<R>::T* __restrict__ E,
+                                              const typename CT<R>::T* __restrict__ ia, long long nsite, double k3,
+                                              double* red, unsigned* cnt, int RB, double* out) {
+  typedef typename CT<R>::T C;
+  double acc[2] = {0.0, 0.0};
+  for (long long j = (long long)blockIdx.x * KNT + threadIdx.x; j < nsite; j += (long long)RB * KNT) {
+    const C a = ia[j];
+    if (a.x == (R)0 && a.y == (R)0) continue;
+    double p2 = 0.0, ext = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const C p = P[j * 3 + c], e = E[j * 3 + c];
+      ext += (double)e.x * p.y - (double)e.y * p.x;       // Im(conj(e) p)
+      p2 += (double)p.x * p.x + (double)p.y * p.y;
+    }
+    // Im(P . conj(ia) P*) = Im(conj(ia)) |P|^2 = -Im(ia) |P|^2
+    acc[0] += ext;
+    acc[1] += (-(double)a.y - (2.0 / 3.0) * k3) * p2;
+  }
+  double tot[2];
+  if (reduce_last<2>(acc, tot, red, cnt, 0, RB) && threadIdx.x == 0) {
+    out[0] = tot[0];
+    out[1] = tot[1];
+  }
+}
+
+// ---------------------------------------------------------------------------
+int grid_for(long long n, int nb, int num_sms) {
+  long long want = (n + KNT - 1) / KNT;
+  long long cap = (4LL * num_sms + nb - 1) / nb;
+  if (cap < 1) cap = 1;
+  if (want > cap) want = cap;
+  if (want < 1) want = 1;
+  return (int)want;
+}
+
+template <typename R>
+void launch_make_b(InstState* st, int nb, long long nsite, int src, int dst, int num_sms, cudaStream_t s) {
+  k_make_b<R><<<dim3(grid_for(nsite * 3, nb, num_sms), nb), KNT, 0, s>>>(st, nsite, src, dst);
+  note_launch(s, 1);
+}
+template void launch_make_b<float>(InstState*, int, long long, int, int, int, cudaStream_t);
+template void launch_make_b<double>(InstState*, int, long long, int, int, int, cudaStream_t);
+
+void launch_down(InstState* dst, int did, const InstState* src, int sid, int nb, long long n3, int num_sms,
+                 cudaStream_t s) {
+  k_down<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(dst, did, src, sid, n3);
+  note_launch(s, 1);
+}
+
+void launch_accum(InstState* st128, int xid, const InstState* st64, int nb, long long n3, int num_sms,
+                  cudaStream_t s) {
+  k_accum<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(st128, xid, st64, n3);
+  note_launch(s, 1);
+}
+
+template <typename R>
+void launch_norm2(InstState* st, int id, int nb, long long n3, double* red, unsigned* cnt, int RB, double* out,
+                  cudaStream_t s) {
+  k_norm2<R><<<dim3(RB, nb), KNT, 0, s>>>(st, id, n3, red, cnt, RB, out);
+  note_launch(s, 1);
+}
+template void launch_norm2<float>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
+template void launch_norm2<double>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
+
+template <typename R>
+void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, double k, double* red, unsigned* cnt,
+                 int RB, double* out, cudaStream_t s) {
+  typedef typename CT<R>::T C;
+  k_xsec<R><<<RB, KNT, 0, s>>>((const C*)P, (const C*)E, (const C*)ia, nsite, k * k * k, red, cnt, RB, out);
+  note_launch(s, 1);
+}
+template void launch_xsec<float>(const void*, const void*, const void*, long long, double, double*, unsigned*, int,
+                                 double*, cudaStream_t);
+template void launch_xsec<double>(const void*, const void*, const void*, long long, double, double*, unsigned*, int,
+                                  double*, cudaStream_t);
+
+}  // namespace dda

@@ -1,0 +1,330 @@
+"""Device-resident DDA operator and solvers on top of the C ABI.
+
+``DDAOperator`` holds, for one geometry on one GPU, the FFT'd interaction
+tensor (built once per (grid, kd) by the engine's Green kernels), the inverse
+polarizability and the transform scratch.  Its methods call the engine's
+sm_100a kernels through ``libdda_b200.so``; PyTorch only provides device
+memory and the current stream.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_C64, _C128 = torch.complex64, torch.complex128
+
+
+def _dt_code(dtype) -> int:
+    if dtype == _C64:
+        return L.DDA_C64
+    if dtype == _C128:
+        return L.DDA_C128
+    raise TypeError(f"dtype must be complex64 or complex128, got {dtype}")
+
+
+def _device(device=None) -> torch.device:
+    if device is None:
+        if not torch.cuda.is_available():
+            raise RuntimeError("the DDA engine needs a CUDA device; none is available")
+        return torch.device("cuda", torch.cuda.current_device())
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise RuntimeError("the DDA engine runs on CUDA devices only")
+    return torch.device("cuda", d.index if d.index is not None else torch.cuda.current_device())
+
+
+def as_device(x, dtype, device) -> torch.Tensor:
+    """Contiguous device tensor of ``dtype`` from a torch tensor, any
+    DLPack-capable array (CuPy, JAX, ...) or anything NumPy accepts."""
+    if not isinstance(x, torch.Tensor):
+        if hasattr(x, "__dlpack__") and not isinstance(x, np.ndarray):
+            x = torch.from_dlpack(x)
+        else:
+            x = torch.from_numpy(np.ascontiguousarray(np.asarray(x)))
+    return x.to(device=device, dtype=dtype).contiguous()
+
+
+def stream_handle(device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+_compiled_cache: dict[int, list] = {}
+
+
+def compiled_fft_lengths(dtype=_C128) -> list:
+    code = _dt_code(dtype)
+    if code not in _compiled_cache:
+        lib = L.lib()
+        _compiled_cache[code] = [n for n in range(2, 1025, 2) if lib.dda_fft_length_ok(n, code)]
+    return _compiled_cache[code]
+
+
+def fft_lengths(shape, dtype=_C128, exact=False):
+    """FFT lengths (Lx,Ly,Lz): the smallest compiled length >= 2n per axis
+    (exactly 2n when ``exact``, as the reference's octant layout needs)."""
+    sizes = compiled_fft_lengths(dtype)
+    out = []
+    for n in shape:
+        if exact:
+            if 2 * n not in sizes:
+                raise ValueError(f"no compiled FFT length 2*{n}={2 * n}; compiled lengths: {sizes}")
+            out.append(2 * n)
+        else:
+            cand = [s for s in sizes if s >= 2 * n]
+            if not cand:
+                raise ValueError(f"box axis {n} too large (largest FFT length {sizes[-1]})")
+            out.append(cand[0])
+    return tuple(out)
+
+
+def green_octant(shape, k, d, L_=None, scale=1.0, dtype=_C128, device=None) -> torch.Tensor:
+    """scale * FFT(-G) cropped to the (Lx/2+1, Ly/2+1, Lz/2+1, 6) octant,
+    computed in FP64 by the engine (generate_interaction_row,
+    ddaforgit.py:1046-1080)."""
+    dev = _device(device)
+    nx, ny, nz = (int(v) for v in shape)
+    Lx, Ly, Lz = L_ if L_ is not None else fft_lengths(shape, _C128, exact=False)
+    out = torch.empty((Lx // 2 + 1, Ly // 2 + 1, Lz // 2 + 1, 6), dtype=dtype, device=dev)
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        p128 = out.data_ptr() if dtype == _C128 else None
+        p64 = out.data_ptr() if dtype == _C64 else None
+        L.check(L.lib().dda_green_build(ctx.handle, nx, ny, nz, Lx, Ly, Lz, float(k), float(d), float(scale),
+                                        p128, p64, stream_handle(dev)))
+    return out
+
+
+@dataclass
+class SolveInfo:
+    """Outcome of one solve (mirrors the reference's return tuple)."""
+    iters: int
+    status: str
+    lowest_rel: float
+    first_rel: float
+    true_relres: float = float("nan")
+    outer: int = 0
+    resets: int = 0
+    extra: dict = field(default_factory=dict)
+
+
+_STATUS = {L.DDA_OK: "converged", L.DDA_NOT_CONVERGED: "max_iter", L.DDA_ERR_NAN: "nan_or_stagnation"}
+
+
+def _info(r: L.dda_result) -> SolveInfo:
+    return SolveInfo(int(r.iters), _STATUS.get(r.status, str(r.status)), float(r.lowest_rel), float(r.first_rel),
+                     float(r.true_relres), int(r.outer), int(r.resets))
+
+
+class DDAOperator:
+    """A = diag(1/alpha) + off-diagonal dipole interactions of one lattice.
+
+    Parameters
+    ----------
+    inv_alpha : (nx,ny,nz) complex, 0 outside the scatterer
+    k, d      : wave number and lattice spacing (same length unit)
+    dtype     : complex64 or complex128 for vectors and the tensor
+    L         : FFT lengths (default: smallest compiled >= 2n)
+    ghat      : optional precomputed octant (e.g. the reference's
+                (nx+1,ny+1,nz+1,6) array); ``ghat_scale`` multiplies it inside
+                the kernels (default 1/(Lx Ly Lz) for an unscaled FFT(-G)).
+    """
+
+    def __init__(self, inv_alpha, k, d, dtype=_C128, L_=None, ghat=None, ghat_scale=None, device=None):
+        self.device = _device(device)
+        self.dtype = dtype
+        self.k = float(k)
+        self.d = float(d)
+        self.inv_alpha = as_device(inv_alpha, dtype, self.device)
+        if self.inv_alpha.dim() != 3:
+            raise ValueError("inv_alpha must have shape (nx, ny, nz)")
+        self.shape = tuple(int(s) for s in self.inv_alpha.shape)
+        self.nsite = int(np.prod(self.shape))
+        if ghat is not None:
+            if L_ is None:
+                L_ = tuple(2 * n for n in self.shape)
+            self.ghat = as_device(ghat, dtype, self.device)
+            want = (L_[0] // 2 + 1, L_[1] // 2 + 1, L_[2] // 2 + 1, 6)
+            if tuple(self.ghat.shape) != want:
+                raise ValueError(f"interaction matrix shape {tuple(self.ghat.shape)} != {want}")
+            self.gscale = (1.0 / (L_[0] * L_[1] * L_[2])) if ghat_scale is None else float(ghat_scale)
+        else:
+            if L_ is None:
+                L_ = fft_lengths(self.shape, dtype)
+            self.ghat = green_octant(self.shape, self.k, self.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dtype,
+                                     self.device)
+            self.gscale = 1.0
+        self.L = tuple(int(v) for v in L_)
+        self._ctx = L.context(self.device.index)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_op_create(self._ctx.handle, _dt_code(dtype), *self.shape, *self.L,
+                                          self.ghat.data_ptr(), self.gscale, self.inv_alpha.data_ptr(),
+                                          C.byref(h)))
+        self._op = h
+        self._twin = None
+
+    def __del__(self):
+        try:
+            if getattr(self, "_op", None):
+                L.lib().dda_op_destroy(self._op)
+        except Exception:
+            pass
+
+    # -- helpers ---------------------------------------------------------
+    @property
+    def mask(self) -> torch.Tensor:
+        return self.inv_alpha != 0
+
+    def _vec(self, x) -> torch.Tensor:
+        t = as_device(x, self.dtype, self.device)
+        if t.numel() != self.nsite * 3:
+            raise ValueError(f"vector size {t.numel()} doesn't match expected size {self.nsite * 3}")
+        return t.reshape(*self.shape, 3)
+
+    def _mv(self, mode, x, b=None) -> torch.Tensor:
+        x = self._vec(x)
+        y = torch.empty_like(x)
+        bp = self._vec(b).data_ptr() if b is not None else None
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_matvec(self._op, mode, x.data_ptr(), y.data_ptr(), bp, stream_handle(self.device)))
+        return y
+
+    # -- products --------------------------------------------------------
+    def matvec(self, x) -> torch.Tensor:
+        """A.x = inv_alpha x - mask * conv(x) (interaction_mult)."""
+        return self._mv(L.MV_AX, x)
+
+    def residual(self, b, x) -> torch.Tensor:
+        """mask*b - A.x."""
+        bm = self._vec(b) * self.mask[..., None]
+        return self._mv(L.MV_RESIDUAL, x, bm)
+
+    def conv(self, x) -> torch.Tensor:
+        """IFFT[FFT(-G) FFT(x)] on the box, no mask (E_field_solver)."""
+        return self._mv(L.MV_CONV, x)
+
+    def conv_masked(self, x) -> torch.Tensor:
+        """mask * conv(x) (fft_matvec)."""
+        return self._mv(L.MV_CONV_MASKED, x)
+
+    # -- precision twin (for mixed precision) ------------------------------
+    def twin(self, dtype) -> "DDAOperator":
+        """The same operator in another precision (tensor rebuilt in FP64
+        and rounded, not down-converted from this one's)."""
+        if dtype == self.dtype:
+            return self
+        if self._twin is None or self._twin.dtype != dtype:
+            if self.gscale == 1.0:
+                self._twin = DDAOperator(self.inv_alpha, self.k, self.d, dtype, self.L, device=self.device)
+            else:
+                self._twin = DDAOperator(self.inv_alpha, self.k, self.d, dtype, self.L,
+                                         ghat=self.ghat.to(dtype), ghat_scale=self.gscale, device=self.device)
+        return self._twin
+
+    # -- solves ------------------------------------------------------------
+    def solve(self, E_inc, tol=1e-5, max_iter=2000, ratio=100.0, precision=None, inner_tol=1e-4,
+              max_outer=12):
+        """Solve A.P = mask*E_inc from P0 = 0.
+
+        precision: None/'native' (this operator's dtype, reference GPBiCGSTAB),
+        'c64', 'c128', or 'mixed' (complex64 sweeps + FP64 refinement; P is
+        complex128).  Returns (P, SolveInfo)."""
+        P, infos = solve_many([self], [E_inc], tol=tol, max_iter=max_iter, ratio=ratio, precision=precision,
+                              inner_tol=inner_tol, max_outer=max_outer)
+        return P[0], infos[0]
+
+    def cross_sections(self, P, E_inc, E0=1.0):
+        return cross_sections(P, E_inc, self.inv_alpha, self.k, E0)
+
+
+def _same_bucket(ops):
+    o0 = ops[0]
+    for o in ops[1:]:
+        if o.shape != o0.shape or o.L != o0.L or o.dtype != o0.dtype or o.gscale != o0.gscale \
+                or o.device != o0.device:
+            raise ValueError("batched instances must share box, FFT lengths, dtype, tensor scale and device")
+
+
+def solve_many(ops, E_incs, tol=1e-5, max_iter=2000, ratio=100.0, precision=None, inner_tol=1e-4, max_outer=12):
+    """Batched solve: instance j is (ops[j], E_incs[j]).  Instances may share
+    an operator (many incidences) or not (many geometries of one box size).
+    Returns ([P_j], [SolveInfo_j])."""
+    ops = list(ops)
+    if len(ops) != len(E_incs):
+        raise ValueError("one incident field per operator instance")
+    if not ops:
+        return [], []
+    _same_bucket(ops)
+    o0 = ops[0]
+    dev = o0.device
+    nb = len(ops)
+    res = (L.dda_result * nb)()
+    ctx = L.context(dev.index)
+    if precision in (None, "native"):
+        precision = "c128" if o0.dtype == _C128 else "c64"
+    if precision in ("c64", "c128"):
+        dt = _C64 if precision == "c64" else _C128
+        tops = [o.twin(dt) for o in ops]
+        Es = [tops[j]._vec(E_incs[j]) for j in range(nb)]
+        Ps = [torch.empty_like(e) for e in Es]
+        inst = (L.dda_instance * nb)()
+        for j in range(nb):
+            inst[j].ghat = tops[j].ghat.data_ptr()
+            inst[j].inv_alpha = tops[j].inv_alpha.data_ptr()
+            inst[j].e_inc = Es[j].data_ptr()
+            inst[j].p_out = Ps[j].data_ptr()
+        t0 = tops[0]
+        with torch.cuda.device(dev):
+            L.check(L.lib().dda_solve_batch(ctx.handle, _dt_code(dt), *t0.shape, *t0.L, t0.gscale, inst, nb,
+                                            float(tol), int(max_iter), float(ratio), res, stream_handle(dev)))
+        return Ps, [_info(res[j]) for j in range(nb)]
+    if precision != "mixed":
+        raise ValueError("precision must be None, 'native', 'c64', 'c128' or 'mixed'")
+    o64 = [o.twin(_C64) for o in ops]
+    o128 = [o.twin(_C128) for o in ops]
+    E128 = [o128[j]._vec(E_incs[j]) for j in range(nb)]
+    P128 = [torch.empty_like(e) for e in E128]
+    i64 = (L.dda_instance * nb)()
+    i128 = (L.dda_instance * nb)()
+    for j in range(nb):
+        i64[j].ghat = o64[j].ghat.data_ptr()
+        i64[j].inv_alpha = o64[j].inv_alpha.data_ptr()
+        i128[j].ghat = o128[j].ghat.data_ptr()
+        i128[j].inv_alpha = o128[j].inv_alpha.data_ptr()
+        i128[j].e_inc = E128[j].data_ptr()
+        i128[j].p_out = P128[j].data_ptr()
+    t0 = o128[0]
+    if o64[0].gscale != t0.gscale:
+        raise ValueError("precision twins disagree on tensor scale")
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_solve_mixed_batch(ctx.handle, *t0.shape, *t0.L, t0.gscale, i64, i128, nb, float(tol),
+                                              float(inner_tol), int(max_iter), int(max_outer), float(ratio), res,
+                                              stream_handle(dev)))
+    return P128, [_info(res[j]) for j in range(nb)]
+
+
+def cross_sections(P, E_inc, inv_alpha, k, E0=1.0):
+    """(C_ext, C_abs, C_sca) reduced in FP64 on the device (Draine & Flatau
+    1994); arrays are brought to the precision of P."""
+    if not isinstance(P, torch.Tensor):
+        P = as_device(P, _C128, _device())
+    dev = _device(P.device)
+    dt = P.dtype if P.dtype in (_C64, _C128) else _C128
+    P = as_device(P, dt, dev)
+    E = as_device(E_inc, dt, dev)
+    ia = as_device(inv_alpha, dt, dev)
+    nsite = ia.numel()
+    if P.numel() != 3 * nsite or E.numel() != 3 * nsite:
+        raise ValueError("P, E_inc and inv_alpha sizes disagree")
+    out = (C.c_double * 3)()
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_cross_sections(ctx.handle, _dt_code(dt), nsite, P.data_ptr(), E.data_ptr(),
+                                           ia.data_ptr(), float(k), float(E0), out, stream_handle(dev)))
+    return float(out[0]), float(out[1]), float(out[2])

@@ -1,0 +1,178 @@
+"""The reference's call surface, backed by the engine.
+
+Same names, argument meanings, return tuples and errors as the reference's
+Python functions (Gpbicgstab.py, ExcitedField.py, ddaforgit.py), so callers
+of that path can switch imports.  Arrays may be NumPy, torch or any
+DLPack-capable device array; results are new torch CUDA tensors owned by the
+caller (the reference returns new CuPy arrays).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .engine import (DDAOperator, as_device, _device, fft_lengths, green_octant, solve_many, cross_sections,
+                     SolveInfo)
+
+_C64, _C128 = torch.complex64, torch.complex128
+
+
+def _reference_octant_dims(nx, ny, nz):
+    return (nx + 1, ny + 1, nz + 1, 6)
+
+
+def generate_interaction_row(nx, ny, nz, k, lattice_spacing, reduced=True, double_precision=False):
+    """FFT(-G) of the 2n-embedded Green's tensor (ddaforgit.py:1046-1080).
+
+    reduced=True returns the (nx+1,ny+1,nz+1,6) octant; reduced=False the full
+    (2nx,2ny,2nz,6) spectrum expanded from it by the mirror rule."""
+    dt = _C128 if double_precision else _C64
+    Ls = fft_lengths((nx, ny, nz), _C128, exact=True)
+    oct_ = green_octant((nx, ny, nz), k, lattice_spacing, Ls, 1.0, dt)
+    if reduced:
+        return oct_
+    return expand_octant(oct_, Ls)
+
+
+def expand_octant(oct_, Ls):
+    """Full (Lx,Ly,Lz,6) spectrum from the octant: index i > L/2 reads L - i,
+    xy/xz/yz flip sign when exactly one index of the pair is mirrored
+    (Gpbicgstab.py:192-211)."""
+    dev = oct_.device
+    idx, flip = [], []
+    for Ln in Ls:
+        i = torch.arange(Ln, device=dev)
+        f = i > Ln // 2
+        idx.append(torch.where(f, Ln - i, i))
+        flip.append(f)
+    full = oct_[idx[0]][:, idx[1]][:, :, idx[2]].clone()
+    fx, fy, fz = flip[0][:, None, None], flip[1][None, :, None], flip[2][None, None, :]
+    for comp, (a, b) in ((1, (fx, fy)), (2, (fx, fz)), (4, (fy, fz))):
+        s = torch.where(a != b, -1.0, 1.0).to(full.real.dtype)
+        full[..., comp] = full[..., comp] * s
+    return full
+
+
+def prepare_interaction_matrices(grid_size, k, refract_mult, x_expansion, y_expansion, z_expansion, alpha_array,
+                                 lattice_spacing, reduced=True, is_2d=False, cutoff=False, double_precision=False):
+    """(inv_alpha, mask, interaction_matrix, preconditioner) as in
+    ddaforgit.py:1085-1159.  The reference's preconditioner builders are not
+    part of it (they are imported from missing modules), so preconditioner is
+    None and solves run with precon=False."""
+    dt = _C128 if double_precision else _C64
+    dev = _device()
+    a = as_device(alpha_array, dt, dev)
+    if cutoff:
+        a = torch.where(a.abs() < 1.0, torch.zeros_like(a), a)
+    nz_ = a != 0
+    inv_alpha = torch.where(nz_, 1.0 / torch.where(nz_, a, torch.ones_like(a)), torch.zeros_like(a))
+    mask = nz_
+    nx, ny, nz = grid_size
+    G = generate_interaction_row(nx, ny, nz, k, lattice_spacing, reduced=reduced, double_precision=double_precision)
+    return inv_alpha, mask, G, None
+
+
+def _inv_alpha_box(alpha_inv, nx, ny, nz, dt, dev):
+    t = as_device(alpha_inv, dt, dev)
+    if t.numel() == 3 * nx * ny * nz:          # the reference's repeat(inv_alpha, 3) form
+        t = t.reshape(-1)[::3].contiguous()
+    if t.numel() != nx * ny * nz:
+        raise ValueError(f"inverse polarizability size {t.numel()} doesn't match grid {(nx, ny, nz)}")
+    return t.reshape(nx, ny, nz)
+
+
+def _check_mask(mask, ia):
+    if mask is None:
+        return
+    m = as_device(mask, torch.bool, ia.device).reshape(ia.shape) if not isinstance(mask, torch.Tensor) \
+        else mask.to(ia.device).reshape(ia.shape).bool()
+    if not torch.equal(m, ia != 0):
+        raise ValueError("mask must equal (inv_alpha != 0), as prepare_interaction_matrices builds it")
+
+
+def _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dt):
+    dev = _device()
+    ia = _inv_alpha_box(alpha_inv, nx, ny, nz, dt, dev)
+    G = as_device(interaction_matrix, dt, dev)
+    if tuple(G.shape) != _reference_octant_dims(nx, ny, nz):
+        raise ValueError(f"interaction matrix shape {tuple(G.shape)} != {_reference_octant_dims(nx, ny, nz)}")
+    return DDAOperator(ia, 1.0, 1.0, dtype=dt, L_=(2 * nx, 2 * ny, 2 * nz), ghat=G, device=dev)
+
+
+def interaction_mult(in_array, out_array, interaction_matrix, alpha_inv, mask, chunk_params, nx, ny, nz,
+                     dtype=_C64):
+    """A.x = alpha_inv*x - mask*conv(x) (Gpbicgstab.py:828-830), flattened
+    to 3N like the reference.  out_array and chunk_params are accepted and
+    ignored (the engine needs no chunking)."""
+    op = _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dtype)
+    _check_mask(mask, op.inv_alpha)
+    return op.matvec(in_array).reshape(-1)
+
+
+def fft_matvec(in_array, out_array, matrix, mask, chunk_params, nx, ny, nz, dtype=_C64):
+    """mask * IFFT[Ghat FFT(pad x)] cropped (Gpbicgstab.py:742-772), 3N flat."""
+    dev = _device()
+    m = as_device(mask, torch.bool, dev).reshape(nx, ny, nz)
+    ia = torch.where(m, torch.ones((), dtype=dtype, device=dev), torch.zeros((), dtype=dtype, device=dev))
+    op = _op_from_reference(matrix, ia, nx, ny, nz, dtype)
+    return op.conv_masked(in_array).reshape(-1)
+
+
+def E_field_solver(polarization, interaction_matrix, grid_size, dtype=_C64):
+    """Excited field IFFT[FFT(-A) FFT(P)] on the lattice, (nx,ny,nz,3), no
+    mask and no alpha term (ExcitedField.py:129-195).  Raises ValueError on a
+    size mismatch like the reference (:143-152)."""
+    nx, ny, nz = grid_size
+    expected = nx * ny * nz * 3
+    size = polarization.numel() if isinstance(polarization, torch.Tensor) else np.size(polarization)
+    if size != expected:
+        raise ValueError(f"Polarization size {size} doesn't match expected size {expected}")
+    dev = _device()
+    ones = torch.ones((nx, ny, nz), dtype=dtype, device=dev)
+    op = _op_from_reference(interaction_matrix, ones, nx, ny, nz, dtype)
+    return op.conv(polarization)
+
+
+def solve_gpbicgstab(grid_size, inv_alpha, interaction_matrix, preconditioner, E_inc, mask, ratio, max_iter,
+                     target=1e-5, initial_p=None, is_2d=False, precon=True, dtype=_C64):
+    """GPBiCGSTAB solve of A.P = E_inc*mask (Gpbicgstab.py:879-1201).
+
+    Returns (iters, P (nx,ny,nz,3), lowest_norm/initial, first_norm/initial)
+    with the reference's codes: i+1 when converged, max_iter when not,
+    -(i+1) on NaN or stagnation.  The reference computes in complex64; pass
+    dtype=torch.complex128 for the FP64 solve it imports from a missing
+    module.  precon=True needs the reference's preconditioner builder, which
+    it does not ship; it raises NotImplementedError, as does is_2d."""
+    if is_2d:
+        raise NotImplementedError("the 2D preconditioned path is not part of the engine")
+    if precon:
+        raise NotImplementedError("preconditioned solves need the reference's missing preconditioner builder; "
+                                  "call with precon=False")
+    nx, ny, nz = grid_size
+    op = _op_from_reference(interaction_matrix, inv_alpha, nx, ny, nz, dtype)
+    _check_mask(mask, op.inv_alpha)
+    P, info = op.solve(E_inc, tol=target, max_iter=max_iter, ratio=ratio)
+    return info.iters, P, info.lowest_rel, info.first_rel
+
+
+def Gpbicgstab(A, E_inc, tol=1e-5, maxiter=2000, ratio=100.0, precision=None):
+    """Short form: solve A.P = E_inc for a DDAOperator A; returns (P, iters)."""
+    P, info = A.solve(E_inc, tol=tol, max_iter=maxiter, ratio=ratio, precision=precision)
+    return P, info.iters
+
+
+def run_solver(grid_size, k, alpha_array, lattice_spacing, x_expansion, y_expansion, z_expansion, refract_mult,
+               E_inc, precon=True, max_iter=20000, double=False, ratio=0):
+    """prepare_interaction_matrices + solve_gpbicgstab with ratio forced to
+    100, returning (iters, P, lowest_rel) (ddaforgit.py:1174-1210); errors
+    are re-raised as RuntimeError("Solver failed: ...")."""
+    try:
+        inv_alpha, mask, G, pre = prepare_interaction_matrices(grid_size, k, refract_mult, x_expansion,
+                                                               y_expansion, z_expansion, alpha_array,
+                                                               lattice_spacing, double_precision=double)
+        ratio = 100
+        r = solve_gpbicgstab(grid_size, inv_alpha, G, pre, E_inc, mask, ratio, max_iter, precon=precon,
+                             dtype=_C128 if double else _C64)
+        return r[0], r[1], r[2]
+    except Exception as e:  # noqa: BLE001 - same contract as the reference wrapper
+        raise RuntimeError(f"Solver failed: {str(e)}")

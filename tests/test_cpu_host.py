@@ -1,0 +1,119 @@
+"""CPU checks of the host-side product code and of the C-ABI library (no
+compute calls: there is no GPU here)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import dda_oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "dda_b200.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(dda_[a-z0-9_]+)\s*\(", txt)))
+
+
+def _lib():
+    from precondda_b200 import _lib as L
+    if not os.path.exists(L.LIB_PATH):
+        pytest.skip("engine library not built")
+    return L
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib()
+    lib = L.lib()
+    decl = _declared_symbols()
+    assert len(decl) >= 10
+    for name in decl:
+        assert hasattr(lib, name), name
+    assert set(decl) == set(L.EXPORTS)
+
+
+def test_library_host_only_entry_points():
+    L = _lib()
+    lib = L.lib()
+    assert lib.dda_version() >= 100
+    ok = [n for n in range(2, 600, 2) if lib.dda_fft_length_ok(n, L.DDA_C128)]
+    assert 16 in ok and 64 in ok and 128 in ok and 256 in ok and 512 in ok
+    assert not lib.dda_fft_length_ok(22, L.DDA_C128)      # 11 is not a compiled factor
+    assert not lib.dda_fft_length_ok(7, L.DDA_C128)       # odd
+    for n in ok:
+        m = n
+        for p in (2, 3, 5, 7):
+            while m % p == 0:
+                m //= p
+        assert m == 1
+
+
+def test_fft_lengths_choice():
+    _lib()
+    from precondda_b200 import fft_lengths
+    assert fft_lengths((32, 32, 32)) == (64, 64, 64)
+    assert fft_lengths((64, 48, 128)) == (128, 96, 256)
+    Lx, Ly, Lz = fft_lengths((33, 50, 7))
+    assert Lx >= 66 and Ly >= 100 and Lz >= 14
+    with pytest.raises(ValueError):
+        fft_lengths((11, 4, 4), exact=True)
+
+
+def test_alpha_matches_oracle():
+    from precondda_b200 import calculate_alpha
+    for meth in ("CM", "RR"):
+        assert calculate_alpha(1.7 + 0.1j, 0.02, 12.0, method=meth) == O.calculate_alpha(1.7 + 0.1j, 0.02, 12.0,
+                                                                                         method=meth)
+    a = calculate_alpha(1.7 + 0.1j, 0.02, 12.0, (0, 0, 1), (1, 0, 0))
+    assert a == O.calculate_alpha(1.7 + 0.1j, 0.02, 12.0, (0, 0, 1), (1, 0, 0))
+
+
+def test_sphere_and_ellipsoid_occupancy():
+    from precondda_b200 import sphere_occupancy, ellipsoid_occupancy, euler_rotation
+    assert sphere_occupancy(32, 16.0).sum() == 17256
+    assert np.array_equal(sphere_occupancy(20, 9.3), O.sphere_lattice(20, 9.3))
+    R = euler_rotation(0.3, 1.1, -0.7)
+    assert np.allclose(R @ R.T, np.eye(3))
+    occ = ellipsoid_occupancy((24, 20, 16), (10, 8, 6), R)
+    pts = O.voxel_centres((24, 20, 16), 1.0) - np.array([12.0, 10.0, 8.0])
+    ref = O.ellipsoid_mask(pts.reshape(-1, 3), (0, 0, 0), (10, 8, 6), rotation=R).reshape(24, 20, 16)
+    assert np.array_equal(occ, ref)
+
+
+def test_build_problem_from_shapes_sphere():
+    from precondda_b200 import build_problem_from_shapes
+    d = 0.02
+    prob = build_problem_from_shapes([{"type": "sphere", "center": [0.16, 0.16, 0.16], "radius": 0.16, "n": 1.5}],
+                                     np.array([0.0, 0.0, 1.0]), [1.0, 0.0, 0.0], 0.5, d, method="RR")
+    a = prob["alpha_array"]
+    assert a.shape[0] % 2 == 0 and a.shape[1] % 2 == 0 and a.shape[2] % 2 == 0
+    assert np.count_nonzero(a) > 0
+    assert np.all(a[a != 0] == O.calculate_alpha(1.5, d, 2 * np.pi / 0.5, method="RR"))
+    E = prob["E_inc"]
+    assert E.shape == a.shape + (3,)
+    assert np.allclose(E, O.incident_field(a.shape, d, 2 * np.pi / 0.5, (0, 0, 1), (1, 0, 0)))
+
+
+def test_trim_zero_faces_pads_to_even():
+    from precondda_b200 import trim_zero_faces
+    a = np.zeros((9, 9, 9), complex)
+    a[2:5, 1:8, 3:4] = 1
+    t = trim_zero_faces(a)
+    assert t.shape == (4, 8, 2)
+    assert np.array_equal(t, O.trim_zero_faces(a))
+
+
+def test_shape_membership_zoo():
+    from precondda_b200.lattice import inside_rectangle, inside_cylinder, inside_prism
+    g = O.voxel_centres((12, 12, 12), 1.0).reshape(-1, 3)
+    r = inside_rectangle(g, (6, 6, 6), (4, 6, 8))
+    assert r.sum() == 4 * 6 * 8
+    c = inside_cylinder(g, (6, 6, 6), 3.0, 4.0, "z")
+    assert c.sum() > 0 and c.sum() < np.pi * 9 * 4 * 1.3
+    p = inside_prism(g, (6, 6, 6), 4.0, 6.0, 4, "z")
+    assert p.sum() > 0
+    # a square prism (4 sides, vertices on the axes) has area 2 r^2
+    assert abs(p.sum() / 6 - 2 * 16) < 12

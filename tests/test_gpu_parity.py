@@ -1,0 +1,180 @@
+"""GPU parity of the engine against the CPU oracle (complex128 restatement of
+the reference's algorithm).  Every call goes through libdda_b200.so."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import dda_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+C64, C128 = torch.complex64, torch.complex128
+
+
+def _pkg():
+    import precondda_b200 as P
+    return P
+
+
+def _rand_problem(shape, seed, m=1.5 + 0.1j, fill=0.7, wavelength=0.5, kd=0.4):
+    rng = np.random.default_rng(seed)
+    k = 2 * np.pi / wavelength
+    d = kd / k
+    a = O.calculate_alpha(m, d, k, method="RR")
+    alpha = np.where(rng.random(shape) < fill, a, 0).astype(np.complex128)
+    x = rng.standard_normal(shape + (3,)) + 1j * rng.standard_normal(shape + (3,))
+    return k, d, alpha, x
+
+
+def _rel(a, b):
+    a = np.asarray(a); b = np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("shape,L", [((4, 6, 8), None), ((6, 10, 12), None), ((5, 7, 9), None),
+                                     ((4, 4, 4), (16, 12, 8))])
+def test_green_octant_matches_oracle(shape, L):
+    P = _pkg()
+    k, d = 2 * np.pi / 0.5, 0.02
+    Ls = L or P.fft_lengths(shape)
+    g = P.green_octant(shape, k, d, Ls, 1.0, C128).cpu().numpy()
+    ref = O.generate_interaction_row(*shape, k, d, L=Ls)
+    assert g.shape == ref.shape
+    assert _rel(g, ref) < 1e-12
+    g64 = P.green_octant(shape, k, d, Ls, 1.0, C64).cpu().numpy()
+    assert _rel(g64, ref) < 1e-6
+
+
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 10, 12), (5, 7, 9), (12, 4, 6), (16, 16, 16)])
+@pytest.mark.parametrize("dtype,tol", [(C128, 1e-12), (C64, 2e-5)])
+def test_matvec_matches_oracle(shape, dtype, tol):
+    P = _pkg()
+    k, d, alpha, x = _rand_problem(shape, seed=sum(shape))
+    ia, mask, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=dtype)
+    Gref = O.generate_interaction_row(*shape, k, d, L=op.L)
+    ref = O.interaction_mult(x, Gref, ia, mask, L=op.L)
+    y = op.matvec(x).cpu().numpy()
+    assert _rel(y, ref) < tol
+    # the other pass-5 modes
+    conv = O.fft_convolve(x, Gref, op.L)
+    assert _rel(op.conv(x).cpu().numpy(), conv) < tol
+    assert _rel(op.conv_masked(x).cpu().numpy(), conv * mask[..., None]) < tol
+    b = x[::-1].copy()
+    r = op.residual(b, x).cpu().numpy()
+    assert _rel(r, b * mask[..., None] - ref) < tol
+
+
+def test_matvec_dense_tiny():
+    P = _pkg()
+    k, d, alpha, x = _rand_problem((4, 4, 4), seed=3)
+    ia, mask, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    dense = O.dense_interaction_mult(x, ia, k, d, mask)
+    assert _rel(op.matvec(x).cpu().numpy(), dense) < 1e-12
+
+
+def _sphere_problem(n, m, kd=0.5, wavelength=0.5, pol=(1, 0, 0), kdir=(0, 0, 1)):
+    k = 2 * np.pi / wavelength
+    d = kd / (abs(m) * k)
+    occ = O.sphere_lattice(n, n / 2.0)
+    a = O.calculate_alpha(m, d, k, method="RR")
+    alpha = np.where(occ, a, 0).astype(np.complex128)
+    E = O.incident_field((n, n, n), d, k, kdir, pol)
+    return k, d, alpha, E
+
+
+@pytest.mark.parametrize("n,m", [(8, 1.5 + 0.01j), (12, 1.7 + 0.1j)])
+def test_solver_c128_matches_oracle(n, m):
+    P = _pkg()
+    k, d, alpha, E = _sphere_problem(n, m)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    it_ref, P_ref, low_ref, first_ref = O.solve_gpbicgstab((n, n, n), ia, G, E, mask, 100, 500, target=1e-6)
+    op = P.DDAOperator(ia, k, d, dtype=C128, L_=(2 * n,) * 3)
+    Pg, info = op.solve(E, tol=1e-6, max_iter=500, ratio=100)
+    assert info.iters == it_ref > 0
+    assert _rel(Pg.cpu().numpy(), P_ref) < 1e-8
+    assert abs(info.lowest_rel - low_ref) <= 1e-8 * max(low_ref, 1e-12) + 1e-14
+    assert abs(info.first_rel - first_ref) <= 1e-9
+    rr = O.true_relative_residual(Pg.cpu().numpy(), E, G, ia, mask)
+    assert rr < 5e-6
+
+
+def test_solver_c64_close_to_oracle():
+    P = _pkg()
+    n, m = 12, 1.5 + 0.01j
+    k, d, alpha, E = _sphere_problem(n, m)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    _, P_ref, _, _ = O.solve_gpbicgstab((n, n, n), ia, G, E, mask, 100, 500, target=1e-8)
+    op = P.DDAOperator(ia, k, d, dtype=C64)
+    Pg, info = op.solve(E, tol=1e-5, max_iter=500, ratio=100)
+    assert info.status == "converged"
+    err = np.linalg.norm(Pg.cpu().numpy() - P_ref) / np.linalg.norm(P_ref)
+    assert err < 1e-4
+
+
+def test_mixed_precision_reaches_fp64_tolerance():
+    P = _pkg()
+    n, m = 12, 1.7 + 0.1j
+    k, d, alpha, E = _sphere_problem(n, m)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    _, P_ref, _, _ = O.solve_gpbicgstab((n, n, n), ia, G, E, mask, 100, 1000, target=1e-10)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    Pg, info = op.solve(E, tol=1e-6, max_iter=500, ratio=100, precision="mixed", inner_tol=1e-4)
+    assert info.status == "converged", info
+    assert info.true_relres <= 1e-6
+    Pn = Pg.cpu().numpy()
+    assert O.true_relative_residual(Pn, E, G, ia, mask) <= 1.05e-6
+    assert np.linalg.norm(Pn - P_ref) / np.linalg.norm(P_ref) < 1e-5
+    ce, ca, cs = O.cross_sections(P_ref, E, ia, k)
+    ge, ga, gs = op.cross_sections(Pg, E)
+    assert abs(ge - ce) / abs(ce) < 1e-5 and abs(ga - ca) / abs(ca) < 1e-5
+
+
+def test_cross_sections_match_oracle():
+    P = _pkg()
+    rng = np.random.default_rng(5)
+    shape = (6, 7, 8)
+    ia = np.where(rng.random(shape) < 0.6, rng.standard_normal(shape) + 1j * rng.standard_normal(shape), 0)
+    Pv = rng.standard_normal(shape + (3,)) + 1j * rng.standard_normal(shape + (3,))
+    E = rng.standard_normal(shape + (3,)) + 1j * rng.standard_normal(shape + (3,))
+    k = 3.7
+    ref = O.cross_sections(Pv, E, ia, k, E0=1.3)
+    got = P.cross_sections(torch.tensor(Pv, device="cuda"), E, ia, k, E0=1.3)
+    for a, b in zip(got, ref):
+        assert abs(a - b) <= 1e-11 * max(abs(b), 1.0)
+
+
+def test_batch_matches_single():
+    P = _pkg()
+    n, m = 10, 1.5 + 0.05j
+    k, d, alpha, _ = _sphere_problem(n, m)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    dirs = [((0, 0, 1), (1, 0, 0)), ((0, 0, 1), (0, 1, 0)), ((1, 0, 0), (0, 0, 1)), ((0, 1, 0), (1, 0, 0))]
+    Es = [O.incident_field((n, n, n), d, k, kd_, pol) for kd_, pol in dirs]
+    Pb, infos = P.solve_many([op] * len(Es), Es, tol=1e-6, max_iter=400, ratio=100)
+    for E, Pj, inf in zip(Es, Pb, infos):
+        Ps, inf1 = op.solve(E, tol=1e-6, max_iter=400, ratio=100)
+        assert inf.iters == inf1.iters
+        assert _rel(Pj.cpu().numpy(), Ps.cpu().numpy()) < 1e-9
+
+
+def test_reference_api_solve_and_near_field():
+    P = _pkg()
+    n, m = 8, 1.5 + 0.01j
+    k, d, alpha, E = _sphere_problem(n, m)
+    ia, mask, G, _ = P.prepare_interaction_matrices((n, n, n), k, None, 0, 0, 0, alpha, d, double_precision=True)
+    iters, Pg, low, first = P.solve_gpbicgstab((n, n, n), ia, G, None, E, mask, 100, 300, target=1e-6,
+                                               precon=False, dtype=C128)
+    ia_o, mask_o, G_o, _ = O.prepare_interaction_matrices(alpha, k, d)
+    assert np.abs(G.cpu().numpy() - G_o).max() / np.abs(G_o).max() < 1e-12
+    it_ref, P_ref, _, _ = O.solve_gpbicgstab((n, n, n), ia_o, G_o, E, mask_o, 100, 300, target=1e-6)
+    assert iters == it_ref
+    assert _rel(Pg.cpu().numpy(), P_ref) < 1e-8
+    Ef = P.E_field_solver(Pg, G, (n, n, n), dtype=C128).cpu().numpy()
+    assert _rel(Ef, O.E_field_solver(P_ref, G_o, (n, n, n))) < 1e-8
+    with pytest.raises(ValueError):
+        P.E_field_solver(Pg.reshape(-1)[:-3], G, (n, n, n))
+    with pytest.raises(NotImplementedError):
+        P.solve_gpbicgstab((n, n, n), ia, G, None, E, mask, 100, 10, precon=True)
