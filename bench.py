@@ -34,8 +34,9 @@ N_BOX, M_REF, KD_M, WAVELENGTH = 64, 1.7 + 0.1j, 0.5, 0.5
 TOL, INNER_TOL, MAX_ITER, RATIO = 1e-6, 1e-4, 2000, 100.0
 # Iterations the reference's complex128 GPBiCGSTAB (ratio 100, tol 1e-6) takes
 # on this problem, x polarisation, measured with the CPU oracle; it scales the
-# CPU per-iteration time to a whole solve for the CPU arms.
-REF_ITERS_64 = None
+# CPU per-iteration time to a whole solve for the CPU arms (oracle run: 123
+# iterations, relative residual 7.0e-7).
+REF_ITERS_64 = 123
 
 
 def problem(n=N_BOX, m=M_REF):
@@ -356,6 +357,34 @@ def run_ours(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_profile_matvec(args, local):
+    """Matvecs only, for ncu: box n^3 (sphere-like fill), given dtype."""
+    import torch
+    import precondda_b200 as P
+    dev = torch.device("cuda", local)
+    n = args.profile_matvec
+    dt = torch.complex64 if args.dtype == "c64" else torch.complex128
+    k = 2 * math.pi / WAVELENGTH
+    d = KD_M / (abs(M_REF) * k)
+    from precondda_b200 import sphere_occupancy
+    occ = sphere_occupancy(n, n / 2.0)
+    ia = np.where(occ, 1.0 / (0.01 + 0.001j), 0).astype(np.complex128)
+    op = P.DDAOperator(ia, k, d, dtype=dt, device=dev)
+    x = torch.randn(n, n, n, 3, dtype=dt, device=dev)
+    for _ in range(args.reps):
+        y = op.matvec(x)
+    torch.cuda.synchronize()
+    out = {"profile_matvec": n, "dtype": args.dtype, "reps": args.reps, "L": op.L,
+           "p3_variant": os.environ.get("DDA_P3_VARIANT", "default"), "checksum": float(y.abs().sum())}
+    if args.time:
+        flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+        t = time_matvec(op, 20, flush)
+        B = matvec_bytes(op.shape, 8 if dt == torch.complex64 else 16)
+        peak, _ = measured_peak()
+        out.update({"ms": t * 1e3, "GBps": B / t / 1e9, "frac": B / t / 1e9 / peak})
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -363,8 +392,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile-matvec", type=int, default=0, help="only run matvecs on an n^3 box (for ncu)")
+    ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--time", action="store_true", help="with --profile-matvec: time 20 launches (L2 flushed)")
     args = ap.parse_args()
     ws, rank, local = dist_init()
+    if args.profile_matvec:
+        run_profile_matvec(args, local)
+        return
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)

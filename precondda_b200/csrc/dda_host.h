@@ -66,12 +66,13 @@ struct Ctx {
 
 // Launch geometry of the five matvec passes for one (Geo, dtype).
 struct PassCfg {
-  int NL, WS1;      // z passes: lines per tile, smem row stride
-  int Tz2, WS2;     // y passes: kz per tile
-  int Tz3, WS3;     // x pass
-  size_t smem1, smem2, smem3;
-  int ntz2, ntz3;
-  long long grid1, grid2, grid3;
+  int nl = 1, th1 = 0;           // z passes: lines per CTA, threads
+  int tz2 = 1, th2 = 0, ntz2 = 1;  // y passes: kz columns per CTA
+  int tz3 = 1, th3 = 0, ntz3 = 1;  // x pass
+  int p3reg = 0;                 // x pass keeps 3 components per thread
+  int p3var = 0;                 // x pass kernel variant
+  size_t smem1 = 0, smem2 = 0, smem3 = 0;
+  long long grid1 = 0, grid2 = 0, grid3 = 0;
 };
 
 PassCfg make_pass_cfg(const Geo& g, bool dbl);

@@ -43,39 +43,36 @@ template <class C> __device__ __forceinline__ void dft8(C* a) {
 
 template <class C> __device__ __forceinline__ void dft16(C* a) {
   typedef decltype(a[0].x) R;
-  // 16 = 4 x 4: columns, twiddle W16^(n1*k2), rows
+  // 16 = 4 x 4 in place: DFT4 over n2 (stride 4), twiddle W16^(n1*k2),
+  // DFT4 over n1, then the index transpose X[4 k1 + k2] = a[4 k2 + k1]
+  // (a register renaming once unrolled).
   const R c1 = (R)0.9238795325112867, s1 = (R)0.3826834323650898, h = (R)0.7071067811865476;
-  C b[16];
 #pragma unroll
-  for (int n1 = 0; n1 < 4; ++n1) {
-    C x0 = a[n1], x1 = a[n1 + 4], x2 = a[n1 + 8], x3 = a[n1 + 12];
-    dft4(x0, x1, x2, x3);
-    b[n1 * 4 + 0] = x0; b[n1 * 4 + 1] = x1; b[n1 * 4 + 2] = x2; b[n1 * 4 + 3] = x3;
-  }
-  // twiddles W16^(n1*k2) for n1,k2 in 1..3
-  auto tw = [&](C v, int e) -> C {
-    C w;
-    switch (e) {
-      case 1: w.x = c1; w.y = -s1; break;
-      case 2: w.x = h; w.y = -h; break;
-      case 3: w.x = s1; w.y = -c1; break;
-      case 4: w.x = 0; w.y = -1; break;
-      case 6: w.x = -h; w.y = -h; break;
-      case 9: w.x = -c1; w.y = s1; break;
-      default: w.x = 1; w.y = 0; break;
-    }
-    return cmul(v, w);
-  };
+  for (int n1 = 0; n1 < 4; ++n1) dft4(a[n1], a[n1 + 4], a[n1 + 8], a[n1 + 12]);
+  // now a[n1 + 4 k2]; twiddles
+  C t;
+  // n1=1: W^1, W^2, W^3
+  t = a[5];  a[5].x = c1 * t.x + s1 * t.y;  a[5].y = c1 * t.y - s1 * t.x;
+  t = a[9];  a[9].x = h * (t.x + t.y);      a[9].y = h * (t.y - t.x);
+  t = a[13]; a[13].x = s1 * t.x + c1 * t.y; a[13].y = s1 * t.y - c1 * t.x;
+  // n1=2: W^2, W^4, W^6
+  t = a[6];  a[6].x = h * (t.x + t.y);      a[6].y = h * (t.y - t.x);
+  a[10] = cmul_mi(a[10]);
+  t = a[14]; a[14].x = h * (t.y - t.x);     a[14].y = -h * (t.x + t.y);
+  // n1=3: W^3, W^6, W^9
+  t = a[7];  a[7].x = s1 * t.x + c1 * t.y;  a[7].y = s1 * t.y - c1 * t.x;
+  t = a[11]; a[11].x = h * (t.y - t.x);     a[11].y = -h * (t.x + t.y);
+  t = a[15]; a[15].x = -c1 * t.x - s1 * t.y; a[15].y = -c1 * t.y + s1 * t.x;
 #pragma unroll
-  for (int n1 = 1; n1 < 4; ++n1)
+  for (int k2 = 0; k2 < 4; ++k2) dft4(a[4 * k2], a[4 * k2 + 1], a[4 * k2 + 2], a[4 * k2 + 3]);
+  // a[4 k2 + k1] holds X[4 k1 + k2]: transpose the 4x4 index
+  C o[16];
 #pragma unroll
-    for (int k2 = 1; k2 < 4; ++k2) b[n1 * 4 + k2] = tw(b[n1 * 4 + k2], n1 * k2);
+  for (int k1 = 0; k1 < 4; ++k1)
 #pragma unroll
-  for (int k2 = 0; k2 < 4; ++k2) {
-    C x0 = b[0 * 4 + k2], x1 = b[1 * 4 + k2], x2 = b[2 * 4 + k2], x3 = b[3 * 4 + k2];
-    dft4(x0, x1, x2, x3);
-    a[k2] = x0; a[k2 + 4] = x1; a[k2 + 8] = x2; a[k2 + 12] = x3;
-  }
+    for (int k2 = 0; k2 < 4; ++k2) o[4 * k1 + k2] = a[4 * k2 + k1];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) a[i] = o[i];
 }
 
 // odd radix via the conjugate-pair formulation:

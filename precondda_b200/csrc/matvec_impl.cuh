@@ -11,106 +11,109 @@
 //           Ghat read from the reduced octant through the mirror rule
 //   pass 4  y-IFFT, keep rows y < ny           T2               -> T1
 //   pass 5  z-IFFT, keep z < nz, fused combine T1               -> y
-// The reference computes the same product with separate padded cuFFT calls in
-// x-chunks (Gpbicgstab.py:742-772) and the mirrored tensor kernel
+// Each pass loads its first FFT stage straight from global memory into
+// registers and stores its last stage straight back (fftreg.cuh), so a
+// two-stage length costs one shared-memory exchange.  The reference computes
+// the same product with separate padded cuFFT calls in x-chunks
+// (Gpbicgstab.py:742-772) and the mirrored tensor kernel
 // chunked_dot_product_reduced_kernel (Gpbicgstab.py:167-237).
 #pragma once
 #include "dda_host.h"
-#include "fft_core.cuh"
+#include "fftreg.cuh"
 #include "fft_sizes.h"
+#include <cstdlib>
+#include <type_traits>
 
 namespace dda {
 
-template <typename R> struct KP;            // per-precision tile constants
-template <> struct KP<float> { static constexpr int EPT = 24, NT = 256; };
-template <> struct KP<double> { static constexpr int EPT = 12, NT = 256; };
+constexpr int kMvMaxThreads = 384;
+
+template <typename R, int L>
+struct MvShape {
+  typedef typename PlanFor<L, R>::type P;
+  static constexpr int T = P::T, E = P::E, LP = ppad_len(L);
+};
+
+// Pass-3 variants (chosen by the launch configuration):
+//   0: default plan, tensor product through shared memory
+//   1: radix<=8 plan, three components per thread, tensor product in registers
+//   2: radix<=8 plan, tensor product through shared memory
+template <typename R, int L, int V>
+struct P3Shape {
+  typedef typename std::conditional<V == 0, typename PlanFor<L, R>::type, typename Plan8<L>::type>::type P;
+  static constexpr int T = P::T, E = P::E, LP = ppad_len(L);
+  static constexpr bool REG = (V == 1);
+};
+constexpr int kP3Variants = 3;
 
 __device__ __forceinline__ int inst_of(const int* act) { return act ? act[blockIdx.y] : (int)blockIdx.y; }
 
 // ---------------------------------------------------------------------------
-// pass 1: forward z on NL lines; input zero beyond nz
+// pass 1: forward z on nl lines x 3 components; input zero beyond nz
+// thread = (c fastest, t, line)
 // ---------------------------------------------------------------------------
 template <typename R, int LZ>
-__global__ void __launch_bounds__(KP<R>::NT) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                        InstState* st, const int* act, int in_id, int cond, int NL) {
+__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                            InstState* st, const int* act, int in_id, int cond,
+                                                            int nl) {
   typedef typename CT<R>::T C;
-  constexpr int NT = KP<R>::NT;
-  constexpr int LS = 3 * LZ;
+  typedef MvShape<R, LZ> SH;
+  typedef typename SH::P P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   const C* __restrict__ x = (const C*)S.vec[in_id];
   C* __restrict__ t1 = (C*)S.t1;
+  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
+  const int t = rest % SH::T, l = rest / SH::T;
   const long long nlines = (long long)g.nx * g.ny;
-  const long long line0 = (long long)blockIdx.x * NL;
-  for (int idx = threadIdx.x; idx < NL * g.nz; idx += NT) {
-    const int l = idx / g.nz, iz = idx - l * g.nz;
-    const long long line = line0 + l;
-    C v0 = czero<C>(), v1 = v0, v2 = v0;
-    if (line < nlines) {
-      const C* p = x + (line * g.nz + iz) * 3;
-      v0 = p[0]; v1 = p[1]; v2 = p[2];
-    }
-    C* q = s + l * LS + iz * 3;
-    q[0] = v0; q[1] = v1; q[2] = v2;
-  }
-  const int zc = 3 * (LZ - g.nz);
-  for (int idx = threadIdx.x; idx < NL * zc; idx += NT) {
-    const int l = idx / zc, r = idx - l * zc;
-    s[l * LS + 3 * g.nz + r] = czero<C>();
-  }
-  __syncthreads();
-  LayLine<3> lay{NL, LS};
-  fft_tile<LZ, false, KP<R>::EPT, NT>(s, lay, tw);
-  for (int idx = threadIdx.x; idx < NL * LS; idx += NT) {
-    const int l = idx / LS, r = idx - l * LS;
-    const long long line = line0 + l;
-    if (line < nlines) t1[line * LS + r] = s[l * LS + r];
-  }
+  const long long line = (long long)blockIdx.x * nl + l;
+  const bool ok = line < nlines;
+  const int nz = g.nz;
+  const C* xl = x + line * nz * 3 + c;
+  C* tl = t1 + line * (long long)LZ * 3 + c;
+  C* sl = s + l * 3 * SH::LP + c;
+  auto ld = [&](int, int pos) -> C { return (ok && pos < nz) ? xl[pos * 3] : czero<C>(); };
+  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
+  auto stf = [&](int, int pos, C v) { if (ok) tl[pos * 3] = v; };
+  C a[P::E];
+  rfft<P, 1, false>(a, t, ld, sm, stf, tw);
 }
 
 // ---------------------------------------------------------------------------
-// pass 2 / 4: y transforms on a (ix, kz-tile) slab.  INV=false: T1 -> T2 with
-// rows y >= ny zero; INV=true: T2 -> T1 keeping rows y < ny.
+// pass 2 / 4: y transforms on a (ix, kz-tile) slab, W = 3 tz transforms;
+// thread = (w fastest, t).  INV=false: T1 -> T2 (rows y >= ny are zero);
+// INV=true: T2 -> T1 keeping rows y < ny.
 // ---------------------------------------------------------------------------
 template <typename R, bool INV, int LY>
-__global__ void __launch_bounds__(KP<R>::NT) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                         InstState* st, const int* act, int cond, int Tz, int ntz) {
+__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                             InstState* st, const int* act, int cond, int tz,
+                                                             int ntz) {
   typedef typename CT<R>::T C;
-  constexpr int NT = KP<R>::NT;
+  typedef MvShape<R, LY> SH;
+  typedef typename SH::P P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t1 = (C*)S.t1;
   C* __restrict__ t2 = (C*)S.t2;
+  const int W = 3 * tz;
+  const int w = threadIdx.x % W, t = threadIdx.x / W;
   const int ix = blockIdx.x / ntz, kzt = blockIdx.x - ix * ntz;
-  const int kz0 = kzt * Tz;
-  const int tzn = min(Tz, g.Lz - kz0);
-  const int W = 3 * Tz, Wv = 3 * tzn;
-  const int rows_in = INV ? LY : g.ny;
-  const C* __restrict__ src = INV ? t2 : t1;
-  const long long src_row0 = INV ? (long long)ix * LY : (long long)ix * g.ny;
-  for (int idx = threadIdx.x; idx < rows_in * W; idx += NT) {
-    const int r = idx / W, w = idx - r * W;
-    C v = czero<C>();
-    if (w < Wv) v = src[((src_row0 + r) * g.Lz + kz0) * 3 + w];
-    s[r * W + w] = v;
-  }
-  if (!INV) {
-    for (int idx = threadIdx.x; idx < (LY - g.ny) * W; idx += NT) s[g.ny * W + idx] = czero<C>();
-  }
-  __syncthreads();
-  LayCol lay{W, W};
-  fft_tile<LY, INV, KP<R>::EPT, NT>(s, lay, tw);
-  const int rows_out = INV ? g.ny : LY;
-  C* __restrict__ dst = INV ? t1 : t2;
-  const long long dst_row0 = INV ? (long long)ix * g.ny : (long long)ix * LY;
-  for (int idx = threadIdx.x; idx < rows_out * Wv; idx += NT) {
-    const int r = idx / Wv, w = idx - r * Wv;
-    dst[((dst_row0 + r) * g.Lz + kz0) * 3 + w] = s[r * W + w];
-  }
+  const int kz0 = kzt * tz;
+  const bool ok = w < 3 * min(tz, g.Lz - kz0);
+  const int ny = g.ny;
+  const long long rs = (long long)g.Lz * 3;                 // row stride of T1/T2
+  const C* src = (INV ? t2 + (long long)ix * LY * rs : t1 + (long long)ix * ny * rs) + kz0 * 3 + w;
+  C* dst = (INV ? t1 + (long long)ix * ny * rs : t2 + (long long)ix * LY * rs) + kz0 * 3 + w;
+  C* sw = s + w;
+  auto ld = [&](int, int pos) -> C { return (ok && (INV || pos < ny)) ? src[pos * rs] : czero<C>(); };
+  auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
+  auto stf = [&](int, int pos, C v) { if (ok && (!INV || pos < ny)) dst[pos * rs] = v; };
+  C a[P::E];
+  rfft<P, 1, INV>(a, t, ld, sm, stf, tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -118,72 +121,161 @@ __global__ void __launch_bounds__(KP<R>::NT) k_mv_pass_y(Geo g, const typename C
 // mirrored octant, inverse x-FFT, keep rows x < nx (in place in T2).
 // Mirror rule (Gpbicgstab.py:192-211): an index i > L/2 maps to L - i, and the
 // xy / xz / yz entries change sign when exactly one index of the pair is
-// mirrored.
+// mirrored.  The pencil row order 0, 1, Ly-1, 2, Ly-2, ... keeps mirrored
+// pencils (which read the same octant rows) adjacent in time so the second
+// read hits L2.
 // ---------------------------------------------------------------------------
-template <typename R, int LX>
-__global__ void __launch_bounds__(KP<R>::NT) k_mv_pass3(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                        InstState* st, const int* act, int cond, int Tz, int ntz,
-                                                        R gscale) {
+template <class C, typename R>
+__device__ __forceinline__ void tensor3(const C* __restrict__ gh, const Geo& g, int LX, int kx, int my, bool fy,
+                                        int kz, R gscale, C& a, C& b, C& c) {
+  const bool fx = kx > LX / 2, fz = kz > g.Lz / 2;
+  const int mx = fx ? LX - kx : kx;
+  const int mz = fz ? g.Lz - kz : kz;
+  const C* q = gh + (((long long)mx * g.hy + my) * g.hz + mz) * 6;
+  C gxx = q[0], gxy = q[1], gxz = q[2], gyy = q[3], gyz = q[4], gzz = q[5];
+  const R sxy = (fx != fy) ? -gscale : gscale;
+  const R sxz = (fx != fz) ? -gscale : gscale;
+  const R syz = (fy != fz) ? -gscale : gscale;
+  gxx = cscale(gxx, gscale); gyy = cscale(gyy, gscale); gzz = cscale(gzz, gscale);
+  gxy = cscale(gxy, sxy); gxz = cscale(gxz, sxz); gyz = cscale(gyz, syz);
+  const C a0 = a, b0 = b, c0 = c;
+  a = cadd(cadd(cmul(gxx, a0), cmul(gxy, b0)), cmul(gxz, c0));
+  b = cadd(cadd(cmul(gxy, a0), cmul(gyy, b0)), cmul(gyz, c0));
+  c = cadd(cadd(cmul(gxz, a0), cmul(gyz, b0)), cmul(gzz, c0));
+}
+
+__device__ __forceinline__ int pencil_ky(int p, int Ly) {
+  if (p == 0) return 0;
+  const int pr = (p + 1) >> 1;
+  return (p & 1) ? pr : Ly - pr;
+}
+
+// variant with the three components of a pencil in one thread:
+// thread = (kzl fastest, t)
+template <typename R, int LX, int V>
+__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                             InstState* st, const int* act, int cond, int tz,
+                                                             int ntz, R gscale) {
   typedef typename CT<R>::T C;
-  constexpr int NT = KP<R>::NT;
+  typedef P3Shape<R, LX, V> SH;
+  typedef typename SH::P P;
+  typedef RevPlan<P> Q;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t2 = (C*)S.t2;
   const C* __restrict__ gh = (const C*)S.ghat;
-  // pencil order 0, 1, Ly-1, 2, Ly-2, ... keeps mirrored pencils (which read
-  // the same octant rows) adjacent in time so the second read hits L2
+  const int kzl = threadIdx.x % tz, t = threadIdx.x / tz;
   const int p = blockIdx.x / ntz, kzt = blockIdx.x - p * ntz;
-  int ky;
-  if (p == 0) ky = 0;
-  else { const int pr = (p + 1) >> 1; ky = (p & 1) ? pr : g.Ly - pr; }
-  const int kz0 = kzt * Tz;
-  const int tzn = min(Tz, g.Lz - kz0);
-  const int W = 3 * Tz, Wv = 3 * tzn;
-  const long long rstride = (long long)g.Ly * g.Lz * 3;   // between x rows
-  const long long base = ((long long)ky * g.Lz + kz0) * 3;
-  for (int idx = threadIdx.x; idx < g.nx * W; idx += NT) {
-    const int r = idx / W, w = idx - r * W;
-    C v = czero<C>();
-    if (w < Wv) v = t2[r * rstride + base + w];
-    s[r * W + w] = v;
-  }
-  for (int idx = threadIdx.x; idx < (LX - g.nx) * W; idx += NT) s[g.nx * W + idx] = czero<C>();
-  __syncthreads();
-  LayCol lay{W, W};
-  fft_tile<LX, false, KP<R>::EPT, NT>(s, lay, tw);
+  const int ky = pencil_ky(p, g.Ly);
+  const int kz0 = kzt * tz;
+  const int kz = kz0 + kzl;
+  const bool ok = kz < g.Lz;
+  const int nx = g.nx;
+  const long long rs = (long long)g.Ly * g.Lz * 3;          // x-row stride of T2
+  C* col = t2 + ((long long)ky * g.Lz + kz) * 3;
+  const int W = 3 * tz;
+  C* sw = s + 3 * kzl;
+  auto ld = [&](int c, int pos) -> C { return (ok && pos < nx) ? col[pos * rs + c] : czero<C>(); };
+  auto sm = [&](int c, int pp) -> C& { return sw[pp * W + c]; };
+  C a[3 * P::E];
+  rload<P, 3>(a, t, ld);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rstage<P, 0, false>(a + c * P::E, t, tw);
+  rrest<P, 3, 0, false>(a, t, sm, tw);
+  // tensor product at the positions this thread owns after the last stage
+  constexpr int RL = P::r[P::S - 1];
   const bool fy = ky > g.Ly / 2;
   const int my = fy ? g.Ly - ky : ky;
-  for (int idx = threadIdx.x; idx < LX * tzn; idx += NT) {
+  if (ok) {
+#pragma unroll
+    for (int b = 0; b < P::E / RL; ++b)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) {
+        const int i = b * RL + q;
+        tensor3(gh, g, LX, rout_pos<P, P::S - 1>(t, b, q), my, fy, kz, gscale, a[i], a[P::E + i], a[2 * P::E + i]);
+      }
+  }
+  // inverse transform with the reversed plan: its stage 0 owns the same positions
+  const int ti = opaque(t);
+  C* colo = opaque_ptr(col);
+  auto stf = [&](int c, int pos, C v) { if (ok && pos < nx) colo[pos * rs + c] = v; };
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rstage<Q, 0, true>(a + c * P::E, ti, tw);
+  rrest<Q, 3, 0, true>(a, ti, sm, tw);
+  rstore<Q, 3>(a, ti, stf);
+}
+
+// variant with one component per thread and the tensor product through
+// shared memory (bounded registers for complex128): thread = (w fastest, t)
+template <typename R, int LX, int V>
+__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                             InstState* st, const int* act, int cond, int tz,
+                                                             int ntz, R gscale) {
+  typedef typename CT<R>::T C;
+  typedef P3Shape<R, LX, V> SH;
+  typedef typename SH::P P;
+  typedef RevPlan<P> Q;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  C* __restrict__ t2 = (C*)S.t2;
+  const C* __restrict__ gh = (const C*)S.ghat;
+  const int W = 3 * tz;
+  const int w = threadIdx.x % W, t = threadIdx.x / W;
+  const int p = blockIdx.x / ntz, kzt = blockIdx.x - p * ntz;
+  const int ky = pencil_ky(p, g.Ly);
+  const int kz0 = kzt * tz;
+  const int tzn = min(tz, g.Lz - kz0);
+  const bool ok = w < 3 * tzn;
+  const int nx = g.nx;
+  const long long rs = (long long)g.Ly * g.Lz * 3;
+  C* col = t2 + ((long long)ky * g.Lz + kz0) * 3 + w;
+  C* sw = s + w;
+  auto ld = [&](int, int pos) -> C { return (ok && pos < nx) ? col[pos * rs] : czero<C>(); };
+  auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
+  C a[P::E];
+  rload<P, 1>(a, t, ld);
+  rstage<P, 0, false>(a, t, tw);
+  rrest<P, 1, 0, false>(a, t, sm, tw);
+  constexpr int RL = P::r[P::S - 1];
+#pragma unroll
+  for (int b = 0; b < P::E / RL; ++b)
+#pragma unroll
+    for (int q = 0; q < RL; ++q) sm(0, ppad(rout_pos<P, P::S - 1>(t, b, q))) = a[b * RL + q];
+  __syncthreads();
+  const bool fy = ky > g.Ly / 2;
+  const int my = fy ? g.Ly - ky : ky;
+  for (int idx = threadIdx.x; idx < LX * tzn; idx += blockDim.x) {
     const int kx = idx / tzn, kzl = idx - kx * tzn;
-    const int kz = kz0 + kzl;
-    const bool fx = kx > LX / 2, fz = kz > g.Lz / 2;
-    const int mx = fx ? LX - kx : kx;
-    const int mz = fz ? g.Lz - kz : kz;
-    const C* q = gh + (((long long)mx * g.hy + my) * g.hz + mz) * 6;
-    C gxx = q[0], gxy = q[1], gxz = q[2], gyy = q[3], gyz = q[4], gzz = q[5];
-    const R sxy = (fx != fy) ? -gscale : gscale;
-    const R sxz = (fx != fz) ? -gscale : gscale;
-    const R syz = (fy != fz) ? -gscale : gscale;
-    gxx = cscale(gxx, gscale); gyy = cscale(gyy, gscale); gzz = cscale(gzz, gscale);
-    gxy = cscale(gxy, sxy); gxz = cscale(gxz, sxz); gyz = cscale(gyz, syz);
-    C* v = s + kx * W + 3 * kzl;
-    const C a = v[0], b = v[1], c = v[2];
-    v[0] = cadd(cadd(cmul(gxx, a), cmul(gxy, b)), cmul(gxz, c));
-    v[1] = cadd(cadd(cmul(gxy, a), cmul(gyy, b)), cmul(gyz, c));
-    v[2] = cadd(cadd(cmul(gxz, a), cmul(gyz, b)), cmul(gzz, c));
+    C* v = s + ppad(kx) * W + 3 * kzl;
+    C a0 = v[0], a1 = v[1], a2 = v[2];
+    tensor3(gh, g, LX, kx, my, fy, kz0 + kzl, gscale, a0, a1, a2);
+    v[0] = a0; v[1] = a1; v[2] = a2;
   }
   __syncthreads();
-  fft_tile<LX, true, KP<R>::EPT, NT>(s, lay, tw);
-  for (int idx = threadIdx.x; idx < g.nx * Wv; idx += NT) {
-    const int r = idx / Wv, w = idx - r * Wv;
-    t2[r * rstride + base + w] = s[r * W + w];
-  }
+  // inverse half: fresh copies of the index and pointers keep the compiler
+  // from carrying the forward half's address arithmetic across the kernel
+  const int ti = opaque(t);
+  C* colo = opaque_ptr(col);
+  C* swo = opaque_ptr(sw);
+  auto smo = [&](int, int pp) -> C& { return swo[pp * W]; };
+  auto stf = [&](int, int pos, C v) { if (ok && pos < nx) colo[pos * rs] = v; };
+  constexpr int R0 = Q::r[0];
+#pragma unroll
+  for (int b = 0; b < Q::E / R0; ++b)
+#pragma unroll
+    for (int m = 0; m < R0; ++m) a[b * R0 + m] = smo(0, ppad(rin_pos<Q, 0>(ti, b, m)));
+  __syncthreads();
+  rstage<Q, 0, true>(a, ti, tw);
+  rrest<Q, 1, 0, true>(a, ti, smo, tw);
+  rstore<Q, 1>(a, ti, stf);
 }
 
 // ---------------------------------------------------------------------------
-// pass 5: inverse z on NL lines, keep z < nz, fused combine:
+// pass 5: inverse z on nl lines, keep z < nz, fused combine:
 //   MV_AX           y = ia*x - mask*conv        (interaction_mult)
 //   MV_RESIDUAL     y = b - (ia*x - mask*conv)  (b already masked)
 //   MV_CONV         y = conv                    (E_field_solver)
@@ -191,57 +283,51 @@ __global__ void __launch_bounds__(KP<R>::NT) k_mv_pass3(Geo g, const typename CT
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
 // ---------------------------------------------------------------------------
 template <typename R, int LZ>
-__global__ void __launch_bounds__(KP<R>::NT) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                        InstState* st, const int* act, int in_id, int out_id,
-                                                        int mode, int cond, int NL) {
+__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                            InstState* st, const int* act, int in_id, int out_id,
+                                                            int mode, int cond, int nl) {
   typedef typename CT<R>::T C;
-  constexpr int NT = KP<R>::NT;
-  constexpr int LS = 3 * LZ;
+  typedef MvShape<R, LZ> SH;
+  typedef typename SH::P P;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   const C* __restrict__ t1 = (const C*)S.t1;
+  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
+  const int t = rest % SH::T, l = rest / SH::T;
   const long long nlines = (long long)g.nx * g.ny;
-  const long long line0 = (long long)blockIdx.x * NL;
-  for (int idx = threadIdx.x; idx < NL * LS; idx += NT) {
-    const int l = idx / LS, r = idx - l * LS;
-    const long long line = line0 + l;
-    s[l * LS + r] = (line < nlines) ? t1[line * LS + r] : czero<C>();
-  }
+  const long long line = (long long)blockIdx.x * nl + l;
+  const bool ok = line < nlines;
+  const int nz = g.nz;
+  const C* tl = t1 + line * (long long)LZ * 3 + c;
+  C* sl = s + l * 3 * SH::LP + c;
+  auto ld = [&](int, int pos) -> C { return ok ? tl[pos * 3] : czero<C>(); };
+  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
+  auto stf = [&](int, int pos, C v) { if (pos < nz) sl[ppad(pos) * 3] = v; };
+  C a[P::E];
+  rfft<P, 1, true>(a, t, ld, sm, stf, tw);
   __syncthreads();
-  LayLine<3> lay{NL, LS};
-  fft_tile<LZ, true, KP<R>::EPT, NT>(s, lay, tw);
-  const C* __restrict__ x = (const C*)S.vec[in_id];
-  C* __restrict__ y = (C*)S.vec[out_id];
-  const C* __restrict__ ia = (const C*)S.inva;
-  const C* __restrict__ b = (const C*)S.vec[V_B];
-  for (int idx = threadIdx.x; idx < NL * g.nz; idx += NT) {
-    const int l = idx / g.nz, iz = idx - l * g.nz;
-    const long long line = line0 + l;
-    if (line >= nlines) continue;
-    const long long site = line * g.nz + iz;
-    const C* q = s + l * LS + iz * 3;
-    C c0 = q[0], c1 = q[1], c2 = q[2];
-    C* yo = y + site * 3;
-    if (mode == MV_CONV) {
-      yo[0] = c0; yo[1] = c1; yo[2] = c2;
-      continue;
-    }
-    const C a = ia[site];
-    const bool m = (a.x != (R)0) || (a.y != (R)0);
-    if (!m) { c0 = c1 = c2 = czero<C>(); }
-    if (mode == MV_CONV_MASKED) {
-      yo[0] = c0; yo[1] = c1; yo[2] = c2;
-      continue;
-    }
-    const C* xi = x + site * 3;
-    C r0 = csub(cmul(a, xi[0]), c0), r1 = csub(cmul(a, xi[1]), c1), r2 = csub(cmul(a, xi[2]), c2);
-    if (mode == MV_RESIDUAL) {
-      const C* bi = b + site * 3;
-      r0 = csub(bi[0], r0); r1 = csub(bi[1], r1); r2 = csub(bi[2], r2);
-    }
-    yo[0] = r0; yo[1] = r1; yo[2] = r2;
+  // combine: consecutive threads take consecutive (site, component)
+  const long long site_base = (long long)blockIdx.x * nl * nz;
+  const int nv = (int)min((long long)nl, nlines - (long long)blockIdx.x * nl) * nz * 3;
+  const C* __restrict__ xg = (const C*)S.vec[in_id] + site_base * 3;
+  C* __restrict__ yg = (C*)S.vec[out_id] + site_base * 3;
+  const C* __restrict__ iag = (const C*)S.inva + site_base;
+  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site_base * 3 : nullptr;
+#pragma unroll 4
+  for (int idx = threadIdx.x; idx < nv; idx += blockDim.x) {
+    const int cc = idx % 3, sidx = idx / 3;
+    const int ll = sidx / nz, pos = sidx - ll * nz;
+    C v = s[ll * 3 * SH::LP + ppad(pos) * 3 + cc];
+    if (mode == MV_CONV) { yg[idx] = v; continue; }
+    const C a_ = iag[sidx];
+    const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
+    if (!msk) v = czero<C>();
+    if (mode == MV_CONV_MASKED) { yg[idx] = v; continue; }
+    C r = csub(cmul(a_, xg[idx]), v);
+    if (mode == MV_RESIDUAL) r = csub(bg[idx], r);
+    yg[idx] = r;
   }
 }
 
@@ -270,9 +356,12 @@ template <typename R> struct MvKernels {
     }
     return nullptr;
   }
-  static P3 p3(int L) {
+  static P3 p3(int L, int v) {
     switch (L) {
-#define DDA_K(n) case n: return k_mv_pass3<R, n>;
+#define DDA_K(n)                                                           \
+  case n:                                                                  \
+    return v == 1 ? (P3)k_mv_pass3r<R, n, 1>                               \
+                  : (v == 2 ? (P3)k_mv_pass3s<R, n, 2> : (P3)k_mv_pass3s<R, n, 0>);
       DDA_FFT_SIZES(DDA_K)
 #undef DDA_K
     }
@@ -293,10 +382,9 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
                                int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
   typedef typename CT<R>::T C;
   constexpr bool dbl = sizeof(R) == 8;
-  constexpr int NT = KP<R>::NT;
   auto k1 = MvKernels<R>::p1(g.Lz);
   auto k2 = MvKernels<R>::py(g.Ly, false);
-  auto k3 = MvKernels<R>::p3(g.Lx);
+  auto k3 = MvKernels<R>::p3(g.Lx, pc.p3var);
   auto k4 = MvKernels<R>::py(g.Ly, true);
   auto k5 = MvKernels<R>::p5(g.Lz);
   if (!k1 || !k2 || !k3 || !k4 || !k5) return cudaErrorInvalidValue;
@@ -306,18 +394,88 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
   if (!twx || !twy || !twz) return cudaErrorMemoryAllocation;
   const int mx = 200 * 1024;
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute((const void*)k1, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-  if ((e = cudaFuncSetAttribute((const void*)k2, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-  if ((e = cudaFuncSetAttribute((const void*)k3, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-  if ((e = cudaFuncSetAttribute((const void*)k4, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-  if ((e = cudaFuncSetAttribute((const void*)k5, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-  k1<<<dim3((unsigned)pc.grid1, nb), NT, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.NL);
-  k2<<<dim3((unsigned)pc.grid2, nb), NT, pc.smem2, s>>>(g, twy, st, act, cond, pc.Tz2, pc.ntz2);
-  k3<<<dim3((unsigned)pc.grid3, nb), NT, pc.smem3, s>>>(g, twx, st, act, cond, pc.Tz3, pc.ntz3, (R)gscale);
-  k4<<<dim3((unsigned)pc.grid2, nb), NT, pc.smem2, s>>>(g, twy, st, act, cond, pc.Tz2, pc.ntz2);
-  k5<<<dim3((unsigned)pc.grid1, nb), NT, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.NL);
+  const void* ks[5] = {(const void*)k1, (const void*)k2, (const void*)k3, (const void*)k4, (const void*)k5};
+  for (int i = 0; i < 5; ++i) {
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
+  }
+  k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl);
+  k2<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
+  k3<<<dim3((unsigned)pc.grid3, nb), pc.th3, pc.smem3, s>>>(g, twx, st, act, cond, pc.tz3, pc.ntz3, (R)gscale);
+  k4<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
+  k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl);
   note_launch(s, 5);
   return cudaGetLastError();
+}
+
+// Tile shapes: about 128 (complex64) or 64 (complex128) transforms' worth of
+// threads per CTA, at most one tile dimension's extent.
+template <typename R>
+static int lanes() { return sizeof(R) == 4 ? 128 : 64; }
+
+template <typename R>
+static bool tile_dims(int L, int& T, int& LP) {
+  switch (L) {
+#define DDA_K(n) case n: T = MvShape<R, n>::T; LP = MvShape<R, n>::LP; return true;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+  }
+  return false;
+}
+
+template <typename R>
+static bool tile_dims3(int L, int v, int& T, int& LP) {
+  switch (L) {
+#define DDA_K(n)                                                                      \
+  case n:                                                                             \
+    if (v == 0) { T = P3Shape<R, n, 0>::T; LP = P3Shape<R, n, 0>::LP; }               \
+    else { T = P3Shape<R, n, 1>::T; LP = P3Shape<R, n, 1>::LP; }                      \
+    return true;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+  }
+  return false;
+}
+
+// Pass-3 variant: DDA_P3_VARIANT overrides; default 0 for complex64 and 2
+// for complex128 (both one component per thread, coalesced columns).
+template <typename R>
+static int p3_variant() {
+  const char* e = getenv("DDA_P3_VARIANT");
+  if (e && *e >= '0' && *e < '0' + kP3Variants) return *e - '0';
+  return sizeof(R) == 4 ? 0 : 2;
+}
+
+template <typename R>
+PassCfg make_pass_cfg_impl(const Geo& g) {
+  PassCfg c{};
+  const size_t esz = sizeof(R) * 2;
+  int T, LP;
+  const int LN = lanes<R>();
+  // z passes: nl lines x 3 components, 3*T threads per line
+  tile_dims<R>(g.Lz, T, LP);
+  const long long nlines = (long long)g.nx * g.ny;
+  c.nl = (int)std::min<long long>(std::max(1, LN / T), nlines);
+  c.th1 = 3 * T * c.nl;
+  c.smem1 = (size_t)c.nl * 3 * LP * esz;
+  c.grid1 = (nlines + c.nl - 1) / c.nl;
+  // y passes: tz kz columns, 3*tz transforms of T threads
+  tile_dims<R>(g.Ly, T, LP);
+  c.tz2 = std::min(std::max(1, LN / T), g.Lz);
+  c.th2 = 3 * c.tz2 * T;
+  c.smem2 = (size_t)3 * c.tz2 * LP * esz;
+  c.ntz2 = (g.Lz + c.tz2 - 1) / c.tz2;
+  c.grid2 = (long long)g.nx * c.ntz2;
+  // x pass
+  c.p3var = p3_variant<R>();
+  tile_dims3<R>(g.Lx, c.p3var, T, LP);
+  c.p3reg = c.p3var == 1;
+  c.tz3 = std::min(std::max(1, LN / T), g.Lz);
+  c.th3 = (c.p3reg ? 1 : 3) * c.tz3 * T;
+  c.smem3 = (size_t)3 * c.tz3 * LP * esz;
+  c.ntz3 = (g.Lz + c.tz3 - 1) / c.tz3;
+  c.grid3 = (long long)g.Ly * c.ntz3;
+  return c;
 }
 
 }  // namespace dda

@@ -65,6 +65,20 @@ def test_matvec_matches_oracle(shape, dtype, tol):
     assert _rel(r, b * mask[..., None] - ref) < tol
 
 
+@pytest.mark.parametrize("variant", ["0", "1", "2"])
+@pytest.mark.parametrize("shape", [(8, 8, 8), (6, 10, 12), (16, 12, 32), (32, 32, 32)])
+@pytest.mark.parametrize("dtype,tol", [(C128, 1e-12), (C64, 2e-5)])
+def test_matvec_pass3_variants(variant, shape, dtype, tol, monkeypatch):
+    P = _pkg()
+    monkeypatch.setenv("DDA_P3_VARIANT", variant)
+    k, d, alpha, x = _rand_problem(shape, seed=7)
+    ia, mask, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=dtype)
+    Gref = O.generate_interaction_row(*shape, k, d, L=op.L)
+    ref = O.interaction_mult(x, Gref, ia, mask, L=op.L)
+    assert _rel(op.matvec(x).cpu().numpy(), ref) < tol
+
+
 def test_matvec_dense_tiny():
     P = _pkg()
     k, d, alpha, x = _rand_problem((4, 4, 4), seed=3)
