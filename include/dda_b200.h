@@ -15,10 +15,14 @@
  *       (Gpbicgstab.py:937, :1172);
  *   inverse polarisability inv_alpha: (nx, ny, nz) complex, 0 outside the
  *       scatterer; the mask is inv_alpha != 0 (ddaforgit.py:1105-1108);
- *   FFT'd interaction tensor ghat: reduced octant (Lx/2+1, Ly/2+1, Lz/2+1, 6)
- *       of FFT(-G), components (xx, xy, xz, yy, yz, zz) fastest
- *       (ddaforgit.py:1069-1077).  With Ln = 2 nn this is exactly the
- *       reference's (nx+1, ny+1, nz+1, 6) array.
+ *   FFT'd interaction tensor ghat: reduced octant (hx, hy, hz) = (Lx/2+1,
+ *       Ly/2+1, Lz/2+1) of FFT(-G), components (xx, xy, xz, yy, yz, zz), in
+ *       one of two layouts:
+ *         DDA_GHAT_REFERENCE  (hx, hy, hz, 6), component fastest -- with
+ *             Ln = 2 nn exactly the reference's (nx+1, ny+1, nz+1, 6) array
+ *             (ddaforgit.py:1069-1077);
+ *         DDA_GHAT_ENGINE     (6, hx, hy, hz), the layout every solver and
+ *             matvec entry point reads (coalesced tensor gathers).
  * dtype: DDA_C64 = complex64 (float2), DDA_C128 = complex128 (double2).
  */
 #ifndef DDA_B200_H
@@ -41,6 +45,10 @@ extern "C" {
 #define DDA_ERR_CUDA 6
 #define DDA_ERR_ARG 7
 
+/* octant layouts */
+#define DDA_GHAT_REFERENCE 0
+#define DDA_GHAT_ENGINE 1
+
 /* matvec modes of dda_matvec */
 #define DDA_MV_AX 0            /* y = inv_alpha*x - mask*conv(x)          */
 #define DDA_MV_RESIDUAL 1      /* y = b - A.x  (b already masked)          */
@@ -55,7 +63,7 @@ typedef struct dda_op dda_op;
  * shared between instances (many incidences of one geometry) or not (many
  * geometries padded into one size bucket). */
 typedef struct dda_instance {
-  const void* ghat;        /* octant, dtype of the solve                  */
+  const void* ghat;        /* octant, engine layout, dtype of the solve   */
   const void* inv_alpha;   /* (nx,ny,nz) complex, dtype of the solve      */
   const void* e_inc;       /* (nx,ny,nz,3) complex, dtype of the solve    */
   void* p_out;             /* (nx,ny,nz,3) complex, dtype of the solve    */
@@ -90,13 +98,18 @@ int dda_fft_length_ok(int L, int dtype);
 
 /* Replaces generate_interaction_row (ddaforgit.py:1046-1080): builds
  * scale * FFT(-G) on the (Lx,Ly,Lz) embedding of the (nx,ny,nz) box, cropped
- * to the octant.  scale = 1 gives the reference's array.  Writes complex128 to
- * out_c128 and/or complex64 to out_c64 (either may be NULL). */
+ * to the octant, in the given layout.  scale = 1 with DDA_GHAT_REFERENCE gives
+ * the reference's array.  Writes complex128 to out_c128 and/or complex64 to
+ * out_c64 (either may be NULL).  Computed in FP64. */
 int dda_green_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d,
-                    double scale, void* out_c128, void* out_c64, void* stream);
+                    double scale, int layout, void* out_c128, void* out_c64, void* stream);
 
-/* Operator A for one geometry: references caller-owned ghat (octant with the
- * given scale, i.e. the kernel multiplies by gscale) and inv_alpha; owns the
+/* Reference-layout octant -> engine layout (same dtype, src != dst). */
+int dda_ghat_to_engine(dda_ctx* ctx, int dtype, int hx, int hy, int hz, const void* src, void* dst,
+                       void* stream);
+
+/* Operator A for one geometry: references caller-owned ghat (engine layout,
+ * multiplied by gscale inside the kernels) and inv_alpha; owns the
  * transform scratch.  Replaces the state prepared by prepare_interaction_matrices
  * (ddaforgit.py:1085-1159) and setup_chunked_values (Gpbicgstab.py:832-876). */
 int dda_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* ghat,

@@ -12,7 +12,8 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libdda_b200.so")
+# DDA_LIB_PATH selects an alternative build of the same library (A/B tuning).
+LIB_PATH = os.environ.get("DDA_LIB_PATH") or os.path.join(_HERE, "libdda_b200.so")
 
 DDA_C64 = 0
 DDA_C128 = 1
@@ -26,6 +27,9 @@ DDA_ERR_TIMEOUT = 5
 DDA_ERR_CUDA = 6
 DDA_ERR_ARG = 7
 
+GHAT_REFERENCE = 0
+GHAT_ENGINE = 1
+
 MV_AX = 0
 MV_RESIDUAL = 1
 MV_CONV = 2
@@ -34,7 +38,7 @@ MV_CONV_MASKED = 3
 # every symbol include/dda_b200.h declares
 EXPORTS = (
     "dda_version", "dda_last_error", "dda_kernel_launches", "dda_ctx_create", "dda_ctx_destroy", "dda_ctx_trim",
-    "dda_fft_length_ok", "dda_green_build", "dda_op_create", "dda_op_destroy", "dda_matvec",
+    "dda_fft_length_ok", "dda_green_build", "dda_ghat_to_engine", "dda_op_create", "dda_op_destroy", "dda_matvec",
     "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
 )
 
@@ -70,7 +74,8 @@ def _declare(lib):
     lib.dda_ctx_destroy.restype = None
     lib.dda_ctx_trim.argtypes = [vp]
     lib.dda_fft_length_ok.argtypes = [i, i]
-    lib.dda_green_build.argtypes = [vp, i, i, i, i, i, i, d, d, d, vp, vp, vp]
+    lib.dda_green_build.argtypes = [vp, i, i, i, i, i, i, d, d, d, i, vp, vp, vp]
+    lib.dda_ghat_to_engine.argtypes = [vp, i, i, i, i, vp, vp, vp]
     lib.dda_op_create.argtypes = [vp, i, i, i, i, i, i, i, vp, d, vp, C.POINTER(vp)]
     lib.dda_op_destroy.argtypes = [vp]
     lib.dda_op_destroy.restype = None

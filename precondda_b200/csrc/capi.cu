@@ -118,14 +118,29 @@ int dda_ctx_trim(dda_ctx* ctx) {
 int dda_fft_length_ok(int L, int dtype) { return length_ok(L, dtype) ? 1 : 0; }
 
 int dda_green_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d, double scale,
-                    void* out_c128, void* out_c64, void* stream) {
+                    int layout, void* out_c128, void* out_c64, void* stream) {
   int rc = check_ctx(ctx);
   if (rc) return rc;
   Geo g;
   if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, DDA_C128, &g))) return rc;
   if (!(k > 0) || !(d > 0)) { set_error("k and d must be positive"); return DDA_ERR_ARG; }
   if (!out_c128 && !out_c64) { set_error("no output"); return DDA_ERR_ARG; }
-  return green_build(ctx->c, g, k, d, scale, out_c128, out_c64, (cudaStream_t)stream);
+  if (layout != DDA_GHAT_REFERENCE && layout != DDA_GHAT_ENGINE) { set_error("bad octant layout"); return DDA_ERR_ARG; }
+  return green_build(ctx->c, g, k, d, scale, out_c128, out_c64, layout == DDA_GHAT_ENGINE ? 1 : 0,
+                     (cudaStream_t)stream);
+}
+
+int dda_ghat_to_engine(dda_ctx* ctx, int dtype, int hx, int hy, int hz, const void* src, void* dst, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!src || !dst || src == dst) { set_error("octant conversion needs distinct src and dst"); return DDA_ERR_ARG; }
+  if (hx < 1 || hy < 1 || hz < 1) { set_error("bad octant extents"); return DDA_ERR_BAD_SHAPE; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  if (ghat_to_soa(src, dst, (long long)hx * hy * hz, dtype == DDA_C128, (cudaStream_t)stream)) {
+    set_error("octant conversion launch failed");
+    return DDA_ERR_CUDA;
+  }
+  return DDA_OK;
 }
 
 int dda_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* ghat,

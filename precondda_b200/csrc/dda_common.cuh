@@ -31,6 +31,18 @@ template <class C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return 
 template <class C> __device__ __forceinline__ C cmul_mi(C a) { C c; c.x = a.y; c.y = -a.x; return c; }
 template <class C> __device__ __forceinline__ C czero() { C c; c.x = 0; c.y = 0; return c; }
 
+// complex64 add / subtract / real scale as single packed sm_100 float2
+// instructions (round-to-nearest, bitwise the same results as the two scalar
+// operations they replace); off by default (see DDA_PACKED_F32).
+#ifndef DDA_PACKED_F32
+#define DDA_PACKED_F32 0
+#endif
+#if DDA_PACKED_F32 && defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 1000)
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+#endif
+
 // complex double helpers used by the scalar control logic
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return cmul(a, b); }
 __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {
@@ -79,7 +91,7 @@ enum SolveStatus { ST_RUNNING = 0, ST_CONVERGED = 1, ST_MAXITER = 2, ST_NAN = 3,
 struct InstState {
   // vector table (device pointers, element type given by the batch dtype)
   void* vec[kNumVec];
-  const void* ghat;    // octant of FFT(-G)/(LxLyLz), (hx,hy,hz,6)
+  const void* ghat;    // octant of FFT(-G), engine layout (6,hx,hy,hz)
   const void* inva;    // inverse polarizability per site (N complex)
   void* t1;            // scratch (nx,ny,Lz,3)
   void* t2;            // scratch (nx,Ly,Lz,3)

@@ -132,7 +132,10 @@ void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, 
 
 // Green's tensor build: FFT(-G) octant (hx,hy,hz,6) scaled by `scale`.
 // Writes complex128 to out128 (if non-null) and complex64 to out64 (if non-null).
-int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64,
+// soa = 0: reference layout (hx,hy,hz,6); soa = 1: engine layout (6,hx,hy,hz).
+int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64, int soa,
                 cudaStream_t s);
+// Reference-layout octant -> engine layout (H = hx*hy*hz points).
+int ghat_to_soa(const void* src, void* dst, long long H, bool dbl, cudaStream_t s);
 
 }  // namespace dda

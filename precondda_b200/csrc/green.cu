@@ -87,7 +87,7 @@ template <int AX, int L>
 __global__ void __launch_bounds__(GNT) k_green_col(Geo g, const double2* __restrict__ tw, int Tz, int ntz,
                                                    const double2* __restrict__ src,
                                                    double2* __restrict__ dst128, float2* __restrict__ dst64,
-                                                   double scale) {
+                                                   double scale, int soa) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double2* s = reinterpret_cast<double2*>(smem_raw);
   const int o = blockIdx.x / ntz, kzt = blockIdx.x - o * ntz;   // o = ix (G2) or ky (G3)
@@ -113,7 +113,9 @@ __global__ void __launch_bounds__(GNT) k_green_col(Geo g, const double2* __restr
     if (AX == 1) {
       dst128[(((long long)o * g.hy + r) * g.hz + kz0) * 6 + w] = v;
     } else {
-      const long long off = (((long long)r * g.hy + o) * g.hz + kz0) * 6 + w;
+      // AoS (reference layout): (kx,ky,kz,6); SoA (engine layout): (6,kx,ky,kz)
+      const long long pt = ((long long)r * g.hy + o) * g.hz + kz0 + w / 6;
+      const long long off = soa ? (long long)(w % 6) * g.hx * g.hy * g.hz + pt : pt * 6 + (w % 6);
       const double2 u = make_double2(-scale * v.x, -scale * v.y);
       if (dst128) dst128[off] = u;
       if (dst64) dst64[off] = make_float2((float)u.x, (float)u.y);
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(GNT) k_green_col(Geo g, const double2* __restr
 }
 
 typedef void (*GZ)(Geo, const double2*, double, double, int, double2*);
-typedef void (*GC)(Geo, const double2*, int, int, const double2*, double2*, float2*, double);
+typedef void (*GC)(Geo, const double2*, int, int, const double2*, double2*, float2*, double, int);
 
 static GZ green_z_kernel(int L) {
   switch (L) {
@@ -141,7 +143,25 @@ static GC green_col_kernel(int L, int ax) {
   return nullptr;
 }
 
-int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64,
+// Reference (AoS) octant -> engine (SoA) octant, same precision.
+template <class C>
+__global__ void k_ghat_aos_to_soa(const C* __restrict__ src, C* __restrict__ dst, long long H) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < H * 6; i += (long long)gridDim.x * blockDim.x) {
+    const long long p = i / 6;
+    const int c = (int)(i - p * 6);
+    dst[c * H + p] = src[i];
+  }
+}
+
+int ghat_to_soa(const void* src, void* dst, long long H, bool dbl, cudaStream_t s) {
+  const int blocks = (int)std::min<long long>((H * 6 + 255) / 256, 4096);
+  if (dbl) k_ghat_aos_to_soa<double2><<<blocks, 256, 0, s>>>((const double2*)src, (double2*)dst, H);
+  else k_ghat_aos_to_soa<float2><<<blocks, 256, 0, s>>>((const float2*)src, (float2*)dst, H);
+  note_launch(s, 1);
+  return cudaGetLastError() == cudaSuccess ? 0 : 6;
+}
+
+int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64, int soa,
                 cudaStream_t s) {
   const int cap = GEPT * GNT;
   if (6 * g.Lz > cap || 6 * g.Ly > cap || 6 * g.Lx > cap) {
@@ -175,14 +195,14 @@ int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* 
   if (Tz > g.hz) Tz = g.hz;
   int ntz = (g.hz + Tz - 1) / Tz;
   ky<<<(unsigned)(g.Lx * ntz), GNT, (size_t)g.Ly * 6 * Tz * sizeof(double2), s>>>(g, twy, Tz, ntz, b1, b2, nullptr,
-                                                                                  1.0);
+                                                                                  1.0, 0);
   // G3: x, negate, scale, crop to the octant
   Tz = cap / (6 * g.Lx);
   if (Tz > g.hz) Tz = g.hz;
   ntz = (g.hz + Tz - 1) / Tz;
   kx<<<(unsigned)(g.hy * ntz), GNT, (size_t)g.Lx * 6 * Tz * sizeof(double2), s>>>(g, twx, Tz, ntz, b2,
                                                                                   (double2*)out128, (float2*)out64,
-                                                                                  scale);
+                                                                                  scale, soa);
   note_launch(s, 3);
   e = cudaGetLastError();
   cudaFreeAsync(b1, s);

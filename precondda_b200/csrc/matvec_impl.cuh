@@ -125,14 +125,18 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass_y(Geo g, const typena
 // pencils (which read the same octant rows) adjacent in time so the second
 // read hits L2.
 // ---------------------------------------------------------------------------
+// Ghat is stored structure-of-arrays inside the engine: component c of octant
+// point (mx,my,mz) at gh[c*H + (mx*hy + my)*hz + mz], H = hx*hy*hz, so the
+// lanes of a warp (consecutive kz) read consecutive addresses.
 template <class C, typename R>
 __device__ __forceinline__ void tensor3(const C* __restrict__ gh, const Geo& g, int LX, int kx, int my, bool fy,
                                         int kz, R gscale, C& a, C& b, C& c) {
   const bool fx = kx > LX / 2, fz = kz > g.Lz / 2;
   const int mx = fx ? LX - kx : kx;
   const int mz = fz ? g.Lz - kz : kz;
-  const C* q = gh + (((long long)mx * g.hy + my) * g.hz + mz) * 6;
-  C gxx = q[0], gxy = q[1], gxz = q[2], gyy = q[3], gyz = q[4], gzz = q[5];
+  const long long H = (long long)g.hx * g.hy * g.hz;
+  const C* q = gh + ((long long)mx * g.hy + my) * g.hz + mz;
+  C gxx = q[0], gxy = q[H], gxz = q[2 * H], gyy = q[3 * H], gyz = q[4 * H], gzz = q[5 * H];
   const R sxy = (fx != fy) ? -gscale : gscale;
   const R sxz = (fx != fz) ? -gscale : gscale;
   const R syz = (fy != fz) ? -gscale : gscale;
@@ -248,12 +252,17 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3s(Geo g, const typena
   __syncthreads();
   const bool fy = ky > g.Ly / 2;
   const int my = fy ? g.Ly - ky : ky;
-  for (int idx = threadIdx.x; idx < LX * tzn; idx += blockDim.x) {
-    const int kx = idx / tzn, kzl = idx - kx * tzn;
-    C* v = s + ppad(kx) * W + 3 * kzl;
-    C a0 = v[0], a1 = v[1], a2 = v[2];
-    tensor3(gh, g, LX, kx, my, fy, kz0 + kzl, gscale, a0, a1, a2);
-    v[0] = a0; v[1] = a1; v[2] = a2;
+  {
+    // thread -> (kzl fastest, kx); no division inside the loop
+    const int kzl = threadIdx.x % tz, kxs = blockDim.x / tz;
+    if (kzl < tzn) {
+      for (int kx = threadIdx.x / tz; kx < LX; kx += kxs) {
+        C* v = s + ppad(kx) * W + 3 * kzl;
+        C a0 = v[0], a1 = v[1], a2 = v[2];
+        tensor3(gh, g, LX, kx, my, fy, kz0 + kzl, gscale, a0, a1, a2);
+        v[0] = a0; v[1] = a1; v[2] = a2;
+      }
+    }
   }
   __syncthreads();
   // inverse half: fresh copies of the index and pointers keep the compiler

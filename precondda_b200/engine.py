@@ -83,20 +83,36 @@ def fft_lengths(shape, dtype=_C128, exact=False):
     return tuple(out)
 
 
-def green_octant(shape, k, d, L_=None, scale=1.0, dtype=_C128, device=None) -> torch.Tensor:
-    """scale * FFT(-G) cropped to the (Lx/2+1, Ly/2+1, Lz/2+1, 6) octant,
-    computed in FP64 by the engine (generate_interaction_row,
-    ddaforgit.py:1046-1080)."""
+def green_octant(shape, k, d, L_=None, scale=1.0, dtype=_C128, device=None, layout="reference") -> torch.Tensor:
+    """scale * FFT(-G) on the octant (Lx/2+1, Ly/2+1, Lz/2+1), computed in
+    FP64 by the engine (generate_interaction_row, ddaforgit.py:1046-1080).
+    layout "reference": (hx,hy,hz,6) as the reference stores it;
+    "engine": (6,hx,hy,hz) as the engine's kernels read it."""
     dev = _device(device)
     nx, ny, nz = (int(v) for v in shape)
     Lx, Ly, Lz = L_ if L_ is not None else fft_lengths(shape, _C128, exact=False)
-    out = torch.empty((Lx // 2 + 1, Ly // 2 + 1, Lz // 2 + 1, 6), dtype=dtype, device=dev)
+    h = (Lx // 2 + 1, Ly // 2 + 1, Lz // 2 + 1)
+    eng = layout == "engine"
+    out = torch.empty((6,) + h if eng else h + (6,), dtype=dtype, device=dev)
     ctx = L.context(dev.index)
     with torch.cuda.device(dev):
         p128 = out.data_ptr() if dtype == _C128 else None
         p64 = out.data_ptr() if dtype == _C64 else None
         L.check(L.lib().dda_green_build(ctx.handle, nx, ny, nz, Lx, Ly, Lz, float(k), float(d), float(scale),
-                                        p128, p64, stream_handle(dev)))
+                                        L.GHAT_ENGINE if eng else L.GHAT_REFERENCE, p128, p64,
+                                        stream_handle(dev)))
+    return out
+
+
+def ghat_to_engine(ghat_ref: torch.Tensor) -> torch.Tensor:
+    """(hx,hy,hz,6) reference-layout octant -> (6,hx,hy,hz) engine layout."""
+    dev = ghat_ref.device
+    hx, hy, hz, six = ghat_ref.shape
+    out = torch.empty((6, hx, hy, hz), dtype=ghat_ref.dtype, device=dev)
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_ghat_to_engine(ctx.handle, _dt_code(ghat_ref.dtype), hx, hy, hz,
+                                           ghat_ref.contiguous().data_ptr(), out.data_ptr(), stream_handle(dev)))
     return out
 
 
@@ -148,19 +164,36 @@ class DDAOperator:
         if ghat is not None:
             if L_ is None:
                 L_ = tuple(2 * n for n in self.shape)
-            self.ghat = as_device(ghat, dtype, self.device)
+            g_ref = as_device(ghat, dtype, self.device)
             want = (L_[0] // 2 + 1, L_[1] // 2 + 1, L_[2] // 2 + 1, 6)
-            if tuple(self.ghat.shape) != want:
-                raise ValueError(f"interaction matrix shape {tuple(self.ghat.shape)} != {want}")
+            if tuple(g_ref.shape) != want:
+                raise ValueError(f"interaction matrix shape {tuple(g_ref.shape)} != {want}")
+            self.ghat = ghat_to_engine(g_ref)
             self.gscale = (1.0 / (L_[0] * L_[1] * L_[2])) if ghat_scale is None else float(ghat_scale)
         else:
             if L_ is None:
                 L_ = fft_lengths(self.shape, dtype)
             self.ghat = green_octant(self.shape, self.k, self.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dtype,
-                                     self.device)
+                                     self.device, layout="engine")
             self.gscale = 1.0
         self.L = tuple(int(v) for v in L_)
         self._ctx = L.context(self.device.index)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_op_create(self._ctx.handle, _dt_code(dtype), *self.shape, *self.L,
+                                          self.ghat.data_ptr(), self.gscale, self.inv_alpha.data_ptr(),
+                                          C.byref(h)))
+        self._op = h
+        self._twin = None
+
+    def _init_from_engine_ghat(self, other, dtype):
+        """Precision twin of ``other`` sharing its scale, tensor converted."""
+        self.device, self.dtype, self.k, self.d = other.device, dtype, other.k, other.d
+        self.inv_alpha = other.inv_alpha.to(dtype)
+        self.shape, self.nsite, self.L = other.shape, other.nsite, other.L
+        self.ghat = other.ghat.to(dtype)
+        self.gscale = other.gscale
+        self._ctx = other._ctx
         h = C.c_void_p()
         with torch.cuda.device(self.device):
             L.check(L.lib().dda_op_create(self._ctx.handle, _dt_code(dtype), *self.shape, *self.L,
@@ -223,8 +256,8 @@ class DDAOperator:
             if self.gscale == 1.0:
                 self._twin = DDAOperator(self.inv_alpha, self.k, self.d, dtype, self.L, device=self.device)
             else:
-                self._twin = DDAOperator(self.inv_alpha, self.k, self.d, dtype, self.L,
-                                         ghat=self.ghat.to(dtype), ghat_scale=self.gscale, device=self.device)
+                self._twin = DDAOperator.__new__(DDAOperator)
+                self._twin._init_from_engine_ghat(self, dtype)
         return self._twin
 
     # -- solves ------------------------------------------------------------

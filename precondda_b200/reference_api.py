@@ -28,7 +28,7 @@ def generate_interaction_row(nx, ny, nz, k, lattice_spacing, reduced=True, doubl
     (2nx,2ny,2nz,6) spectrum expanded from it by the mirror rule."""
     dt = _C128 if double_precision else _C64
     Ls = fft_lengths((nx, ny, nz), _C128, exact=True)
-    oct_ = green_octant((nx, ny, nz), k, lattice_spacing, Ls, 1.0, dt)
+    oct_ = green_octant((nx, ny, nz), k, lattice_spacing, Ls, 1.0, dt, layout="reference")
     if reduced:
         return oct_
     return expand_octant(oct_, Ls)
