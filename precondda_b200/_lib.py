@@ -39,7 +39,7 @@ MV_CONV_MASKED = 3
 EXPORTS = (
     "dda_version", "dda_last_error", "dda_kernel_launches", "dda_ctx_create", "dda_ctx_destroy", "dda_ctx_trim",
     "dda_fft_length_ok", "dda_green_build", "dda_ghat_to_engine", "dda_op_create", "dda_op_destroy", "dda_matvec",
-    "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
+    "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
 )
 
 
@@ -80,6 +80,7 @@ def _declare(lib):
     lib.dda_op_destroy.argtypes = [vp]
     lib.dda_op_destroy.restype = None
     lib.dda_matvec.argtypes = [vp, i, vp, vp, vp, vp]
+    lib.dda_matvec_noalloc.argtypes = [i, i, i, i, i, i, i, vp, d, vp, i, vp, vp, vp, vp]
     lib.dda_gpbicgstab.argtypes = [vp, vp, d, i, d, vp, C.POINTER(dda_result), vp]
     lib.dda_solve_batch.argtypes = [vp, i, i, i, i, i, i, i, d, C.POINTER(dda_instance), i, d, i, d,
                                     C.POINTER(dda_result), vp]

@@ -108,6 +108,11 @@ template <typename R>
 cudaError_t launch_matvec(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s);
 
+// One matvec with explicit twiddle tables (allocation-free entry point).
+template <typename R>
+cudaError_t launch_matvec_tw(const Geo& g, const PassCfg& pc, InstState* st, const void* twx, const void* twy,
+                             const void* twz, int in_id, int out_id, int mode, double gscale, cudaStream_t s);
+
 // Batched GPBiCGSTAB kernels (krylov.cu); RB CTAs per instance.
 struct KrylovLaunch {
   InstState* st; const int* act; int nb; double* red; unsigned* cnt; long long n3; int RB;

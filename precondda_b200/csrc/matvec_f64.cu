@@ -7,4 +7,11 @@ cudaError_t launch_matvec<double>(Ctx& ctx, const Geo& g, const PassCfg& pc, Ins
                                  int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
   return launch_matvec_impl<double>(ctx, g, pc, st, act, nb, in_id, out_id, mode, cond, gscale, s);
 }
+template <>
+cudaError_t launch_matvec_tw<double>(const Geo& g, const PassCfg& pc, InstState* st, const void* twx, const void* twy,
+                                   const void* twz, int in_id, int out_id, int mode, double gscale, cudaStream_t s) {
+  typedef typename CT<double>::T C;
+  return launch_matvec_tw_impl<double>(g, pc, st, (const C*)twx, (const C*)twy, (const C*)twz, in_id, out_id, mode,
+                                     gscale, s);
+}
 }  // namespace dda

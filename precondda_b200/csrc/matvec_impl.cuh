@@ -417,6 +417,33 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
   return cudaGetLastError();
 }
 
+// Same five launches with caller-provided twiddle tables (used by the
+// allocation-free entry point, whose tables live in its own static buffer).
+template <typename R>
+cudaError_t launch_matvec_tw_impl(const Geo& g, const PassCfg& pc, InstState* st, const typename CT<R>::T* twx,
+                                  const typename CT<R>::T* twy, const typename CT<R>::T* twz, int in_id,
+                                  int out_id, int mode, double gscale, cudaStream_t s) {
+  auto k1 = MvKernels<R>::p1(g.Lz);
+  auto k2 = MvKernels<R>::py(g.Ly, false);
+  auto k3 = MvKernels<R>::p3(g.Lx, pc.p3var);
+  auto k4 = MvKernels<R>::py(g.Ly, true);
+  auto k5 = MvKernels<R>::p5(g.Lz);
+  if (!k1 || !k2 || !k3 || !k4 || !k5) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const void* ks[5] = {(const void*)k1, (const void*)k2, (const void*)k3, (const void*)k4, (const void*)k5};
+  for (int i = 0; i < 5; ++i) {
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
+  }
+  k1<<<dim3((unsigned)pc.grid1, 1), pc.th1, pc.smem1, s>>>(g, twz, st, nullptr, in_id, C_ALWAYS, pc.nl);
+  k2<<<dim3((unsigned)pc.grid2, 1), pc.th2, pc.smem2, s>>>(g, twy, st, nullptr, C_ALWAYS, pc.tz2, pc.ntz2);
+  k3<<<dim3((unsigned)pc.grid3, 1), pc.th3, pc.smem3, s>>>(g, twx, st, nullptr, C_ALWAYS, pc.tz3, pc.ntz3, (R)gscale);
+  k4<<<dim3((unsigned)pc.grid2, 1), pc.th2, pc.smem2, s>>>(g, twy, st, nullptr, C_ALWAYS, pc.tz2, pc.ntz2);
+  k5<<<dim3((unsigned)pc.grid1, 1), pc.th1, pc.smem1, s>>>(g, twz, st, nullptr, in_id, out_id, mode, C_ALWAYS, pc.nl);
+  note_launch(s, 5);
+  return cudaGetLastError();
+}
+
 // Tile shapes: about 128 (complex64) or 64 (complex128) transforms' worth of
 // threads per CTA, at most one tile dimension's extent.
 template <typename R>
