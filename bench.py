@@ -80,12 +80,20 @@ class ClockSampler:
         self.lines = []
 
     def __enter__(self):
+        return self.start()
+
+    def start(self, wait_s=5.0):
+        """Start sampling and wait (bounded) for the first sample."""
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
                                          stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < wait_s and self.proc.poll() is None:
+                time.sleep(0.05)
+            self.lines.clear()
         except Exception:
             self.proc = None
         return self
@@ -227,7 +235,7 @@ def run_ours(args, ws, rank, local):
 
     dev = torch.device("cuda", local)
     k, d, ia, Es, ndip = problem()
-    op = P.DDAOperator(ia, k, d, dtype=torch.complex128, device=dev)
+    op = P.DDAOperator(ia, k, d, dtype=torch.complex128, device=dev, with_twin=True)
     op64 = op.twin(torch.complex64)
 
     def step():
@@ -272,7 +280,7 @@ def run_ours(args, ws, rank, local):
     for _ in range(args.steps):
         ia_d = ia_h.to(dev, non_blocking=True)
         Ed = [E.to(dev, non_blocking=True) for E in Es_h]
-        op_e = P.DDAOperator(ia_d, k, d, dtype=torch.complex128, L_=op.L, device=dev)
+        op_e = P.DDAOperator(ia_d, k, d, dtype=torch.complex128, L_=op.L, device=dev, with_twin=True)
         Pe, inf_e = P.solve_many([op_e, op_e], Ed, tol=TOL, max_iter=MAX_ITER, ratio=RATIO, precision="mixed",
                                  inner_tol=INNER_TOL)
         xs = [op_e.cross_sections(Pe[j], Ed[j]) for j in range(2)]
@@ -388,7 +396,7 @@ def run_profile_matvec(args, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

@@ -156,27 +156,32 @@ int dda_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int L
   if (!op) { set_error("host allocation failed"); return DDA_ERR_OOM; }
   op->ctx = ctx; op->dtype = dtype; op->g = g; op->gscale = gscale; op->ghat = ghat; op->inva = inv_alpha;
   op->pc = make_pass_cfg(g, dtype == DDA_C128);
-  const size_t esz = dtype == DDA_C128 ? 16 : 8;
-  const size_t t1n = (size_t)g.nx * g.ny * g.Lz * 3, t2n = (size_t)g.nx * g.Ly * g.Lz * 3;
+  // transform scratch is allocated on the first dda_matvec (solves use the
+  // context's workspaces instead)
+  *out = op;
+  return DDA_OK;
+}
+
+static int op_scratch(dda_op* op) {
+  if (op->scratch) return DDA_OK;
+  const size_t esz = op->dtype == DDA_C128 ? 16 : 8;
+  const size_t t1n = (size_t)op->g.nx * op->g.ny * op->g.Lz * 3, t2n = (size_t)op->g.nx * op->g.Ly * op->g.Lz * 3;
   if (cudaMalloc(&op->scratch, (t1n + t2n) * esz) != cudaSuccess ||
       cudaMalloc((void**)&op->d_st, sizeof(InstState)) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(op->scratch);
-    delete op;
+    op->scratch = nullptr;
     set_error("operator scratch: out of device memory");
     return DDA_ERR_OOM;
   }
-  *out = op;
   return DDA_OK;
 }
 
 void dda_op_destroy(dda_op* op) {
   if (!op) return;
   cudaSetDevice(op->ctx->c.device);
-  cudaStreamSynchronize(op->ctx->c.stream);
-  cudaDeviceSynchronize();
-  cudaFree(op->scratch);
-  cudaFree(op->d_st);
+  if (op->scratch) cudaFree(op->scratch);     // cudaFree waits for work using it
+  if (op->d_st) cudaFree(op->d_st);
   delete op;
 }
 
@@ -187,6 +192,7 @@ int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void
   if (!x || !y || (mode == DDA_MV_RESIDUAL && !b)) { set_error("null vector"); return DDA_ERR_ARG; }
   if (mode < 0 || mode > 3) { set_error("bad matvec mode"); return DDA_ERR_ARG; }
   if (x == y) { set_error("x and y must not alias"); return DDA_ERR_ARG; }
+  if ((rc = op_scratch(op))) return rc;
   InstState S;
   std::memset(&S, 0, sizeof(S));
   S.vec[V_R] = (void*)x;

@@ -1,6 +1,7 @@
 // Host side of the engine: FFT plans and twiddles, solver workspaces, the
 // batched GPBiCGSTAB driver (graph-captured iterations, pipelined status
 // polling) and the mixed-precision iterative-refinement driver.
+#include <algorithm>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -317,7 +318,11 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
       w64->base_state(j, H64[j]);
       H64[j].ghat = i64[j].ghat;
       H64[j].inva = i64[j].inv_alpha;
-      H64[j].target = inner_tol;
+      // inner target: inner_tol, relaxed on later sweeps to what the FP64
+      // target still needs (with a safety factor), never above 0.5
+      double tj = inner_tol;
+      if (sweep > 0 && relres[j] > 0) tj = std::max(inner_tol, std::min(0.5, 0.3 * tol / relres[j]));
+      H64[j].target = tj;
       H64[j].ratio = ratio;
       H64[j].max_iter = max_iter;
       H64[j].active = active[j];

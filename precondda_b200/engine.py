@@ -104,6 +104,21 @@ def green_octant(shape, k, d, L_=None, scale=1.0, dtype=_C128, device=None, layo
     return out
 
 
+def green_octant_pair(shape, k, d, L_, scale, device=None):
+    """Engine-layout octant in complex128 and complex64 from one FP64 build."""
+    dev = _device(device)
+    nx, ny, nz = (int(v) for v in shape)
+    Lx, Ly, Lz = L_
+    h = (Lx // 2 + 1, Ly // 2 + 1, Lz // 2 + 1)
+    g128 = torch.empty((6,) + h, dtype=_C128, device=dev)
+    g64 = torch.empty((6,) + h, dtype=_C64, device=dev)
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_green_build(ctx.handle, nx, ny, nz, Lx, Ly, Lz, float(k), float(d), float(scale),
+                                        L.GHAT_ENGINE, g128.data_ptr(), g64.data_ptr(), stream_handle(dev)))
+    return g128, g64
+
+
 def ghat_to_engine(ghat_ref: torch.Tensor) -> torch.Tensor:
     """(hx,hy,hz,6) reference-layout octant -> (6,hx,hy,hz) engine layout."""
     dev = ghat_ref.device
@@ -151,7 +166,8 @@ class DDAOperator:
                 the kernels (default 1/(Lx Ly Lz) for an unscaled FFT(-G)).
     """
 
-    def __init__(self, inv_alpha, k, d, dtype=_C128, L_=None, ghat=None, ghat_scale=None, device=None):
+    def __init__(self, inv_alpha, k, d, dtype=_C128, L_=None, ghat=None, ghat_scale=None, device=None,
+                 with_twin=False):
         self.device = _device(device)
         self.dtype = dtype
         self.k = float(k)
@@ -173,8 +189,15 @@ class DDAOperator:
         else:
             if L_ is None:
                 L_ = fft_lengths(self.shape, dtype)
-            self.ghat = green_octant(self.shape, self.k, self.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dtype,
-                                     self.device, layout="engine")
+            if with_twin:
+                # both precisions from one FP64 Green build
+                g128, g64 = green_octant_pair(self.shape, self.k, self.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]),
+                                              self.device)
+                self.ghat = g128 if dtype == _C128 else g64
+                twin_ghat = g64 if dtype == _C128 else g128
+            else:
+                self.ghat = green_octant(self.shape, self.k, self.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dtype,
+                                         self.device, layout="engine")
             self.gscale = 1.0
         self.L = tuple(int(v) for v in L_)
         self._ctx = L.context(self.device.index)
@@ -185,13 +208,18 @@ class DDAOperator:
                                           C.byref(h)))
         self._op = h
         self._twin = None
+        if ghat is None and with_twin:
+            tw = DDAOperator.__new__(DDAOperator)
+            tw._init_from_engine_ghat(self, _C64 if dtype == _C128 else _C128, twin_ghat)
+            self._twin = tw
 
-    def _init_from_engine_ghat(self, other, dtype):
-        """Precision twin of ``other`` sharing its scale, tensor converted."""
+    def _init_from_engine_ghat(self, other, dtype, ghat=None):
+        """Precision twin of ``other`` sharing its scale; the tensor is
+        ``ghat`` when given (already in ``dtype``), else ``other``'s converted."""
         self.device, self.dtype, self.k, self.d = other.device, dtype, other.k, other.d
         self.inv_alpha = other.inv_alpha.to(dtype)
         self.shape, self.nsite, self.L = other.shape, other.nsite, other.L
-        self.ghat = other.ghat.to(dtype)
+        self.ghat = ghat if ghat is not None else other.ghat.to(dtype)
         self.gscale = other.gscale
         self._ctx = other._ctx
         h = C.c_void_p()
