@@ -164,6 +164,43 @@ int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, 
                           double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
                           void* stream);
 
+/* ---- lattice setup on the device ---------------------------------------- */
+#define DDA_SHAPE_SPHERE 0
+#define DDA_SHAPE_ELLIPSOID 1
+#define DDA_SHAPE_RECTANGLE 2
+#define DDA_SHAPE_CYLINDER 3
+#define DDA_SHAPE_PRISM 4
+
+/* One shape of a voxelisation, in the length unit of d.  p[]: sphere r;
+ * ellipsoid semi-axes (a,b,c); rectangle edge lengths (x,y,z); cylinder
+ * (radius, height); prism (circumradius, height).  axis (0,1,2 = x,y,z) for
+ * cylinder / prism, sides for prism.  rot: ellipsoid body->lab rotation,
+ * row-major (identity for the reference's axis-aligned ellipsoid).
+ * inv_alpha: value written at member sites. */
+typedef struct dda_shape {
+  int type;
+  int axis;
+  int sides;
+  int reserved;
+  double center[3];
+  double p[4];
+  double rot[9];
+  double inv_alpha[2];
+} dda_shape;
+
+/* Replaces mark_shapes / create_alpha_and_n_arrays (ddaforgit.py:615-830)
+ * for a given box: voxelises shapes into inv_alpha (nx,ny,nz) at voxel
+ * centres origin + (i+0.5) d; a site takes the value of the last shape
+ * containing it, 0 if none.  Membership tests as the reference's
+ * (ddaforgit.py:439-572), evaluated on the GPU; shapes is a host array. */
+int dda_voxelize(dda_ctx* ctx, int dtype, const dda_shape* shapes, int nshape, int nx, int ny, int nz, double d,
+                 const double* origin3, void* inv_alpha_out, void* stream);
+
+/* Plane wave E = e exp(i k.r), r = (i,j,k) d, as the reference builds E_inc
+ * (ddaforgit.py:1626-1632); pol6 = (Re ex, Im ex, Re ey, Im ey, Re ez, Im ez). */
+int dda_incident_field(dda_ctx* ctx, int dtype, int nx, int ny, int nz, double d, const double* k3,
+                       const double* pol6, void* e_out, void* stream);
+
 /* Extinction, absorption and scattering cross sections (Draine & Flatau
  * 1994, not present in the reference) reduced in FP64:
  *   out[0] = C_ext = 4 pi k/|E0|^2 sum Im(E_inc* . P)

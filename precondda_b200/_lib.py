@@ -40,6 +40,7 @@ EXPORTS = (
     "dda_version", "dda_last_error", "dda_kernel_launches", "dda_ctx_create", "dda_ctx_destroy", "dda_ctx_trim",
     "dda_fft_length_ok", "dda_green_build", "dda_ghat_to_engine", "dda_op_create", "dda_op_destroy", "dda_matvec",
     "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
+    "dda_voxelize", "dda_incident_field",
 )
 
 
@@ -53,6 +54,15 @@ class DDAError(RuntimeError):
 
 class dda_instance(C.Structure):
     _fields_ = [("ghat", C.c_void_p), ("inv_alpha", C.c_void_p), ("e_inc", C.c_void_p), ("p_out", C.c_void_p)]
+
+
+SHAPE_SPHERE, SHAPE_ELLIPSOID, SHAPE_RECTANGLE, SHAPE_CYLINDER, SHAPE_PRISM = range(5)
+
+
+class dda_shape(C.Structure):
+    _fields_ = [("type", C.c_int), ("axis", C.c_int), ("sides", C.c_int), ("reserved", C.c_int),
+                ("center", C.c_double * 3), ("p", C.c_double * 4), ("rot", C.c_double * 9),
+                ("inv_alpha", C.c_double * 2)]
 
 
 class dda_result(C.Structure):
@@ -87,6 +97,8 @@ def _declare(lib):
     lib.dda_solve_mixed_batch.argtypes = [vp, i, i, i, i, i, i, d, C.POINTER(dda_instance),
                                           C.POINTER(dda_instance), i, d, d, i, i, d, C.POINTER(dda_result), vp]
     lib.dda_cross_sections.argtypes = [vp, i, ll, vp, vp, vp, d, d, C.POINTER(d), vp]
+    lib.dda_voxelize.argtypes = [vp, i, C.POINTER(dda_shape), i, i, i, i, d, C.POINTER(d), vp, vp]
+    lib.dda_incident_field.argtypes = [vp, i, i, i, i, d, C.POINTER(d), C.POINTER(d), vp, vp]
     return lib
 
 

@@ -263,6 +263,47 @@ int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, 
                      (cudaStream_t)stream);
 }
 
+int dda_voxelize(dda_ctx* ctx, int dtype, const dda_shape* shapes, int nshape, int nx, int ny, int nz, double d,
+                 const double* origin3, void* inv_alpha_out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!shapes || nshape < 1 || !inv_alpha_out || !(d > 0)) { set_error("bad voxelize arguments"); return DDA_ERR_ARG; }
+  if (nx < 1 || ny < 1 || nz < 1) { set_error("box dimensions must be >= 1"); return DDA_ERR_BAD_SHAPE; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  for (int i = 0; i < nshape; ++i)
+    if (shapes[i].type < DDA_SHAPE_SPHERE || shapes[i].type > DDA_SHAPE_PRISM ||
+        (shapes[i].type == DDA_SHAPE_PRISM && shapes[i].sides < 3) || shapes[i].axis < 0 || shapes[i].axis > 2) {
+      set_error("bad shape description");
+      return DDA_ERR_ARG;
+    }
+  const double zero[3] = {0, 0, 0};
+  cudaStream_t s = (cudaStream_t)stream;
+  dda_shape* dev = nullptr;
+  cudaError_t e = cudaMallocAsync((void**)&dev, sizeof(dda_shape) * nshape, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_OOM; }
+  e = cudaMemcpyAsync(dev, shapes, sizeof(dda_shape) * nshape, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && voxelize(dev, nshape, nx, ny, nz, d, origin3 ? origin3 : zero, dtype == DDA_C128,
+                                   inv_alpha_out, ctx->c.num_sms, s))
+    e = cudaErrorLaunchFailure;
+  cudaFreeAsync(dev, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  return DDA_OK;
+}
+
+int dda_incident_field(dda_ctx* ctx, int dtype, int nx, int ny, int nz, double d, const double* k3,
+                       const double* pol6, void* e_out, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!k3 || !pol6 || !e_out) { set_error("null argument"); return DDA_ERR_ARG; }
+  if (nx < 1 || ny < 1 || nz < 1) { set_error("box dimensions must be >= 1"); return DDA_ERR_BAD_SHAPE; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  if (plane_wave(nx, ny, nz, d, k3, pol6, dtype == DDA_C128, e_out, ctx->c.num_sms, (cudaStream_t)stream)) {
+    set_error("incident field launch failed");
+    return DDA_ERR_CUDA;
+  }
+  return DDA_OK;
+}
+
 int dda_cross_sections(dda_ctx* ctx, int dtype, long long nsite, const void* p, const void* e_inc,
                        const void* inv_alpha, double k, double e0, double* out3, void* stream) {
   int rc = check_ctx(ctx);

@@ -135,6 +135,25 @@ template <typename R>
 void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, double k, double* red, unsigned* cnt,
                  int RB, double* out, cudaStream_t s);
 
+// Batched helper kernels (util.cu); act = instance list (null: all nb).
+template <typename R>
+void launch_make_b(InstState* st, int nb, long long nsite, int src, int dst, int num_sms, cudaStream_t s,
+                   const int* act);
+void launch_down(InstState* dst, int did, const InstState* src, int sid, int nb, long long n3, int num_sms,
+                 cudaStream_t s, const int* act);
+void launch_accum(InstState* st128, int xid, const InstState* st64, int nb, long long n3, int num_sms,
+                  cudaStream_t s, const int* act);
+template <typename R>
+void launch_norm2(InstState* st, int id, int nb, long long n3, double* red, unsigned* cnt, int RB, double* out,
+                  cudaStream_t s, const int* act);
+int grid_for(long long n, int nb, int num_sms);
+
+// Lattice setup kernels (lattice.cu).
+int voxelize(const dda_shape* shapes_dev, int nshape, int nx, int ny, int nz, double d, const double* origin,
+             bool dbl, void* out, int num_sms, cudaStream_t s);
+int plane_wave(int nx, int ny, int nz, double d, const double* kvec, const double* pol, bool dbl, void* out,
+               int num_sms, cudaStream_t s);
+
 // Green's tensor build: FFT(-G) octant (hx,hy,hz,6) scaled by `scale`.
 // Writes complex128 to out128 (if non-null) and complex64 to out64 (if non-null).
 // soa = 0: reference layout (hx,hy,hz,6); soa = 1: engine layout (6,hx,hy,hz).

@@ -25,11 +25,7 @@ void note_launch(cudaStream_t s, long long n) {
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 const std::string& get_error() { return g_err; }
 
-template <typename R> void launch_make_b(InstState*, int, long long, int, int, int, cudaStream_t);
-void launch_down(InstState*, int, const InstState*, int, int, long long, int, cudaStream_t);
-void launch_accum(InstState*, int, const InstState*, int, long long, int, cudaStream_t);
-template <typename R> void launch_norm2(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
-int grid_for(long long n, int nb, int num_sms);
+
 
 const void* Ctx::twiddles(int L, bool dbl) {
   std::lock_guard<std::mutex> g(mu);
@@ -243,7 +239,7 @@ int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, i
   DDA_CUDA_OK(cudaEventRecord(c.ev_user, user));
   DDA_CUDA_OK(cudaStreamWaitEvent(s, c.ev_user, 0));
   DDA_CUDA_OK(cudaMemcpyAsync(w->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
-  launch_make_b<R>(w->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s);
+  launch_make_b<R>(w->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s, nullptr);
   KrylovLaunch k{w->d_st, nullptr, nb, w->red, w->cnt, (long long)w->n3, w->RB};
   launch_init<R>(k, s);
   DDA_CUDA_OK(cudaGetLastError());
@@ -295,8 +291,9 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
     DDA_CUDA_OK(cudaMemsetAsync(i128[j].p_out, 0, bytes128, s));
   }
   DDA_CUDA_OK(cudaMemcpyAsync(w128->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
-  launch_make_b<double>(w128->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s);
-  launch_norm2<double>(w128->d_st, V_B, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s);
+  launch_make_b<double>(w128->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s, nullptr);
+  launch_norm2<double>(w128->d_st, V_B, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s,
+                       nullptr);
   DDA_CUDA_OK(cudaMemcpyAsync(w128->h_out, w128->d_out, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
   DDA_CUDA_OK(cudaStreamSynchronize(s));
   std::vector<double> bnorm(nb), relres(nb, 1.0);
@@ -330,7 +327,7 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
     }
     DDA_CUDA_OK(cudaMemcpyAsync(w64->d_st, H64, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
     DDA_CUDA_OK(cudaMemcpyAsync(w128->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
-    launch_down(w64->d_st, V_B, w128->d_st, V_R, nb, (long long)w64->n3, c.num_sms, s);
+    launch_down(w64->d_st, V_B, w128->d_st, V_R, nb, (long long)w64->n3, c.num_sms, s, nullptr);
     KrylovLaunch k{w64->d_st, nullptr, nb, w64->red, w64->cnt, (long long)w64->n3, w64->RB};
     launch_init<float>(k, s);
     int rc = run_iterations<float>(c, *w64, gscale, 4);
@@ -347,11 +344,12 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
         lowest_rel[j] = S.initial_norm > 0 ? S.lowest / S.initial_norm : NAN;
       }
     }
-    launch_accum(w128->d_st, V_X, w64->d_st, nb, (long long)w64->n3, c.num_sms, s);
+    launch_accum(w128->d_st, V_X, w64->d_st, nb, (long long)w64->n3, c.num_sms, s, nullptr);
     cudaError_t e = launch_matvec<double>(c, g, w128->pc, w128->d_st, nullptr, nb, V_X, V_R, MV_RESIDUAL, C_ACTIVE,
                                           gscale, s);
     if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
-    launch_norm2<double>(w128->d_st, V_R, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s);
+    launch_norm2<double>(w128->d_st, V_R, nb, (long long)w128->n3, w128->red, w128->cnt, w128->RB, w128->d_out, s,
+                         nullptr);
     DDA_CUDA_OK(cudaMemcpyAsync(w128->h_out, w128->d_out, nb * sizeof(double), cudaMemcpyDeviceToHost, s));
     DDA_CUDA_OK(cudaStreamSynchronize(s));
     for (int j = 0; j < nb; ++j) {

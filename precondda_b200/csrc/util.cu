@@ -9,9 +9,10 @@ namespace dda {
 // b = mask * E  with mask = (inv_alpha != 0) (ddaforgit.py:1108; the
 // reference forms E_inc * mask at Gpbicgstab.py:935, :1064)
 template <typename R>
-__global__ void __launch_bounds__(KNT) k_make_b(InstState* st, long long nsite, int src_id, int dst_id) {
+__global__ void __launch_bounds__(KNT) k_make_b(InstState* st, const int* act, long long nsite, int src_id,
+                                                int dst_id) {
   typedef typename CT<R>::T C;
-  InstState& S = st[blockIdx.y];
+  InstState& S = st[kinst(act)];
   if (!S.active) return;
   const C* __restrict__ e = (const C*)S.vec[src_id];
   const C* __restrict__ ia = (const C*)S.inva;
@@ -24,10 +25,12 @@ __global__ void __launch_bounds__(KNT) k_make_b(InstState* st, long long nsite, 
 }
 
 // dst(c64).vec[did] = (complex64) src(c128).vec[sid]
-__global__ void __launch_bounds__(KNT) k_down(InstState* dst, int did, const InstState* src, int sid, long long n3) {
-  InstState& D = dst[blockIdx.y];
+__global__ void __launch_bounds__(KNT) k_down(InstState* dst, int did, const InstState* src, int sid,
+                                              const int* act, long long n3) {
+  const int j = kinst(act);
+  InstState& D = dst[j];
   if (!D.active) return;
-  const double2* __restrict__ s = (const double2*)src[blockIdx.y].vec[sid];
+  const double2* __restrict__ s = (const double2*)src[j].vec[sid];
   float2* __restrict__ d = (float2*)D.vec[did];
   for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT)
     d[i] = make_float2((float)s[i].x, (float)s[i].y);
@@ -42,12 +45,14 @@ __device__ __forceinline__ const float2* sol64(const InstState& S) {
 }
 
 // x128 += solution(c64)
-__global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const InstState* st64, long long n3) {
-  const InstState& S = st64[blockIdx.y];
-  if (!st128[blockIdx.y].active) return;
+__global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const InstState* st64, const int* act,
+                                               long long n3) {
+  const int j = kinst(act);
+  const InstState& S = st64[j];
+  if (!st128[j].active) return;
   const float2* __restrict__ e = sol64(S);
   if (!e) return;
-  double2* __restrict__ x = (double2*)st128[blockIdx.y].vec[xid];
+  double2* __restrict__ x = (double2*)st128[j].vec[xid];
   for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT) {
     const float2 v = e[i];
     double2 a = x[i];
@@ -58,10 +63,10 @@ __global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const 
 
 // out[inst] = ||vec[id]||^2 (FP64, deterministic)
 template <typename R>
-__global__ void __launch_bounds__(KNT) k_norm2(InstState* st, int id, long long n3, double* red, unsigned* cnt, int RB,
-                                               double* out) {
+__global__ void __launch_bounds__(KNT) k_norm2(InstState* st, const int* act, int id, long long n3, double* red,
+                                               unsigned* cnt, int RB, double* out) {
   typedef typename CT<R>::T C;
-  const int inst = blockIdx.y;
+  const int inst = kinst(act);
   InstState& S = st[inst];
   if (!S.active) return;
   const C* __restrict__ v = (const C*)S.vec[id];
@@ -114,33 +119,36 @@ int grid_for(long long n, int nb, int num_sms) {
 }
 
 template <typename R>
-void launch_make_b(InstState* st, int nb, long long nsite, int src, int dst, int num_sms, cudaStream_t s) {
-  k_make_b<R><<<dim3(grid_for(nsite * 3, nb, num_sms), nb), KNT, 0, s>>>(st, nsite, src, dst);
+void launch_make_b(InstState* st, int nb, long long nsite, int src, int dst, int num_sms, cudaStream_t s,
+                   const int* act) {
+  k_make_b<R><<<dim3(grid_for(nsite * 3, nb, num_sms), nb), KNT, 0, s>>>(st, act, nsite, src, dst);
   note_launch(s, 1);
 }
-template void launch_make_b<float>(InstState*, int, long long, int, int, int, cudaStream_t);
-template void launch_make_b<double>(InstState*, int, long long, int, int, int, cudaStream_t);
+template void launch_make_b<float>(InstState*, int, long long, int, int, int, cudaStream_t, const int*);
+template void launch_make_b<double>(InstState*, int, long long, int, int, int, cudaStream_t, const int*);
 
 void launch_down(InstState* dst, int did, const InstState* src, int sid, int nb, long long n3, int num_sms,
-                 cudaStream_t s) {
-  k_down<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(dst, did, src, sid, n3);
+                 cudaStream_t s, const int* act) {
+  k_down<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(dst, did, src, sid, act, n3);
   note_launch(s, 1);
 }
 
 void launch_accum(InstState* st128, int xid, const InstState* st64, int nb, long long n3, int num_sms,
-                  cudaStream_t s) {
-  k_accum<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(st128, xid, st64, n3);
+                  cudaStream_t s, const int* act) {
+  k_accum<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(st128, xid, st64, act, n3);
   note_launch(s, 1);
 }
 
 template <typename R>
 void launch_norm2(InstState* st, int id, int nb, long long n3, double* red, unsigned* cnt, int RB, double* out,
-                  cudaStream_t s) {
-  k_norm2<R><<<dim3(RB, nb), KNT, 0, s>>>(st, id, n3, red, cnt, RB, out);
+                  cudaStream_t s, const int* act) {
+  k_norm2<R><<<dim3(RB, nb), KNT, 0, s>>>(st, act, id, n3, red, cnt, RB, out);
   note_launch(s, 1);
 }
-template void launch_norm2<float>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
-template void launch_norm2<double>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t);
+template void launch_norm2<float>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t,
+                                  const int*);
+template void launch_norm2<double>(InstState*, int, int, long long, double*, unsigned*, int, double*, cudaStream_t,
+                                   const int*);
 
 template <typename R>
 void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, double k, double* red, unsigned* cnt,

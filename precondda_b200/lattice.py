@@ -5,8 +5,9 @@ build_problem_from_shapes, :1591-1651): shapes are described in physical
 units, snapped to the lattice, voxelised at voxel centres (i+0.5)d, trimmed
 to their bounding box (odd sizes padded to even) and turned into the
 polarizability array alpha (nx,ny,nz) and the incident field E_inc
-(nx,ny,nz,3).  The GPU voxeliser in ``precondda_b200.voxel`` builds the same
-arrays on the device for large lattices.
+(nx,ny,nz,3).  ``voxelize_device`` and ``incident_field_device`` build the
+same arrays with the engine's kernels, on the device, for large lattices and
+the serving path.
 
 Extensions over the reference: ellipsoids accept a rotation matrix (the
 reference's ``axis`` field is unused), and sphere aggregates are a list of
@@ -395,3 +396,79 @@ def ellipsoid_occupancy(box, semi_axes_d, rotation=None):
     X, Y, Z = np.meshgrid(*ax, indexing="ij")
     pts = np.stack([X, Y, Z], -1).reshape(-1, 3)
     return inside_ellipsoid(pts, (0, 0, 0), semi_axes_d, rotation=rotation).reshape(box)
+
+
+# --------------------------------------------------------------------------
+# device builders: the same lattice built by the engine's kernels
+# --------------------------------------------------------------------------
+def _shape_struct(s, inv_alpha):
+    from . import _lib as L
+    st = L.dda_shape()
+    st.inv_alpha[0], st.inv_alpha[1] = float(np.real(inv_alpha)), float(np.imag(inv_alpha))
+    for i in range(9):
+        st.rot[i] = 1.0 if i in (0, 4, 8) else 0.0
+    c = np.asarray(s.center, dtype=np.float64)
+    st.center[0], st.center[1], st.center[2] = c
+    ax = {"x": 0, "y": 1, "z": 2}
+    if isinstance(s, Sphere):
+        st.type, st.p[0] = L.SHAPE_SPHERE, float(s.radius)
+    elif isinstance(s, Ellipsoid):
+        st.type = L.SHAPE_ELLIPSOID
+        for i in range(3):
+            st.p[i] = float(s.semi_axes[i])
+        if s.rotation is not None:
+            R = np.asarray(s.rotation, dtype=np.float64).reshape(9)
+            for i in range(9):
+                st.rot[i] = R[i]
+    elif isinstance(s, Rectangle):
+        st.type = L.SHAPE_RECTANGLE
+        for i in range(3):
+            st.p[i] = float(s.dimensions[i])
+    elif isinstance(s, Cylinder):
+        st.type, st.p[0], st.p[1], st.axis = L.SHAPE_CYLINDER, float(s.radius), float(s.height), ax[s.axis]
+    elif isinstance(s, Prism):
+        st.type, st.p[0], st.p[1] = L.SHAPE_PRISM, float(s.radius), float(s.height)
+        st.axis, st.sides = ax[s.axis], int(s.sides)
+    else:
+        raise ValueError(f"Unsupported shape type: {type(s)}")
+    return st
+
+
+def voxelize_device(shapes, inv_alphas, box, d, origin=(0.0, 0.0, 0.0), dtype=None, device=None):
+    """inv_alpha (nx,ny,nz) on the device: voxel centres origin + (i+0.5) d,
+    each site takes the inverse polarizability of the last shape containing
+    it (the reference's mark_shapes order), 0 elsewhere."""
+    import ctypes as C
+    import torch
+    from . import _lib as L
+    from .engine import _device, _dt_code, stream_handle
+    dtype = dtype or torch.complex128
+    dev = _device(device)
+    n = len(shapes)
+    arr = (L.dda_shape * n)(*[_shape_struct(s, a) for s, a in zip(shapes, inv_alphas)])
+    out = torch.empty(tuple(int(b) for b in box), dtype=dtype, device=dev)
+    org = (C.c_double * 3)(*[float(v) for v in origin])
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_voxelize(ctx.handle, _dt_code(dtype), arr, n, *out.shape, float(d), org,
+                                     out.data_ptr(), stream_handle(dev)))
+    return out
+
+
+def incident_field_device(box, d, k_vec, polarization, dtype=None, device=None):
+    """Plane wave e exp(i k.r), r = (i,j,k) d, on the device (nx,ny,nz,3)."""
+    import ctypes as C
+    import torch
+    from . import _lib as L
+    from .engine import _device, _dt_code, stream_handle
+    dtype = dtype or torch.complex128
+    dev = _device(device)
+    out = torch.empty(tuple(int(b) for b in box) + (3,), dtype=dtype, device=dev)
+    kv = (C.c_double * 3)(*[float(v) for v in k_vec])
+    e = np.asarray(polarization, dtype=np.complex128)
+    pol = (C.c_double * 6)(e[0].real, e[0].imag, e[1].real, e[1].imag, e[2].real, e[2].imag)
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_incident_field(ctx.handle, _dt_code(dtype), *out.shape[:3], float(d), kv, pol,
+                                           out.data_ptr(), stream_handle(dev)))
+    return out

@@ -192,3 +192,33 @@ def test_reference_api_solve_and_near_field():
         P.E_field_solver(Pg.reshape(-1)[:-3], G, (n, n, n))
     with pytest.raises(NotImplementedError):
         P.solve_gpbicgstab((n, n, n), ia, G, None, E, mask, 100, 10, precon=True)
+
+
+def test_device_voxelizer_matches_host_membership():
+    from precondda_b200.lattice import (Sphere, Ellipsoid, Rectangle, Cylinder, Prism, shape_membership,
+                                        voxelize_device, euler_rotation)
+    d = 0.05
+    box = (30, 26, 22)
+    R = euler_rotation(0.4, 1.0, -0.3)
+    shapes = [Rectangle("r", (0.7, 0.6, 0.5), (0.6, 0.5, 0.4), 1.5),
+              Ellipsoid("e", (0.75, 0.65, 0.55), (0.5, 0.35, 0.25), 1.7, rotation=R),
+              Cylinder("c", (0.5, 0.7, 0.5), 0.2, 0.5, "y", 1.4),
+              Prism("p", (1.0, 0.6, 0.6), 0.2, 6, 0.4, 1.3, axis="x"),
+              Sphere("s", (0.4, 0.4, 0.4), 0.23, 1.6)]
+    vals = [1.0 + 0.5j, 2.0 - 1.0j, 3.0 + 0.25j, 4.0, 5.0 - 0.125j]
+    got = voxelize_device(shapes, vals, box, d).cpu().numpy()
+    pts = O.voxel_centres(box, d).reshape(-1, 3)
+    ref = np.zeros(box, np.complex128).reshape(-1)
+    for s, v in zip(shapes, vals):
+        ref[shape_membership(s, pts)] = v
+    assert np.array_equal(got.reshape(-1), ref)
+
+
+def test_device_incident_field_matches_host():
+    from precondda_b200.lattice import incident_field_device
+    k = 2 * np.pi / 0.6
+    kdir = np.array([0.3, -0.5, 0.8]); kdir /= np.linalg.norm(kdir)
+    pol = np.array([1.0, 0.2 + 0.1j, 0.0])
+    got = incident_field_device((9, 7, 5), 0.03, k * kdir, pol).cpu().numpy()
+    ref = O.incident_field((9, 7, 5), 0.03, k, kdir, pol)
+    assert np.abs(got - ref).max() < 1e-13
