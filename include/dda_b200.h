@@ -164,6 +164,45 @@ int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, 
                           double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
                           void* stream);
 
+/* ---- slot pool: continuous batching ------------------------------------- */
+/* A pool of `nslots` solver instances of one box / FFT size that requests
+ * enter and leave independently: a request is admitted into a free slot
+ * while the other slots keep iterating, all occupied slots advance together
+ * through one captured iteration graph, and finished slots are handed back
+ * by dda_slots_poll.  Every slot follows solve_gpbicgstab
+ * (Gpbicgstab.py:879-1201) exactly as a lone solve would: a slot's result
+ * does not depend on what else is in the pool.  The pool runs on its own
+ * stream; admit orders itself after `stream`, poll returns with the finished
+ * slots' outputs complete. */
+#define DDA_PREC_C64 0     /* complex64 GPBiCGSTAB                              */
+#define DDA_PREC_C128 1    /* complex128 GPBiCGSTAB                             */
+#define DDA_PREC_MIXED 2   /* complex64 sweeps + FP64 refinement (as dda_solve_mixed_batch) */
+typedef struct dda_slots dda_slots;
+
+int dda_slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                     int nslots, dda_slots** out);
+void dda_slots_destroy(dda_slots* pool);
+int dda_slots_capacity(const dda_slots* pool);
+/* Index of a free slot, -1 when all are occupied. */
+int dda_slots_free_slot(const dda_slots* pool);
+/* Admit one request into free slot `slot`.  DDA_PREC_C64 reads `lo`,
+ * DDA_PREC_C128 reads `hi`, DDA_PREC_MIXED reads both (lo: complex64 ghat and
+ * inv_alpha; hi: complex128 ghat, inv_alpha, e_inc and p_out).  tol is the
+ * solver target (the FP64 target for mixed pools); inner_tol, max_outer only
+ * matter for mixed pools.  The result lands in p_out when the slot finishes. */
+int dda_slots_admit(dda_slots* pool, int slot, const dda_instance* lo, const dda_instance* hi, double tol,
+                    double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
+/* Enqueue `niter` GPBiCGSTAB iterations of every occupied slot. */
+int dda_slots_run(dda_slots* pool, int niter);
+/* Wait for the pool's stream, then report the slots that finished since the
+ * last poll (finished[0..*nfinished), results in the same order; arrays of
+ * capacity length) and free them.  Mixed pools refine here: a finished
+ * complex64 sweep is accumulated into the FP64 solution, the FP64 residual is
+ * formed, and the slot either finishes or starts another sweep. */
+int dda_slots_poll(dda_slots* pool, int* finished, dda_result* results, int* nfinished, int* nrunning);
+/* Drop a request (cancellation): the slot becomes free, its output is undefined. */
+int dda_slots_release(dda_slots* pool, int slot);
+
 /* ---- lattice setup on the device ---------------------------------------- */
 #define DDA_SHAPE_SPHERE 0
 #define DDA_SHAPE_ELLIPSOID 1

@@ -17,6 +17,7 @@ LIB_PATH = os.environ.get("DDA_LIB_PATH") or os.path.join(_HERE, "libdda_b200.so
 
 DDA_C64 = 0
 DDA_C128 = 1
+DDA_PREC_C64, DDA_PREC_C128, DDA_PREC_MIXED = 0, 1, 2
 
 DDA_OK = 0
 DDA_ERR_BAD_SHAPE = 1
@@ -40,7 +41,8 @@ EXPORTS = (
     "dda_version", "dda_last_error", "dda_kernel_launches", "dda_ctx_create", "dda_ctx_destroy", "dda_ctx_trim",
     "dda_fft_length_ok", "dda_green_build", "dda_ghat_to_engine", "dda_op_create", "dda_op_destroy", "dda_matvec",
     "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
-    "dda_voxelize", "dda_incident_field",
+    "dda_voxelize", "dda_incident_field", "dda_slots_create", "dda_slots_destroy", "dda_slots_capacity",
+    "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
 )
 
 
@@ -99,6 +101,15 @@ def _declare(lib):
     lib.dda_cross_sections.argtypes = [vp, i, ll, vp, vp, vp, d, d, C.POINTER(d), vp]
     lib.dda_voxelize.argtypes = [vp, i, C.POINTER(dda_shape), i, i, i, i, d, C.POINTER(d), vp, vp]
     lib.dda_incident_field.argtypes = [vp, i, i, i, i, d, C.POINTER(d), C.POINTER(d), vp, vp]
+    lib.dda_slots_create.argtypes = [vp, i, i, i, i, i, i, i, d, i, C.POINTER(vp)]
+    lib.dda_slots_destroy.argtypes = [vp]
+    lib.dda_slots_destroy.restype = None
+    lib.dda_slots_capacity.argtypes = [vp]
+    lib.dda_slots_free_slot.argtypes = [vp]
+    lib.dda_slots_admit.argtypes = [vp, i, C.POINTER(dda_instance), C.POINTER(dda_instance), d, d, i, i, d, vp]
+    lib.dda_slots_run.argtypes = [vp, i]
+    lib.dda_slots_poll.argtypes = [vp, C.POINTER(i), C.POINTER(dda_result), C.POINTER(i), C.POINTER(i)]
+    lib.dda_slots_release.argtypes = [vp, i]
     return lib
 
 

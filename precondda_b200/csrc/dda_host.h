@@ -125,6 +125,10 @@ template <typename R> void launch_uzrx(const KrylovLaunch& k, cudaStream_t s);
 template <typename R> void launch_norm(const KrylovLaunch& k, cudaStream_t s);
 template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s);
 
+// One GPBiCGSTAB iteration for every instance of a workspace (solver.cu).
+template <typename R>
+cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s);
+
 template <typename R>
 int solve_batch(Ctx& c, const Geo& g, double gscale, const struct dda_instance* inst, int nb, double target,
                 int max_iter, double ratio, struct dda_result* res, cudaStream_t user);

@@ -130,7 +130,7 @@ void Ctx::trim() {
 // one GPBiCGSTAB iteration for every instance of the workspace
 // ---------------------------------------------------------------------------
 template <typename R>
-static cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s) {
+cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s) {
   KrylovLaunch k{w.d_st, nullptr, w.nb, w.red, w.cnt, (long long)w.n3, w.RB};
   cudaError_t e;
   if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
@@ -147,6 +147,9 @@ static cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStre
   launch_fin<R>(k, s);
   return cudaGetLastError();
 }
+
+template cudaError_t enqueue_iteration<float>(Ctx&, BatchWs&, double, cudaStream_t);
+template cudaError_t enqueue_iteration<double>(Ctx&, BatchWs&, double, cudaStream_t);
 
 template <typename R>
 static int build_graph(Ctx& c, BatchWs& w, double gscale) {

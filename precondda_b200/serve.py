@@ -1,0 +1,396 @@
+"""Continuous-batching DDA solve server on one GPU.
+
+Requests (a lattice: inverse polarizability + incident field, k, d) arrive
+at any time.  Each is padded into a cubic size bucket -- zero polarizability
+outside the scatterer is exactly what the reference's lattices carry in
+their empty voxels, so padding changes no physics (the operator's rows and
+columns of empty sites are zero and Krylov vectors stay zero there) -- and
+admitted into a free slot of that bucket's :class:`SlotPool`.  A pool
+iterates all its occupied slots together in one captured graph
+(``dda_slots_run``); slots finish and are refilled independently
+(``dda_slots_poll``), so a long solve never holds back short ones.
+
+* Green cache: the FFT'd interaction tensor depends on the padded box, the
+  FFT lengths, k and d only; it is built once per key on the device and
+  shared by every request with that key (LRU under a byte budget).
+* HBM admission: a bucket's pool is created with as many slots as fit the
+  memory budget (``slots_per_bucket`` at most); requests wait in FIFO order
+  while their bucket is full.
+* Latency: per request, from submission to the poll that returned it;
+  ``stats()`` gives p50 / p99 and throughput.
+
+Every slot runs the reference's solve_gpbicgstab (Gpbicgstab.py:879-1201)
+recurrence on its own state, so a request's result does not depend on what
+else is in its pool (the GPU tests check this bit for bit).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .engine import (SolveInfo, _device, _info, as_device, fft_lengths, green_octant_pair, stream_handle,
+                     _C64, _C128)
+
+PRECISIONS = {"c64": L.DDA_PREC_C64, "c128": L.DDA_PREC_C128, "mixed": L.DDA_PREC_MIXED}
+DEFAULT_BUCKETS = (8, 12, 16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256)
+
+
+def slot_bytes(box, L_, precision) -> int:
+    """Device bytes one pool slot holds: 16 Krylov vectors and the two FFT
+    scratch volumes in the solver dtype, plus the FP64 right-hand side and
+    residual of a mixed slot."""
+    nx, ny, nz = box
+    Lx, Ly, Lz = L_
+    n3 = nx * ny * nz * 3
+    esz = 16 if precision == "c128" else 8
+    b = (16 * n3 + nx * ny * Lz * 3 + nx * Ly * Lz * 3) * esz
+    if precision == "mixed":
+        b += 2 * n3 * 16
+    return b
+
+
+def request_bytes(box, precision) -> int:
+    """Per-request tensors: inv_alpha and E_inc / P in the solve precisions."""
+    n = box[0] * box[1] * box[2]
+    if precision == "mixed":
+        return n * (8 + 16) + n * 3 * 16 * 2
+    esz = 16 if precision == "c128" else 8
+    return n * esz + n * 3 * esz * 2
+
+
+def choose_bucket(shape, buckets=DEFAULT_BUCKETS) -> int:
+    """Smallest cubic bucket edge that holds the lattice."""
+    m = max(int(v) for v in shape)
+    for b in sorted(buckets):
+        if b >= m:
+            return int(b)
+    raise ValueError(f"lattice {tuple(shape)} exceeds the largest bucket {max(buckets)}")
+
+
+def pool_slots(box, L_, precision, budget_bytes, cap) -> int:
+    """Slots a pool may have under ``budget_bytes`` (HBM admission)."""
+    per = slot_bytes(box, L_, precision) + request_bytes(box, precision)
+    return int(max(0, min(int(cap), int(budget_bytes) // per)))
+
+
+class SlotPool:
+    """``dda_slots_*`` pool: ``nslots`` solver instances of one box / FFT size."""
+
+    def __init__(self, box, L_, nslots, precision="mixed", gscale=1.0, device=None):
+        self.device = _device(device)
+        self.box = tuple(int(v) for v in box)
+        self.L = tuple(int(v) for v in L_)
+        self.precision = precision
+        self.nslots = int(nslots)
+        self._ctx = L.context(self.device.index)
+        h = C.c_void_p()
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_slots_create(self._ctx.handle, PRECISIONS[precision], *self.box, *self.L,
+                                             float(gscale), self.nslots, C.byref(h)))
+        self._h = h
+        self._fin = (C.c_int * self.nslots)()
+        self._res = (L.dda_result * self.nslots)()
+        self._keep = {}        # slot -> tensors the slot reads / writes
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().dda_slots_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def free_slot(self) -> int:
+        return L.lib().dda_slots_free_slot(self._h)
+
+    def admit(self, slot, ghat, inv_alpha, E_inc, tol=1e-5, inner_tol=1e-4, max_iter=2000, max_outer=12,
+              ratio=100.0):
+        """Start a solve in ``slot``.  ``ghat``: engine-layout octant, a
+        (complex64, complex128) pair for mixed pools; inv_alpha / E_inc on the
+        device in the pool's precision (complex128 for mixed pools).  Returns
+        the output tensor, valid once the slot is reported finished."""
+        lo, hi = L.dda_instance(), L.dda_instance()
+        dev = self.device
+        if self.precision == "mixed":
+            g64, g128 = ghat
+            ia128 = as_device(inv_alpha, _C128, dev)
+            ia64 = ia128.to(_C64)
+            E = as_device(E_inc, _C128, dev).reshape(*self.box, 3)
+            P = torch.empty_like(E)
+            lo.ghat, lo.inv_alpha = g64.data_ptr(), ia64.data_ptr()
+            hi.ghat, hi.inv_alpha, hi.e_inc, hi.p_out = g128.data_ptr(), ia128.data_ptr(), E.data_ptr(), P.data_ptr()
+            keep = (g64, g128, ia64, ia128, E, P)
+        else:
+            dt = _C64 if self.precision == "c64" else _C128
+            g = ghat
+            ia = as_device(inv_alpha, dt, dev)
+            E = as_device(E_inc, dt, dev).reshape(*self.box, 3)
+            P = torch.empty_like(E)
+            inst = lo if self.precision == "c64" else hi
+            inst.ghat, inst.inv_alpha, inst.e_inc, inst.p_out = g.data_ptr(), ia.data_ptr(), E.data_ptr(), P.data_ptr()
+            keep = (g, ia, E, P)
+        with torch.cuda.device(dev):
+            L.check(L.lib().dda_slots_admit(self._h, int(slot), C.byref(lo), C.byref(hi), float(tol),
+                                            float(inner_tol), int(max_iter), int(max_outer), float(ratio),
+                                            stream_handle(dev)))
+        self._keep[int(slot)] = keep
+        return P
+
+    def run(self, niter):
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_slots_run(self._h, int(niter)))
+
+    def poll(self):
+        """[(slot, SolveInfo, P)] of the slots that finished; they become free."""
+        nf, nr = C.c_int(0), C.c_int(0)
+        with torch.cuda.device(self.device):
+            L.check(L.lib().dda_slots_poll(self._h, self._fin, self._res, C.byref(nf), C.byref(nr)))
+        self.running = nr.value
+        out = []
+        for q in range(nf.value):
+            s = self._fin[q]
+            keep = self._keep.pop(s)
+            out.append((s, _info(self._res[q]), keep[-1]))
+        return out
+
+    def release(self, slot):
+        L.check(L.lib().dda_slots_release(self._h, int(slot)))
+        self._keep.pop(int(slot), None)
+
+
+class GreenCache:
+    """Device-resident FFT(-G) octants keyed by (box, L, k, d), LRU under a
+    byte budget.  Entries are (complex64, complex128) engine-layout pairs
+    from one FP64 build."""
+
+    def __init__(self, budget_bytes=8 << 30, device=None):
+        self.device = _device(device)
+        self.budget = int(budget_bytes)
+        self.bytes = 0
+        self.hits = 0
+        self.misses = 0
+        self._d: OrderedDict = OrderedDict()
+
+    @staticmethod
+    def key(box, L_, k, d):
+        return (tuple(int(v) for v in box), tuple(int(v) for v in L_), float(k), float(d))
+
+    def get(self, box, L_, k, d):
+        key = self.key(box, L_, k, d)
+        if key in self._d:
+            self._d.move_to_end(key)
+            self.hits += 1
+            return self._d[key]
+        self.misses += 1
+        g128, g64 = green_octant_pair(box, k, d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), self.device)
+        nbytes = g128.numel() * 16 + g64.numel() * 8
+        while self._d and self.bytes + nbytes > self.budget:
+            _, (a, b) = self._d.popitem(last=False)
+            self.bytes -= a.numel() * 8 + b.numel() * 16
+        self._d[key] = (g64, g128)
+        self.bytes += nbytes
+        return g64, g128
+
+    def __len__(self):
+        return len(self._d)
+
+
+@dataclass
+class Request:
+    """One solve: inv_alpha (nx,ny,nz), E_inc (nx,ny,nz,3), k, d."""
+    inv_alpha: object
+    E_inc: object
+    k: float
+    d: float
+    tol: float = 1e-5
+    max_iter: int = 2000
+    rid: int = -1
+    t_submit: float = 0.0
+    t_done: float = 0.0
+    P: object = None
+    info: SolveInfo | None = None
+    bucket: int = 0
+    shape: tuple = ()
+
+
+@dataclass
+class _Bucket:
+    n: int
+    L: tuple
+    pool: SlotPool
+    queue: deque = field(default_factory=deque)
+    active: dict = field(default_factory=dict)    # slot -> Request
+
+
+class DDAServer:
+    """Continuous-batching server (one GPU, one pool per cubic size bucket).
+
+    precision: 'mixed' (complex64 sweeps + FP64 refinement, the default),
+    'c64' or 'c128'.  hbm_budget: bytes the pools may hold (default: 80% of
+    the free device memory at construction)."""
+
+    def __init__(self, precision="mixed", buckets=DEFAULT_BUCKETS, slots_per_bucket=16, chunk_iters=8,
+                 hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None):
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+        self.device = _device(device)
+        self.precision = precision
+        self.buckets = tuple(sorted(int(b) for b in buckets))
+        self.slots_per_bucket = int(slots_per_bucket)
+        self.chunk = int(chunk_iters)
+        if hbm_budget is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            hbm_budget = int(0.8 * free)
+        self.hbm_budget = int(hbm_budget)
+        self.hbm_used = 0
+        self.green = GreenCache(green_budget, self.device)
+        self.inner_tol, self.max_outer, self.ratio = float(inner_tol), int(max_outer), float(ratio)
+        self._b: dict[int, _Bucket] = {}
+        self._next = 0
+        self.done: list[Request] = []
+
+    # -- buckets ------------------------------------------------------------
+    def bucket_for(self, shape) -> int:
+        return choose_bucket(shape, self.buckets)
+
+    def _bucket(self, n) -> _Bucket:
+        if n in self._b:
+            return self._b[n]
+        box = (n, n, n)
+        L_ = fft_lengths(box, _C64 if self.precision == "c64" else _C128)
+        per = slot_bytes(box, L_, self.precision) + request_bytes(box, self.precision)
+        room = self.hbm_budget - self.hbm_used
+        ns = pool_slots(box, L_, self.precision, room, self.slots_per_bucket)
+        if ns < 1:
+            raise MemoryError(f"bucket {n}^3 needs {per / 2**20:.0f} MiB per slot; "
+                              f"{room / 2**20:.0f} MiB of the HBM budget is left")
+        pool = SlotPool(box, L_, ns, self.precision, 1.0, self.device)
+        self.hbm_used += ns * per
+        b = _Bucket(n, L_, pool)
+        self._b[n] = b
+        return b
+
+    # -- requests -----------------------------------------------------------
+    def submit(self, req: Request) -> Request:
+        """Queue a request (arrays on the host or the device)."""
+        ia = req.inv_alpha
+        shape = tuple(int(v) for v in (ia.shape if hasattr(ia, "shape") else np.shape(ia)))
+        if len(shape) != 3:
+            raise ValueError("inv_alpha must have shape (nx, ny, nz)")
+        req.shape = shape
+        req.bucket = self.bucket_for(shape)
+        req.rid = self._next
+        self._next += 1
+        req.t_submit = time.perf_counter()
+        self._bucket(req.bucket).queue.append(req)
+        return req
+
+    def _pad(self, req, n):
+        dt = _C64 if self.precision == "c64" else _C128
+        ia = as_device(req.inv_alpha, dt, self.device)
+        E = as_device(req.E_inc, dt, self.device).reshape(*req.shape, 3)
+        if req.shape == (n, n, n):
+            return ia, E
+        nx, ny, nz = req.shape
+        iap = torch.zeros((n, n, n), dtype=dt, device=self.device)
+        Ep = torch.zeros((n, n, n, 3), dtype=dt, device=self.device)
+        iap[:nx, :ny, :nz] = ia
+        Ep[:nx, :ny, :nz] = E
+        return iap, Ep
+
+    def _fill(self, b: _Bucket):
+        while b.queue:
+            s = b.pool.free_slot()
+            if s < 0:
+                return
+            req = b.queue.popleft()
+            g64, g128 = self.green.get((b.n,) * 3, b.L, req.k, req.d)
+            ghat = (g64, g128) if self.precision == "mixed" else (g64 if self.precision == "c64" else g128)
+            ia, E = self._pad(req, b.n)
+            b.pool.admit(s, ghat, ia, E, tol=req.tol, inner_tol=self.inner_tol, max_iter=req.max_iter,
+                         max_outer=self.max_outer, ratio=self.ratio)
+            b.active[s] = req
+
+    def pending(self) -> int:
+        return sum(len(b.queue) + len(b.active) for b in self._b.values())
+
+    def step(self) -> list:
+        """Admit waiting requests, advance every busy pool by ``chunk_iters``
+        iterations, collect finished requests.  Returns those requests."""
+        for b in self._b.values():
+            self._fill(b)
+        busy = [b for b in self._b.values() if b.active]
+        for b in busy:
+            b.pool.run(self.chunk)
+        out = []
+        for b in busy:
+            for s, info, P in b.pool.poll():
+                req = b.active.pop(s)
+                req.t_done = time.perf_counter()
+                nx, ny, nz = req.shape
+                req.P = P[:nx, :ny, :nz] if P.shape[:3] != req.shape else P
+                req.info = info
+                out.append(req)
+        self.done.extend(out)
+        return out
+
+    def drain(self, timeout_s=600.0) -> list:
+        """Step until every submitted request has finished."""
+        t0 = time.perf_counter()
+        out = []
+        while self.pending():
+            out.extend(self.step())
+            if time.perf_counter() - t0 > timeout_s:
+                raise TimeoutError(f"{self.pending()} requests still running after {timeout_s} s")
+        return out
+
+    def serve(self, requests, arrivals_s=None, timeout_s=600.0) -> list:
+        """Replay ``requests`` arriving at offsets ``arrivals_s`` (seconds
+        from now; all at once when None) and run until all finish."""
+        reqs = list(requests)
+        arr = [0.0] * len(reqs) if arrivals_s is None else list(arrivals_s)
+        order = sorted(range(len(reqs)), key=lambda j: arr[j])
+        t0 = time.perf_counter()
+        q = 0
+        out = []
+        while q < len(order) or self.pending():
+            now = time.perf_counter() - t0
+            while q < len(order) and arr[order[q]] <= now:
+                r = self.submit(reqs[order[q]])
+                r.t_submit = t0 + arr[order[q]]
+                q += 1
+            if self.pending():
+                out.extend(self.step())
+            elif q < len(order):
+                time.sleep(max(0.0, min(1e-3, arr[order[q]] - now)))
+            if now > timeout_s:
+                raise TimeoutError("serve loop exceeded its time limit")
+        return out
+
+    def stats(self, reqs=None) -> dict:
+        reqs = self.done if reqs is None else reqs
+        if not reqs:
+            return {"n": 0}
+        lat = np.array([r.t_done - r.t_submit for r in reqs])
+        span = max(r.t_done for r in reqs) - min(r.t_submit for r in reqs)
+        return {"n": len(reqs), "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                "p99_ms": float(np.percentile(lat, 99) * 1e3), "mean_ms": float(lat.mean() * 1e3),
+                "solves_per_s": len(reqs) / span if span > 0 else math.inf,
+                "green_hits": self.green.hits, "green_misses": self.green.misses,
+                "pools": {b.n: b.pool.nslots for b in self._b.values()}}
+
+    def close(self):
+        for b in self._b.values():
+            b.pool.close()
+        self._b.clear()

@@ -117,3 +117,22 @@ def test_shape_membership_zoo():
     assert p.sum() > 0
     # a square prism (4 sides, vertices on the axes) has area 2 r^2
     assert abs(p.sum() / 6 - 2 * 16) < 12
+
+
+def test_serve_buckets_and_hbm_admission():
+    from precondda_b200.serve import choose_bucket, pool_slots, slot_bytes, request_bytes
+    assert choose_bucket((10, 12, 14), (8, 16, 32)) == 16
+    assert choose_bucket((16, 3, 3), (8, 16, 32)) == 16
+    assert choose_bucket((17, 3, 3), (8, 16, 32)) == 32
+    with pytest.raises(ValueError):
+        choose_bucket((33, 1, 1), (8, 16, 32))
+    box, L = (64, 64, 64), (128, 128, 128)
+    n3 = 64 ** 3 * 3
+    scratch = 64 * 64 * 128 * 3 + 64 * 128 * 128 * 3
+    assert slot_bytes(box, L, "c64") == (16 * n3 + scratch) * 8
+    assert slot_bytes(box, L, "c128") == (16 * n3 + scratch) * 16
+    assert slot_bytes(box, L, "mixed") == (16 * n3 + scratch) * 8 + 2 * n3 * 16
+    per = slot_bytes(box, L, "mixed") + request_bytes(box, "mixed")
+    assert pool_slots(box, L, "mixed", 10 * per + per // 2, 64) == 10
+    assert pool_slots(box, L, "mixed", 10 * per, 4) == 4
+    assert pool_slots(box, L, "mixed", per - 1, 4) == 0
