@@ -75,6 +75,55 @@ template <class C> __device__ __forceinline__ void dft16(C* a) {
   for (int i = 0; i < 16; ++i) a[i] = o[i];
 }
 
+// DFTs whose upper half of inputs is zero (a[R/2..R-1] = 0), as the first
+// stage of a transform of zero-padded data: the first radix-2 layer
+// degenerates into copies.
+template <class C> __device__ __forceinline__ void dft4_zh(C& a0, C& a1, C& a2, C& a3) {
+  const C x0 = a0, x1 = a1, y1 = cmul_mi(a1);
+  a0 = cadd(x0, x1); a2 = csub(x0, x1); a1 = cadd(x0, y1); a3 = csub(x0, y1);
+}
+
+template <class C> __device__ __forceinline__ void dft8_zh(C* a) {
+  typedef decltype(a[0].x) R;
+  const R h = (R)0.7071067811865476;
+  C b0 = a[0], b1 = a[1], b2 = a[2], b3 = a[3];
+  C c0 = a[0], c1 = a[1], c2 = a[2], c3 = a[3];
+  C t;
+  t = c1; c1.x = h * (t.x + t.y); c1.y = h * (t.y - t.x);
+  c2 = cmul_mi(c2);
+  t = c3; c3.x = h * (t.y - t.x); c3.y = -h * (t.x + t.y);
+  dft4(b0, b1, b2, b3);
+  dft4(c0, c1, c2, c3);
+  a[0] = b0; a[2] = b1; a[4] = b2; a[6] = b3;
+  a[1] = c0; a[3] = c1; a[5] = c2; a[7] = c3;
+}
+
+template <class C> __device__ __forceinline__ void dft16_zh(C* a) {
+  typedef decltype(a[0].x) R;
+  const R c1 = (R)0.9238795325112867, s1 = (R)0.3826834323650898, h = (R)0.7071067811865476;
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) dft4_zh(a[n1], a[n1 + 4], a[n1 + 8], a[n1 + 12]);
+  C t;
+  t = a[5];  a[5].x = c1 * t.x + s1 * t.y;  a[5].y = c1 * t.y - s1 * t.x;
+  t = a[9];  a[9].x = h * (t.x + t.y);      a[9].y = h * (t.y - t.x);
+  t = a[13]; a[13].x = s1 * t.x + c1 * t.y; a[13].y = s1 * t.y - c1 * t.x;
+  t = a[6];  a[6].x = h * (t.x + t.y);      a[6].y = h * (t.y - t.x);
+  a[10] = cmul_mi(a[10]);
+  t = a[14]; a[14].x = h * (t.y - t.x);     a[14].y = -h * (t.x + t.y);
+  t = a[7];  a[7].x = s1 * t.x + c1 * t.y;  a[7].y = s1 * t.y - c1 * t.x;
+  t = a[11]; a[11].x = h * (t.y - t.x);     a[11].y = -h * (t.x + t.y);
+  t = a[15]; a[15].x = -c1 * t.x - s1 * t.y; a[15].y = -c1 * t.y + s1 * t.x;
+#pragma unroll
+  for (int k2 = 0; k2 < 4; ++k2) dft4(a[4 * k2], a[4 * k2 + 1], a[4 * k2 + 2], a[4 * k2 + 3]);
+  C o[16];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) o[4 * k1 + k2] = a[4 * k2 + k1];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) a[i] = o[i];
+}
+
 // odd radix via the conjugate-pair formulation:
 // y_q = a0 + sum_k [cos(2 pi kq/R) (a_k + a_{R-k}) - i sin(2 pi kq/R) (a_k - a_{R-k})]
 template <int R_> struct OddTab;
@@ -134,6 +183,14 @@ template <int RAD, class C> __device__ __forceinline__ void dft(C* a) {
   else if constexpr (RAD == 8) dft8(a);
   else if constexpr (RAD == 16) dft16(a);
   else dft_odd<RAD>(a);
+}
+
+template <int RAD, class C> __device__ __forceinline__ void dft_zh(C* a) {
+  static_assert(RAD % 2 == 0, "zero-half DFT needs an even radix");
+  if constexpr (RAD == 2) { a[1] = a[0]; }
+  else if constexpr (RAD == 4) dft4_zh(a[0], a[1], a[2], a[3]);
+  else if constexpr (RAD == 8) dft8_zh(a);
+  else dft16_zh(a);
 }
 
 // ---- compile-time FFT plans ----------------------------------------------

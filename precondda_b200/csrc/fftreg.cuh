@@ -88,49 +88,40 @@ template <int L> struct PlanFor<L, double> : Plan8<L> {};
 
 
 // shared-memory position padding: one spare slot every 16 positions
-__device__ __forceinline__ constexpr int ppad(int pos) { return pos + (pos >> 4); }
-__host__ __device__ constexpr int ppad_len(int L) { return L + (L >> 4) + 1; }
+#ifndef DDA_PPAD
+#define DDA_PPAD 1
+#endif
+__device__ __forceinline__ constexpr int ppad(int pos) { return DDA_PPAD ? pos + (pos >> 4) : pos; }
+__host__ __device__ constexpr int ppad_len(int L) { return DDA_PPAD ? L + (L >> 4) + 1 : L; }
 
-// Compute stage s of plan P on the thread's registers a[E] (twiddles for s>0).
-template <class P, int s, bool INV, class C>
+// Compute stage s of plan P on the thread's registers a[E] (twiddles for
+// s > 0).  Always the forward transform: inverse transforms are run as
+// swap(FFT(swap(x))), swap(a + ib) = b + ia, which costs no instructions.
+// ZH (stage 0 only): the upper half of every butterfly's inputs is zero.
+template <class P, int s, bool ZH = false, class C>
 __device__ __forceinline__ void rstage(C* a, int t, const C* __restrict__ tw) {
+  static_assert(!ZH || s == 0, "zero-half inputs only at stage 0");
   constexpr int R = P::r[s];
   constexpr int NS = P::ns(s);
   constexpr int BPT = P::E / R;
 #pragma unroll
   for (int b = 0; b < BPT; ++b) {
     C* v = a + b * R;
-    if (INV) {
-#pragma unroll
-      for (int m = 0; m < R; ++m) v[m].y = -v[m].y;
-    }
     if constexpr (NS > 1) {
-      // twiddles w^m, w = exp(-2 pi i k/(NS R)): w^1, w^2, w^4, w^8 from the
-      // table, the others as products of those (at most 3 roundings)
+      // twiddles w^m, w = exp(-2 pi i k/(NS R)), straight from the length-L
+      // table (index m k L/(NS R) < L); the lanes of a warp mostly share k,
+      // so the loads are broadcasts out of L1
       constexpr int ST = P::L / (NS * R);
       const int k = (t + b * P::T) % NS;
-      const C w1 = tw[k * ST];
-      const C w2 = (R > 2) ? tw[2 * k * ST] : w1;
-      const C w4 = (R > 4) ? tw[4 * k * ST] : w1;
-      const C w8 = (R > 8) ? tw[8 * k * ST] : w1;
 #pragma unroll
-      for (int m = 1; m < R; ++m) {
-        C w;
-        bool set = false;
-        if (m & 1) { w = w1; set = true; }
-        if (m & 2) { w = set ? cmul(w, w2) : w2; set = true; }
-        if (m & 4) { w = set ? cmul(w, w4) : w4; set = true; }
-        if (m & 8) { w = set ? cmul(w, w8) : w8; set = true; }
-        v[m] = cmul(v[m], w);
-      }
+      for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tw + m * k * ST));
     }
-    dft<R>(v);
-    if (INV) {
-#pragma unroll
-      for (int m = 0; m < R; ++m) v[m].y = -v[m].y;
-    }
+    if constexpr (ZH) dft_zh<R>(v);
+    else dft<R>(v);
   }
 }
+
+template <class C> __device__ __forceinline__ C cswap(C v) { C r; r.x = v.y; r.y = v.x; return r; }
 
 // Positions touched by a thread: input of stage s (butterfly b, leg m) and
 // output of stage s (butterfly b, leg q).
@@ -153,7 +144,7 @@ __device__ __forceinline__ int rout_pos(int t, int b, int q) {
 // `sm(c, ppos)` returns the shared-memory slot of padded position ppos of
 // component c of this thread's transform.  All threads of the CTA must call
 // this together (it contains barriers).
-template <class P, int NC, int s, bool INV, class C, class SM>
+template <class P, int NC, int s, class C, class SM>
 __device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const C* __restrict__ tw) {
   constexpr int R = P::r[s];
   constexpr int R2 = P::r[s + 1];
@@ -172,51 +163,73 @@ __device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const C* __
       for (int m = 0; m < R2; ++m) a[c * P::E + b * R2 + m] = sm(c, ppad(rin_pos<P, s + 1>(t, b, m)));
   __syncthreads();
 #pragma unroll
-  for (int c = 0; c < NC; ++c) rstage<P, s + 1, INV>(a + c * P::E, t, tw);
+  for (int c = 0; c < NC; ++c) rstage<P, s + 1>(a + c * P::E, t, tw);
 }
 
 // Stages s+1..S-1 (stage 0 is computed by the caller after its global load).
-template <class P, int NC, int s, bool INV, class C, class SM>
+template <class P, int NC, int s, class C, class SM>
 __device__ __forceinline__ void rrest(C* a, int t, const SM& sm, const C* __restrict__ tw) {
   if constexpr (s + 1 < P::S) {
-    rexchange<P, NC, s, INV>(a, t, sm, tw);
-    rrest<P, NC, s + 1, INV>(a, t, sm, tw);
+    rexchange<P, NC, s>(a, t, sm, tw);
+    rrest<P, NC, s + 1>(a, t, sm, tw);
   }
 }
 
 // Stage-0 load: a[c*E + b*R0 + m] = ld(c, pos) for the thread's input positions.
-template <class P, int NC, class C, class LD>
+// ZH: positions >= L/2 are known to be zero (they are exactly the legs
+// m >= R0/2, because t + b*T < L/R0) and are not loaded.
+template <class P, int NC, bool ZH = false, class C, class LD>
 __device__ __forceinline__ void rload(C* a, int t, const LD& ld) {
   constexpr int R0 = P::r[0];
+  static_assert(!ZH || R0 % 2 == 0, "zero-half load needs an even first radix");
 #pragma unroll
   for (int m = 0; m < R0; ++m)
 #pragma unroll
     for (int b = 0; b < P::E / R0; ++b)
 #pragma unroll
-      for (int c = 0; c < NC; ++c) a[c * P::E + b * R0 + m] = ld(c, rin_pos<P, 0>(t, b, m));
+      for (int c = 0; c < NC; ++c)
+        a[c * P::E + b * R0 + m] = (ZH && m >= R0 / 2) ? czero<C>() : ld(c, rin_pos<P, 0>(t, b, m));
 }
 
+// Whether the last stage's outputs at positions >= L/2 are exactly the legs
+// q >= R/2 (true for an even last radix: the output position is jb + q*NS
+// with jb < NS and NS*R = L).
+template <class P> constexpr bool half_store_ok() { return P::r[P::S - 1] % 2 == 0; }
+
 // Last-stage store: st(c, pos, value) for the thread's output positions.
-template <class P, int NC, class C, class ST>
+// DH: only positions < L/2 are wanted (requires half_store_ok<P>()).
+template <class P, int NC, bool DH = false, class C, class ST>
 __device__ __forceinline__ void rstore(const C* a, int t, const ST& st) {
   constexpr int RL = P::r[P::S - 1];
+  static_assert(!DH || half_store_ok<P>(), "half store needs an even last radix");
 #pragma unroll
-  for (int q = 0; q < RL; ++q)
+  for (int q = 0; q < (DH ? RL / 2 : RL); ++q)
 #pragma unroll
     for (int b = 0; b < P::E / RL; ++b)
 #pragma unroll
       for (int c = 0; c < NC; ++c) st(c, rout_pos<P, P::S - 1>(t, b, q), a[c * P::E + b * RL + q]);
 }
 
-// Full transform of NC components: load, all stages, store.
-template <class P, int NC, bool INV, class C, class LD, class SM, class ST>
+// Full transform of NC components: load, all stages, store.  INV: the
+// inverse (unnormalised) transform, as swap(FFT(swap(x))).
+// ZH / DH: zero upper half of the input / only the lower half of the output
+// wanted (see rload / rstore).
+template <class P, int NC, bool INV, bool ZH = false, bool DH = false, class C, class LD, class SM, class ST>
 __device__ __forceinline__ void rfft(C* a, int t, const LD& ld, const SM& sm, const ST& st,
                                      const C* __restrict__ tw) {
-  rload<P, NC>(a, t, ld);
+  if constexpr (INV) {
+    rload<P, NC, ZH>(a, t, [&](int c, int pos) -> C { return cswap(ld(c, pos)); });
+  } else {
+    rload<P, NC, ZH>(a, t, ld);
+  }
 #pragma unroll
-  for (int c = 0; c < NC; ++c) rstage<P, 0, INV>(a + c * P::E, t, tw);
-  rrest<P, NC, 0, INV>(a, t, sm, tw);
-  rstore<P, NC>(a, opaque(t), st);
+  for (int c = 0; c < NC; ++c) rstage<P, 0, ZH>(a + c * P::E, t, tw);
+  rrest<P, NC, 0>(a, t, sm, tw);
+  if constexpr (INV) {
+    rstore<P, NC, DH>(a, opaque(t), [&](int c, int pos, C v) { st(c, pos, cswap(v)); });
+  } else {
+    rstore<P, NC, DH>(a, opaque(t), st);
+  }
 }
 
 }  // namespace dda

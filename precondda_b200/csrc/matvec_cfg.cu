@@ -1,7 +1,27 @@
 // Tile shapes of the five matvec passes (see matvec_impl.cuh).
 #include "matvec_impl.cuh"
 
+#include <mutex>
+#include <set>
+#include <utility>
+
 namespace dda {
+
+cudaError_t mv_prepare(const void* const* ks, int n) {
+  static std::mutex mu;
+  static std::set<std::pair<int, const void*>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  for (int i = 0; i < n; ++i) {
+    if (done.count({dev, ks[i]})) continue;
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
+    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
+    done.insert({dev, ks[i]});
+  }
+  return cudaSuccess;
+}
 
 PassCfg make_pass_cfg(const Geo& g, bool dbl) {
   return dbl ? make_pass_cfg_impl<double>(g) : make_pass_cfg_impl<float>(g);

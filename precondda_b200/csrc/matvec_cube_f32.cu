@@ -1,0 +1,16 @@
+// complex64 matvec passes specialised for a cubic box n^3 on a (2n)^3 grid
+// (compiled apart from the general kernels so the two build in parallel).
+#include "matvec_impl.cuh"
+
+namespace dda {
+template <>
+bool mv_cube_set<float>(int L, int p3var, MvSet<float>& o) {
+  if (p3var != 0) return false;
+  switch (L) {
+#define DDA_K(n) case n: mv_cube_fill<float, n, 0>(o); return true;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+  }
+  return false;
+}
+}  // namespace dda

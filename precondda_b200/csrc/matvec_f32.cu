@@ -3,6 +3,10 @@
 
 namespace dda {
 template <>
+bool mv_general_set<float>(int Lx, int Ly, int Lz, int p3var, MvSet<float>& out) {
+  return mv_general_set_impl<float>(Lx, Ly, Lz, p3var, out);
+}
+template <>
 cudaError_t launch_matvec<float>(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                                  int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
   return launch_matvec_impl<float>(ctx, g, pc, st, act, nb, in_id, out_id, mode, cond, gscale, s);

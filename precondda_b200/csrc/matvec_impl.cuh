@@ -49,36 +49,57 @@ constexpr int kP3Variants = 3;
 __device__ __forceinline__ int inst_of(const int* act) { return act ? act[blockIdx.y] : (int)blockIdx.y; }
 
 // ---------------------------------------------------------------------------
+// Tile sizes shared by the host configuration and the compile-time kernels:
+// about 128 (complex64) or 64 (complex128) transforms' worth of threads per
+// CTA.
+// ---------------------------------------------------------------------------
+template <typename R> constexpr int mv_lanes() { return sizeof(R) == 4 ? 128 : 64; }
+constexpr int cmin_i(int a, int b) { return a < b ? a : b; }
+template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T > 1 ? mv_lanes<R>() / T : 1; }
+
+// NC > 0 selects the cubic specialisation of a pass: box NC^3 on the FFT
+// grid (2 NC)^3, every size a compile-time constant, so shared-memory and
+// global addresses become immediate offsets from per-thread bases, the zero
+// half of each padded input is never loaded (and its first butterfly layer
+// is pruned), and only the kept half of each inverse output is formed.
+// NC = 0 reads the sizes from Geo.
+
+// ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
 // thread = (c fastest, t, line)
 // ---------------------------------------------------------------------------
-template <typename R, int LZ>
+template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int cond,
-                                                            int nl) {
+                                                            int nl_) {
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
+  constexpr bool CUBE = NC > 0;
+  static_assert(!CUBE || LZ == 2 * NC, "cubic kernels need L = 2n");
+  constexpr int NLC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), NC * NC) : 1;
+  constexpr bool ZH = CUBE && P::r[0] % 2 == 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   const C* __restrict__ x = (const C*)S.vec[in_id];
   C* __restrict__ t1 = (C*)S.t1;
+  const int nl = CUBE ? NLC : nl_;
+  const int nz = CUBE ? NC : g.nz;
+  const long long nlines = CUBE ? (long long)NC * NC : (long long)g.nx * g.ny;
   const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
   const int t = rest % SH::T, l = rest / SH::T;
-  const long long nlines = (long long)g.nx * g.ny;
   const long long line = (long long)blockIdx.x * nl + l;
-  const bool ok = line < nlines;
-  const int nz = g.nz;
+  const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
   const C* xl = x + line * nz * 3 + c;
   C* tl = t1 + line * (long long)LZ * 3 + c;
   C* sl = s + l * 3 * SH::LP + c;
-  auto ld = [&](int, int pos) -> C { return (ok && pos < nz) ? xl[pos * 3] : czero<C>(); };
+  auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nz)) ? __ldcg(xl + pos * 3) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
-  auto stf = [&](int, int pos, C v) { if (ok) tl[pos * 3] = v; };
+  auto stf = [&](int, int pos, C v) { if (ok) __stcg(tl + pos * 3, v); };
   C a[P::E];
-  rfft<P, 1, false>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -86,34 +107,45 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
 // thread = (w fastest, t).  INV=false: T1 -> T2 (rows y >= ny are zero);
 // INV=true: T2 -> T1 keeping rows y < ny.
 // ---------------------------------------------------------------------------
-template <typename R, bool INV, int LY>
+template <typename R, bool INV, int LY, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                             InstState* st, const int* act, int cond, int tz,
-                                                             int ntz) {
+                                                             InstState* st, const int* act, int cond, int tz_,
+                                                             int ntz_) {
   typedef typename CT<R>::T C;
   typedef MvShape<R, LY> SH;
   typedef typename SH::P P;
+  constexpr bool CUBE = NC > 0;
+  static_assert(!CUBE || LY == 2 * NC, "cubic kernels need L = 2n");
+  constexpr int TZC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), LY) : 1;
+  constexpr int NTZC = (LY + TZC - 1) / TZC;
+  constexpr bool ZH = CUBE && !INV && P::r[0] % 2 == 0;
+  constexpr bool DH = CUBE && INV && half_store_ok<P>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t1 = (C*)S.t1;
   C* __restrict__ t2 = (C*)S.t2;
+  const int tz = CUBE ? TZC : tz_;
+  const int ntz = CUBE ? NTZC : ntz_;
+  const int Lz = CUBE ? LY : g.Lz;
+  const int ny = CUBE ? NC : g.ny;
   const int W = 3 * tz;
   const int w = threadIdx.x % W, t = threadIdx.x / W;
   const int ix = blockIdx.x / ntz, kzt = blockIdx.x - ix * ntz;
   const int kz0 = kzt * tz;
-  const bool ok = w < 3 * min(tz, g.Lz - kz0);
-  const int ny = g.ny;
-  const long long rs = (long long)g.Lz * 3;                 // row stride of T1/T2
+  const bool ok = (CUBE && LY % TZC == 0) || w < 3 * min(tz, Lz - kz0);
+  const long long rs = (long long)Lz * 3;                 // row stride of T1/T2
   const C* src = (INV ? t2 + (long long)ix * LY * rs : t1 + (long long)ix * ny * rs) + kz0 * 3 + w;
   C* dst = (INV ? t1 + (long long)ix * ny * rs : t2 + (long long)ix * LY * rs) + kz0 * 3 + w;
   C* sw = s + w;
-  auto ld = [&](int, int pos) -> C { return (ok && (INV || pos < ny)) ? src[pos * rs] : czero<C>(); };
+  auto ld = [&](int, int pos) -> C {
+    return (ok && (INV || ZH || pos < ny)) ? __ldcg(src + pos * rs) : czero<C>();
+  };
   auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
-  auto stf = [&](int, int pos, C v) { if (ok && (!INV || pos < ny)) dst[pos * rs] = v; };
+  auto stf = [&](int, int pos, C v) { if (ok && (!INV || DH || pos < ny)) __stcg(dst + pos * rs, v); };
   C a[P::E];
-  rfft<P, 1, INV>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, INV, ZH, DH>(a, t, ld, sm, stf, tw);
 }
 
 // ---------------------------------------------------------------------------
@@ -136,7 +168,8 @@ __device__ __forceinline__ void tensor3(const C* __restrict__ gh, const Geo& g, 
   const int mz = fz ? g.Lz - kz : kz;
   const long long H = (long long)g.hx * g.hy * g.hz;
   const C* q = gh + ((long long)mx * g.hy + my) * g.hz + mz;
-  C gxx = q[0], gxy = q[H], gxz = q[2 * H], gyy = q[3 * H], gyz = q[4 * H], gzz = q[5 * H];
+  C gxx = __ldg(q), gxy = __ldg(q + H), gxz = __ldg(q + 2 * H), gyy = __ldg(q + 3 * H), gyz = __ldg(q + 4 * H),
+    gzz = __ldg(q + 5 * H);
   const R sxy = (fx != fy) ? -gscale : gscale;
   const R sxz = (fx != fz) ? -gscale : gscale;
   const R syz = (fy != fz) ? -gscale : gscale;
@@ -155,7 +188,7 @@ __device__ __forceinline__ int pencil_ky(int p, int Ly) {
 }
 
 // variant with the three components of a pencil in one thread:
-// thread = (kzl fastest, t)
+// thread = (kzl fastest, t); general sizes only
 template <typename R, int LX, int V>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz,
@@ -181,13 +214,13 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
   C* col = t2 + ((long long)ky * g.Lz + kz) * 3;
   const int W = 3 * tz;
   C* sw = s + 3 * kzl;
-  auto ld = [&](int c, int pos) -> C { return (ok && pos < nx) ? col[pos * rs + c] : czero<C>(); };
+  auto ld = [&](int c, int pos) -> C { return (ok && pos < nx) ? __ldcg(col + pos * rs + c) : czero<C>(); };
   auto sm = [&](int c, int pp) -> C& { return sw[pp * W + c]; };
   C a[3 * P::E];
   rload<P, 3>(a, t, ld);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) rstage<P, 0, false>(a + c * P::E, t, tw);
-  rrest<P, 3, 0, false>(a, t, sm, tw);
+  for (int c = 0; c < 3; ++c) rstage<P, 0>(a + c * P::E, t, tw);
+  rrest<P, 3, 0>(a, t, sm, tw);
   // tensor product at the positions this thread owns after the last stage
   constexpr int RL = P::r[P::S - 1];
   const bool fy = ky > g.Ly / 2;
@@ -204,63 +237,109 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
   // inverse transform with the reversed plan: its stage 0 owns the same positions
   const int ti = opaque(t);
   C* colo = opaque_ptr(col);
-  auto stf = [&](int c, int pos, C v) { if (ok && pos < nx) colo[pos * rs + c] = v; };
+  auto stf = [&](int c, int pos, C v) { if (ok && pos < nx) __stcg(colo + pos * rs + c, cswap(v)); };
 #pragma unroll
-  for (int c = 0; c < 3; ++c) rstage<Q, 0, true>(a + c * P::E, ti, tw);
-  rrest<Q, 3, 0, true>(a, ti, sm, tw);
+  for (int i = 0; i < 3 * P::E; ++i) a[i] = cswap(a[i]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) rstage<Q, 0>(a + c * P::E, ti, tw);
+  rrest<Q, 3, 0>(a, ti, sm, tw);
   rstore<Q, 3>(a, ti, stf);
 }
 
 // variant with one component per thread and the tensor product through
-// shared memory (bounded registers for complex128): thread = (w fastest, t)
-template <typename R, int LX, int V>
-__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                             InstState* st, const int* act, int cond, int tz,
-                                                             int ntz, R gscale) {
+// shared memory: thread = (w fastest, t)
+// Cubic complex64 kernels of power-of-two length (E <= 16 per thread) fit
+// three CTAs of 384 threads per SM without spills worth the occupancy.
+#ifndef DDA_P3_MINB
+#define DDA_P3_MINB 3
+#endif
+template <typename R, int LX, int NC>
+constexpr int p3_min_blocks() {
+  return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? DDA_P3_MINB : 1;
+}
+template <typename R, int LX, int V, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                             InstState* st, const int* act, int cond, int tz_,
+                                                             int ntz_, R gscale) {
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
   typedef typename SH::P P;
   typedef RevPlan<P> Q;
+  constexpr bool CUBE = NC > 0;
+  static_assert(!CUBE || LX == 2 * NC, "cubic kernels need L = 2n");
+  constexpr int TZC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), LX) : 1;
+  constexpr int NTZC = (LX + TZC - 1) / TZC;
+  constexpr bool ZH = CUBE && P::r[0] % 2 == 0;
+  constexpr bool DH = CUBE && half_store_ok<Q>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t2 = (C*)S.t2;
   const C* __restrict__ gh = (const C*)S.ghat;
+  const int tz = CUBE ? TZC : tz_;
+  const int ntz = CUBE ? NTZC : ntz_;
+  const int Ly = CUBE ? LX : g.Ly, Lz = CUBE ? LX : g.Lz;
+  const int hy = CUBE ? LX / 2 + 1 : g.hy, hz = CUBE ? LX / 2 + 1 : g.hz;
+  const int H = CUBE ? (LX / 2 + 1) * (LX / 2 + 1) * (LX / 2 + 1) : g.hx * g.hy * g.hz;
+  const int nx = CUBE ? NC : g.nx;
   const int W = 3 * tz;
   const int w = threadIdx.x % W, t = threadIdx.x / W;
   const int p = blockIdx.x / ntz, kzt = blockIdx.x - p * ntz;
-  const int ky = pencil_ky(p, g.Ly);
+  const int ky = pencil_ky(p, Ly);
   const int kz0 = kzt * tz;
-  const int tzn = min(tz, g.Lz - kz0);
+  const int tzn = (CUBE && LX % TZC == 0) ? tz : min(tz, Lz - kz0);
   const bool ok = w < 3 * tzn;
-  const int nx = g.nx;
-  const long long rs = (long long)g.Ly * g.Lz * 3;
-  C* col = t2 + ((long long)ky * g.Lz + kz0) * 3 + w;
+  const long long rs = (long long)Ly * Lz * 3;
+  C* col = t2 + ((long long)ky * Lz + kz0) * 3 + w;
   C* sw = s + w;
-  auto ld = [&](int, int pos) -> C { return (ok && pos < nx) ? col[pos * rs] : czero<C>(); };
+  auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nx)) ? __ldcg(col + pos * rs) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
   C a[P::E];
-  rload<P, 1>(a, t, ld);
-  rstage<P, 0, false>(a, t, tw);
-  rrest<P, 1, 0, false>(a, t, sm, tw);
+  rload<P, 1, ZH>(a, t, ld);
+  rstage<P, 0, ZH>(a, t, tw);
+  rrest<P, 1, 0>(a, t, sm, tw);
   constexpr int RL = P::r[P::S - 1];
 #pragma unroll
   for (int b = 0; b < P::E / RL; ++b)
 #pragma unroll
     for (int q = 0; q < RL; ++q) sm(0, ppad(rout_pos<P, P::S - 1>(t, b, q))) = a[b * RL + q];
   __syncthreads();
-  const bool fy = ky > g.Ly / 2;
-  const int my = fy ? g.Ly - ky : ky;
   {
-    // thread -> (kzl fastest, kx); no division inside the loop
-    const int kzl = threadIdx.x % tz, kxs = blockDim.x / tz;
+    // thread -> (kzl fastest, mirror pair j): pair j holds kx = j and
+    // kx = LX - j, which read the same octant row (j = 0 and j = LX/2 stand
+    // alone), so each octant entry is loaded once for two points
+    const int kzl = threadIdx.x % tz, js = blockDim.x / tz;
     if (kzl < tzn) {
-      for (int kx = threadIdx.x / tz; kx < LX; kx += kxs) {
-        C* v = s + ppad(kx) * W + 3 * kzl;
-        C a0 = v[0], a1 = v[1], a2 = v[2];
-        tensor3(gh, g, LX, kx, my, fy, kz0 + kzl, gscale, a0, a1, a2);
-        v[0] = a0; v[1] = a1; v[2] = a2;
+      const int kz = kz0 + kzl;
+      const bool fy = ky > Ly / 2, fz = kz > Lz / 2;
+      const int my = fy ? Ly - ky : ky;
+      const int mz = fz ? Lz - kz : kz;
+      // entry scales at kx <= LX/2 (mirror signs of y and z, tensor scale)
+      const R sd = gscale;
+      const R sxy = fy ? -gscale : gscale, sxz = fz ? -gscale : gscale;
+      const R syz = (fy != fz) ? -gscale : gscale;
+      const C* __restrict__ q0 = gh + my * hz + mz;
+      for (int j = threadIdx.x / tz; j <= LX / 2; j += js) {
+        const C* q = q0 + j * (hy * hz);
+        const C gxx = cscale(__ldg(q), sd), gxy = cscale(__ldg(q + H), sxy), gxz = cscale(__ldg(q + 2 * H), sxz);
+        const C gyy = cscale(__ldg(q + 3 * H), sd), gyz = cscale(__ldg(q + 4 * H), syz);
+        const C gzz = cscale(__ldg(q + 5 * H), sd);
+        {
+          C* v = s + ppad(j) * W + 3 * kzl;
+          const C a0 = v[0], a1 = v[1], a2 = v[2];
+          v[0] = cadd(cadd(cmul(gxx, a0), cmul(gxy, a1)), cmul(gxz, a2));
+          v[1] = cadd(cadd(cmul(gxy, a0), cmul(gyy, a1)), cmul(gyz, a2));
+          v[2] = cadd(cadd(cmul(gxz, a0), cmul(gyz, a1)), cmul(gzz, a2));
+        }
+        if (j > 0 && j < LX / 2) {
+          // kx = LX - j: the x mirror flips the xy and xz entries
+          C* v = s + ppad(LX - j) * W + 3 * kzl;
+          const C a0 = v[0], a1 = v[1], a2 = v[2];
+          v[0] = csub(csub(cmul(gxx, a0), cmul(gxy, a1)), cmul(gxz, a2));
+          v[1] = cadd(csub(cmul(gyy, a1), cmul(gxy, a0)), cmul(gyz, a2));
+          v[2] = cadd(csub(cmul(gyz, a1), cmul(gxz, a0)), cmul(gzz, a2));
+        }
       }
     }
   }
@@ -271,16 +350,16 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3s(Geo g, const typena
   C* colo = opaque_ptr(col);
   C* swo = opaque_ptr(sw);
   auto smo = [&](int, int pp) -> C& { return swo[pp * W]; };
-  auto stf = [&](int, int pos, C v) { if (ok && pos < nx) colo[pos * rs] = v; };
+  auto stf = [&](int, int pos, C v) { if (ok && (DH || pos < nx)) __stcg(colo + pos * rs, cswap(v)); };
   constexpr int R0 = Q::r[0];
 #pragma unroll
   for (int b = 0; b < Q::E / R0; ++b)
 #pragma unroll
-    for (int m = 0; m < R0; ++m) a[b * R0 + m] = smo(0, ppad(rin_pos<Q, 0>(ti, b, m)));
+    for (int m = 0; m < R0; ++m) a[b * R0 + m] = cswap(smo(0, ppad(rin_pos<Q, 0>(ti, b, m))));
   __syncthreads();
-  rstage<Q, 0, true>(a, ti, tw);
-  rrest<Q, 1, 0, true>(a, ti, smo, tw);
-  rstore<Q, 1>(a, ti, stf);
+  rstage<Q, 0>(a, ti, tw);
+  rrest<Q, 1, 0>(a, ti, smo, tw);
+  rstore<Q, 1, DH>(a, ti, stf);
 }
 
 // ---------------------------------------------------------------------------
@@ -291,130 +370,181 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3s(Geo g, const typena
 //   MV_CONV_MASKED  y = mask*conv               (fft_matvec)
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
 // ---------------------------------------------------------------------------
-template <typename R, int LZ>
+template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int out_id,
-                                                            int mode, int cond, int nl) {
+                                                            int mode, int cond, int nl_) {
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
+  constexpr bool CUBE = NC > 0;
+  static_assert(!CUBE || LZ == 2 * NC, "cubic kernels need L = 2n");
+  constexpr int NLC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), NC * NC) : 1;
+  constexpr bool DH = CUBE && half_store_ok<P>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   const C* __restrict__ t1 = (const C*)S.t1;
+  const int nl = CUBE ? NLC : nl_;
+  const int nz = CUBE ? NC : g.nz;
+  const long long nlines = CUBE ? (long long)NC * NC : (long long)g.nx * g.ny;
   const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
   const int t = rest % SH::T, l = rest / SH::T;
-  const long long nlines = (long long)g.nx * g.ny;
   const long long line = (long long)blockIdx.x * nl + l;
-  const bool ok = line < nlines;
-  const int nz = g.nz;
+  const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
   const C* tl = t1 + line * (long long)LZ * 3 + c;
   C* sl = s + l * 3 * SH::LP + c;
-  auto ld = [&](int, int pos) -> C { return ok ? tl[pos * 3] : czero<C>(); };
+  auto ld = [&](int, int pos) -> C { return ok ? __ldcg(tl + pos * 3) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
-  auto stf = [&](int, int pos, C v) { if (pos < nz) sl[ppad(pos) * 3] = v; };
+  auto stf = [&](int, int pos, C v) { if (DH || pos < nz) sl[ppad(pos) * 3] = v; };
   C a[P::E];
-  rfft<P, 1, true>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
   __syncthreads();
-  // combine: consecutive threads take consecutive (site, component)
+  // combine: consecutive threads take consecutive (site, component); the
+  // (line, offset) split of idx advances without divisions
   const long long site_base = (long long)blockIdx.x * nl * nz;
-  const int nv = (int)min((long long)nl, nlines - (long long)blockIdx.x * nl) * nz * 3;
+  const int nlb = (int)min((long long)nl, nlines - (long long)blockIdx.x * nl);
+  const int per = nz * 3;
+  const int nv = nlb * per;
   const C* __restrict__ xg = (const C*)S.vec[in_id] + site_base * 3;
   C* __restrict__ yg = (C*)S.vec[out_id] + site_base * 3;
   const C* __restrict__ iag = (const C*)S.inva + site_base;
   const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site_base * 3 : nullptr;
-#pragma unroll 4
+  int ll = threadIdx.x / per, j = threadIdx.x - (threadIdx.x / per) * per;
   for (int idx = threadIdx.x; idx < nv; idx += blockDim.x) {
-    const int cc = idx % 3, sidx = idx / 3;
-    const int ll = sidx / nz, pos = sidx - ll * nz;
+    const int pos = j / 3, cc = j - 3 * pos;
     C v = s[ll * 3 * SH::LP + ppad(pos) * 3 + cc];
-    if (mode == MV_CONV) { yg[idx] = v; continue; }
-    const C a_ = iag[sidx];
-    const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
-    if (!msk) v = czero<C>();
-    if (mode == MV_CONV_MASKED) { yg[idx] = v; continue; }
-    C r = csub(cmul(a_, xg[idx]), v);
-    if (mode == MV_RESIDUAL) r = csub(bg[idx], r);
-    yg[idx] = r;
+    if (mode == MV_CONV) {
+      __stcg(yg + idx, v);
+    } else {
+      const C a_ = __ldg(iag + ll * nz + pos);     // shared by 3 lanes: keep it in L1
+      const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
+      if (!msk) v = czero<C>();
+      if (mode == MV_CONV_MASKED) {
+        __stcg(yg + idx, v);
+      } else {
+        C r = csub(cmul(a_, __ldcg(xg + idx)), v);
+        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + idx), r);
+        __stcg(yg + idx, r);
+      }
+    }
+    j += blockDim.x;
+    while (j >= per) { j -= per; ++ll; }
   }
 }
 
 // ---------------------------------------------------------------------------
 // host dispatch over the compiled lengths
 // ---------------------------------------------------------------------------
-template <typename R> struct MvKernels {
+template <typename R> struct MvSet {
   typedef typename CT<R>::T C;
   typedef void (*P1)(Geo, const C*, InstState*, const int*, int, int, int);
   typedef void (*PY)(Geo, const C*, InstState*, const int*, int, int, int);
   typedef void (*P3)(Geo, const C*, InstState*, const int*, int, int, int, R);
   typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int);
-  static P1 p1(int L) {
-    switch (L) {
-#define DDA_K(n) case n: return k_mv_pass1<R, n>;
-      DDA_FFT_SIZES(DDA_K)
-#undef DDA_K
-    }
-    return nullptr;
-  }
-  static PY py(int L, bool inv) {
-    switch (L) {
-#define DDA_K(n) case n: return inv ? (PY)k_mv_pass_y<R, true, n> : (PY)k_mv_pass_y<R, false, n>;
-      DDA_FFT_SIZES(DDA_K)
-#undef DDA_K
-    }
-    return nullptr;
-  }
-  static P3 p3(int L, int v) {
-    switch (L) {
-#define DDA_K(n)                                                           \
-  case n:                                                                  \
-    return v == 1 ? (P3)k_mv_pass3r<R, n, 1>                               \
-                  : (v == 2 ? (P3)k_mv_pass3s<R, n, 2> : (P3)k_mv_pass3s<R, n, 0>);
-      DDA_FFT_SIZES(DDA_K)
-#undef DDA_K
-    }
-    return nullptr;
-  }
-  static P5 p5(int L) {
-    switch (L) {
-#define DDA_K(n) case n: return k_mv_pass5<R, n>;
-      DDA_FFT_SIZES(DDA_K)
-#undef DDA_K
-    }
-    return nullptr;
-  }
+  P1 k1 = nullptr; PY k2 = nullptr; P3 k3 = nullptr; PY k4 = nullptr; P5 k5 = nullptr;
+  // tile sizes the kernels were compiled for (cubic set only; 0 = any)
+  int nl = 0, tz2 = 0, tz3 = 0;
 };
+
+// General kernels (sizes from Geo), defined with the instantiations.
+template <typename R> bool mv_general_set(int Lx, int Ly, int Lz, int p3var, MvSet<R>& out);
+// Cubic kernels for the FFT length L = 2n (box n^3): complex64 with pass-3
+// variant 0, complex128 with variant 2 (matvec_cube_f32.cu / _f64.cu).
+template <typename R> bool mv_cube_set(int L, int p3var, MvSet<R>& out);
+template <> bool mv_general_set<float>(int, int, int, int, MvSet<float>&);
+template <> bool mv_general_set<double>(int, int, int, int, MvSet<double>&);
+template <> bool mv_cube_set<float>(int, int, MvSet<float>&);
+template <> bool mv_cube_set<double>(int, int, MvSet<double>&);
+
+template <typename R>
+bool mv_general_set_impl(int Lx, int Ly, int Lz, int p3var, MvSet<R>& o) {
+  typedef MvSet<R> M;
+  switch (Lz) {
+#define DDA_K(n) case n: o.k1 = k_mv_pass1<R, n, 0>; o.k5 = k_mv_pass5<R, n, 0>; break;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+    default: return false;
+  }
+  switch (Ly) {
+#define DDA_K(n) case n: o.k2 = (typename M::PY)k_mv_pass_y<R, false, n, 0>; o.k4 = (typename M::PY)k_mv_pass_y<R, true, n, 0>; break;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+    default: return false;
+  }
+  switch (Lx) {
+#define DDA_K(n)                                                                                   \
+  case n:                                                                                          \
+    o.k3 = p3var == 1 ? (typename M::P3)k_mv_pass3r<R, n, 1>                                       \
+                      : (p3var == 2 ? (typename M::P3)k_mv_pass3s<R, n, 2, 0>                      \
+                                    : (typename M::P3)k_mv_pass3s<R, n, 0, 0>);                    \
+    break;
+    DDA_FFT_SIZES(DDA_K)
+#undef DDA_K
+    default: return false;
+  }
+  return true;
+}
+
+template <typename R, int L, int V>
+void mv_cube_fill(MvSet<R>& o) {
+  typedef MvSet<R> M;
+  constexpr int NC = L / 2;
+  o.k1 = k_mv_pass1<R, L, NC>;
+  o.k2 = (typename M::PY)k_mv_pass_y<R, false, L, NC>;
+  o.k3 = (typename M::P3)k_mv_pass3s<R, L, V, NC>;
+  o.k4 = (typename M::PY)k_mv_pass_y<R, true, L, NC>;
+  o.k5 = k_mv_pass5<R, L, NC>;
+  o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
+  o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
+  o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+}
+
+// The kernel set for a geometry: the cubic one when the box is n^3 on a
+// (2n)^3 grid and its tile sizes match the configuration, else the general.
+template <typename R>
+bool mv_select(const Geo& g, const PassCfg& pc, MvSet<R>& o) {
+  const bool cube = g.nx == g.ny && g.ny == g.nz && g.Lx == g.Ly && g.Ly == g.Lz && g.Lx == 2 * g.nx;
+  if (cube && !getenv("DDA_NO_CUBE") && mv_cube_set<R>(g.Lx, pc.p3var, o) && o.nl == pc.nl &&
+      o.tz2 == pc.tz2 && o.tz3 == pc.tz3)
+    return true;
+  o = MvSet<R>();
+  return mv_general_set<R>(g.Lx, g.Ly, g.Lz, pc.p3var, o);
+}
+
+// Raise the dynamic shared-memory limit of each kernel once per device.
+cudaError_t mv_prepare(const void* const* ks, int n);
+
+template <typename R>
+cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
+                          const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
+                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
+  const void* ks[5] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
+                       (const void*)k.k5};
+  cudaError_t e = mv_prepare(ks, 5);
+  if (e != cudaSuccess) return e;
+  k.k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl);
+  k.k2<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
+  k.k3<<<dim3((unsigned)pc.grid3, nb), pc.th3, pc.smem3, s>>>(g, twx, st, act, cond, pc.tz3, pc.ntz3, (R)gscale);
+  k.k4<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
+  k.k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl);
+  note_launch(s, 5);
+  return cudaGetLastError();
+}
 
 template <typename R>
 cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                                int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
   typedef typename CT<R>::T C;
   constexpr bool dbl = sizeof(R) == 8;
-  auto k1 = MvKernels<R>::p1(g.Lz);
-  auto k2 = MvKernels<R>::py(g.Ly, false);
-  auto k3 = MvKernels<R>::p3(g.Lx, pc.p3var);
-  auto k4 = MvKernels<R>::py(g.Ly, true);
-  auto k5 = MvKernels<R>::p5(g.Lz);
-  if (!k1 || !k2 || !k3 || !k4 || !k5) return cudaErrorInvalidValue;
+  MvSet<R> k;
+  if (!mv_select<R>(g, pc, k)) return cudaErrorInvalidValue;
   const C* twx = (const C*)ctx.twiddles(g.Lx, dbl);
   const C* twy = (const C*)ctx.twiddles(g.Ly, dbl);
   const C* twz = (const C*)ctx.twiddles(g.Lz, dbl);
   if (!twx || !twy || !twz) return cudaErrorMemoryAllocation;
-  const int mx = 200 * 1024;
-  cudaError_t e;
-  const void* ks[5] = {(const void*)k1, (const void*)k2, (const void*)k3, (const void*)k4, (const void*)k5};
-  for (int i = 0; i < 5; ++i) {
-    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, mx))) return e;
-    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
-  }
-  k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl);
-  k2<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
-  k3<<<dim3((unsigned)pc.grid3, nb), pc.th3, pc.smem3, s>>>(g, twx, st, act, cond, pc.tz3, pc.ntz3, (R)gscale);
-  k4<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
-  k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl);
-  note_launch(s, 5);
-  return cudaGetLastError();
+  return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, out_id, mode, cond, gscale, s);
 }
 
 // Same five launches with caller-provided twiddle tables (used by the
@@ -423,31 +553,15 @@ template <typename R>
 cudaError_t launch_matvec_tw_impl(const Geo& g, const PassCfg& pc, InstState* st, const typename CT<R>::T* twx,
                                   const typename CT<R>::T* twy, const typename CT<R>::T* twz, int in_id,
                                   int out_id, int mode, double gscale, cudaStream_t s) {
-  auto k1 = MvKernels<R>::p1(g.Lz);
-  auto k2 = MvKernels<R>::py(g.Ly, false);
-  auto k3 = MvKernels<R>::p3(g.Lx, pc.p3var);
-  auto k4 = MvKernels<R>::py(g.Ly, true);
-  auto k5 = MvKernels<R>::p5(g.Lz);
-  if (!k1 || !k2 || !k3 || !k4 || !k5) return cudaErrorInvalidValue;
-  cudaError_t e;
-  const void* ks[5] = {(const void*)k1, (const void*)k2, (const void*)k3, (const void*)k4, (const void*)k5};
-  for (int i = 0; i < 5; ++i) {
-    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
-    if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
-  }
-  k1<<<dim3((unsigned)pc.grid1, 1), pc.th1, pc.smem1, s>>>(g, twz, st, nullptr, in_id, C_ALWAYS, pc.nl);
-  k2<<<dim3((unsigned)pc.grid2, 1), pc.th2, pc.smem2, s>>>(g, twy, st, nullptr, C_ALWAYS, pc.tz2, pc.ntz2);
-  k3<<<dim3((unsigned)pc.grid3, 1), pc.th3, pc.smem3, s>>>(g, twx, st, nullptr, C_ALWAYS, pc.tz3, pc.ntz3, (R)gscale);
-  k4<<<dim3((unsigned)pc.grid2, 1), pc.th2, pc.smem2, s>>>(g, twy, st, nullptr, C_ALWAYS, pc.tz2, pc.ntz2);
-  k5<<<dim3((unsigned)pc.grid1, 1), pc.th1, pc.smem1, s>>>(g, twz, st, nullptr, in_id, out_id, mode, C_ALWAYS, pc.nl);
-  note_launch(s, 5);
-  return cudaGetLastError();
+  MvSet<R> k;
+  if (!mv_select<R>(g, pc, k)) return cudaErrorInvalidValue;
+  return launch_mv_set<R>(k, g, pc, st, nullptr, 1, twx, twy, twz, in_id, out_id, mode, C_ALWAYS, gscale, s);
 }
 
 // Tile shapes: about 128 (complex64) or 64 (complex128) transforms' worth of
 // threads per CTA, at most one tile dimension's extent.
 template <typename R>
-static int lanes() { return sizeof(R) == 4 ? 128 : 64; }
+static int lanes() { return mv_lanes<R>(); }
 
 template <typename R>
 static bool tile_dims(int L, int& T, int& LP) {
