@@ -116,6 +116,9 @@ cudaError_t launch_matvec_tw(const Geo& g, const PassCfg& pc, InstState* st, con
 // Batched GPBiCGSTAB kernels (krylov.cu); RB CTAs per instance.
 struct KrylovLaunch {
   InstState* st; const int* act; int nb; double* red; unsigned* cnt; long long n3; int RB;
+  // graph conditional handles set by the control code (0: none): the
+  // true-residual matvec at i == 1 and the reset branch's residual matvec
+  unsigned long long cond_true = 0, cond_reset = 0;
 };
 template <typename R> void launch_init(const KrylovLaunch& k, cudaStream_t s);
 template <typename R> void launch_alpha(const KrylovLaunch& k, cudaStream_t s);
@@ -128,6 +131,12 @@ template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s);
 // One GPBiCGSTAB iteration for every instance of a workspace (solver.cu).
 template <typename R>
 cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s);
+// The iteration as a CUDA graph whose two residual matvecs (i == 1, resets)
+// sit in conditional nodes the control kernels switch on; falls back to the
+// plain captured sequence where conditional nodes are unavailable.
+template <typename R>
+cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s, cudaGraph_t* out,
+                              long long* kernels);
 
 template <typename R>
 int solve_batch(Ctx& c, const Geo& g, double gscale, const struct dda_instance* inst, int nb, double target,

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
 // u, z, r, x updates (Gpbicgstab.py:1038-1057) and ||r||^2, <rhat, r>
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
-                                              int RB) {
+                                              int RB, unsigned long long cond_true, unsigned long long cond_reset) {
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -254,13 +254,15 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
     S.cur_x = nxt;
     S.vec[V_X] = S.vec[V_XA + nxt];
     if (!S.flag_true_res) ctrl_check(S, tot[0], make_double2(tot[1], tot[2]));
+    if (cond_true && S.flag_true_res && !S.done) cudaGraphSetConditional(cond_true, 1);
+    if (cond_reset && S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
   }
 }
 
 // ||r||^2, <rhat, r> after the i == 1 true residual (Gpbicgstab.py:1059-1076)
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
-                                              int RB) {
+                                              int RB, unsigned long long cond_reset) {
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -275,8 +277,10 @@ __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, dou
     acc[2] += (double)h.x * rn.y - (double)h.y * rn.x;
   }
   double tot[3];
-  if (reduce_last<3>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0)
+  if (reduce_last<3>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     ctrl_check(S, tot[0], make_double2(tot[1], tot[2]));
+    if (cond_reset && S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
+  }
 }
 
 // end of iteration: reset copies or the w / p updates; buffer swap; i += 1
@@ -342,11 +346,11 @@ template <typename R> void launch_zeta(const KrylovLaunch& k, cudaStream_t s) {
   note_launch(s, 1);
 }
 template <typename R> void launch_uzrx(const KrylovLaunch& k, cudaStream_t s) {
-  k_uzrx<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB);
+  k_uzrx<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_true, k.cond_reset);
   note_launch(s, 1);
 }
 template <typename R> void launch_norm(const KrylovLaunch& k, cudaStream_t s) {
-  k_norm<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB);
+  k_norm<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_reset);
   note_launch(s, 1);
 }
 template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s) {

@@ -135,19 +135,15 @@ int dda_slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx
     const bool dbl = precision == DDA_PREC_C128;
     ctx->c.twiddles(Lx, dbl); ctx->c.twiddles(Ly, dbl); ctx->c.twiddles(Lz, dbl);
     if (precision == DDA_PREC_MIXED) { ctx->c.twiddles(Lx, true); ctx->c.twiddles(Ly, true); ctx->c.twiddles(Lz, true); }
-    cudaGraph_t graph;
-    cudaError_t e1 = cudaStreamBeginCapture(p->s, cudaStreamCaptureModeThreadLocal);
-    cudaError_t e2 = e1 == cudaSuccess ? (dbl ? enqueue_iteration<double>(ctx->c, p->w, gscale, p->s)
-                                              : enqueue_iteration<float>(ctx->c, p->w, gscale, p->s))
-                                       : e1;
-    cudaError_t e3 = e1 == cudaSuccess ? cudaStreamEndCapture(p->s, &graph) : e1;
-    if (e2 != cudaSuccess || e3 != cudaSuccess) {
-      set_error(std::string("slot pool graph capture: ") + cudaGetErrorString(e2 != cudaSuccess ? e2 : e3));
+    cudaGraph_t graph = nullptr;
+    long long nk = 0;
+    cudaError_t e1 = dbl ? capture_iteration<double>(ctx->c, p->w, gscale, p->s, &graph, &nk)
+                         : capture_iteration<float>(ctx->c, p->w, gscale, p->s, &graph, &nk);
+    if (e1 != cudaSuccess) {
+      set_error(std::string("slot pool graph capture: ") + cudaGetErrorString(e1));
       rc = DDA_ERR_CUDA;
     } else {
-      size_t nn = 0;
-      cudaGraphGetNodes(graph, nullptr, &nn);
-      p->w.graph_kernels = (long long)nn;
+      p->w.graph_kernels = nk;
       if (cudaGraphInstantiate(&p->w.gexec, graph, 0) != cudaSuccess) {
         set_error("slot pool graph instantiate failed");
         rc = DDA_ERR_CUDA;

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <vector>
 #include <cstring>
 #include <string>
 
@@ -151,23 +152,129 @@ cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s)
 template cudaError_t enqueue_iteration<float>(Ctx&, BatchWs&, double, cudaStream_t);
 template cudaError_t enqueue_iteration<double>(Ctx&, BatchWs&, double, cudaStream_t);
 
+namespace {
+// Capture launches issued by `fn` on stream s into graph G after `deps`;
+// returns the capture's final dependencies (the segment's sink nodes).
+template <class F>
+cudaError_t capture_segment(cudaStream_t s, cudaGraph_t G, const std::vector<cudaGraphNode_t>& deps,
+                            std::vector<cudaGraphNode_t>& sinks, F fn) {
+  cudaError_t e = cudaStreamBeginCaptureToGraph(s, G, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                                cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t ef = fn();
+  cudaStreamCaptureStatus cs;
+  const cudaGraphNode_t* d = nullptr;
+  size_t nd = 0;
+  cudaError_t ei = cudaStreamGetCaptureInfo(s, &cs, nullptr, nullptr, &d, &nd);
+  if (ei == cudaSuccess) sinks.assign(d, d + nd);
+  cudaGraph_t g2 = nullptr;
+  cudaError_t ee = cudaStreamEndCapture(s, &g2);
+  return ef != cudaSuccess ? ef : (ei != cudaSuccess ? ei : ee);
+}
+
+// IF node on handle h after `deps`; its body is captured from `fn`.
+template <class F>
+cudaError_t add_if(cudaStream_t s, cudaGraph_t G, cudaGraphConditionalHandle h,
+                   const std::vector<cudaGraphNode_t>& deps, cudaGraphNode_t* node, F fn) {
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaError_t e = cudaGraphAddNode(node, G, deps.data(), deps.size(), &cp);
+  if (e != cudaSuccess) return e;
+  std::vector<cudaGraphNode_t> none, sinks;
+  return capture_segment(s, cp.conditional.phGraph_out[0], none, sinks, fn);
+}
+}  // namespace
+
+template <typename R>
+cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s, cudaGraph_t* out,
+                              long long* kernels) {
+  *out = nullptr;
+  cudaGraph_t G = nullptr;
+  cudaError_t e = cudaGraphCreate(&G, 0);
+  if (e != cudaSuccess) return e;
+  cudaGraphConditionalHandle hT = 0, hR = 0;
+  bool cond = !getenv("DDA_NO_GRAPH_COND") &&
+              cudaGraphConditionalHandleCreate(&hT, G, 0, cudaGraphCondAssignDefault) == cudaSuccess &&
+              cudaGraphConditionalHandleCreate(&hR, G, 0, cudaGraphCondAssignDefault) == cudaSuccess;
+  if (cond) {
+    KrylovLaunch k{w.d_st, nullptr, w.nb, w.red, w.cnt, (long long)w.n3, w.RB};
+    k.cond_true = hT;
+    k.cond_reset = hR;
+    std::vector<cudaGraphNode_t> none, d1, d2, d3;
+    cudaGraphNode_t n1 = nullptr, n2 = nullptr;
+    e = capture_segment(s, G, none, d1, [&]() -> cudaError_t {
+      cudaError_t r;
+      if ((r = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return r;
+      launch_alpha<R>(k, s);
+      launch_sy<R>(k, s);
+      if ((r = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return r;
+      launch_zeta<R>(k, s);
+      launch_uzrx<R>(k, s);
+      return cudaGetLastError();
+    });
+    if (e == cudaSuccess)
+      e = add_if(s, G, hT, d1, &n1, [&]() -> cudaError_t {
+        return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s);
+      });
+    if (e == cudaSuccess)
+      e = capture_segment(s, G, std::vector<cudaGraphNode_t>{n1}, d2, [&]() -> cudaError_t {
+        launch_norm<R>(k, s);
+        return cudaGetLastError();
+      });
+    if (e == cudaSuccess)
+      e = add_if(s, G, hR, d2, &n2, [&]() -> cudaError_t {
+        return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s);
+      });
+    if (e == cudaSuccess)
+      e = capture_segment(s, G, std::vector<cudaGraphNode_t>{n2}, d3, [&]() -> cudaError_t {
+        launch_fin<R>(k, s);
+        return cudaGetLastError();
+      });
+    if (e == cudaSuccess) {
+      *out = G;
+      *kernels = 5 + 5 + 6;      // kernels every launch runs (conditional bodies excluded)
+      return cudaSuccess;
+    }
+    cudaGetLastError();
+  }
+  // plain capture: both residual matvecs are launched every iteration and
+  // return at once when no instance needs them
+  cudaGraphDestroy(G);
+  G = nullptr;
+  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+  cudaError_t e1 = enqueue_iteration<R>(c, w, gscale, s);
+  e = cudaStreamEndCapture(s, &G);
+  if (e1 != cudaSuccess || e != cudaSuccess) {
+    if (G) cudaGraphDestroy(G);
+    return e1 != cudaSuccess ? e1 : e;
+  }
+  size_t nn = 0;
+  cudaGraphGetNodes(G, nullptr, &nn);
+  *kernels = (long long)nn;
+  *out = G;
+  return cudaSuccess;
+}
+
+template cudaError_t capture_iteration<float>(Ctx&, BatchWs&, double, cudaStream_t, cudaGraph_t*, long long*);
+template cudaError_t capture_iteration<double>(Ctx&, BatchWs&, double, cudaStream_t, cudaGraph_t*, long long*);
+
 template <typename R>
 static int build_graph(Ctx& c, BatchWs& w, double gscale) {
   if (w.gexec && w.graph_gscale == gscale) return DDA_OK;
   if (w.gexec) { cudaGraphExecDestroy(w.gexec); w.gexec = nullptr; }
   // make sure lazily created resources exist before capture
   c.twiddles(w.g.Lx, sizeof(R) == 8); c.twiddles(w.g.Ly, sizeof(R) == 8); c.twiddles(w.g.Lz, sizeof(R) == 8);
-  cudaGraph_t graph;
-  DDA_CUDA_OK(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = enqueue_iteration<R>(c, w, gscale, c.stream);
-  cudaError_t e2 = cudaStreamEndCapture(c.stream, &graph);
-  if (e != cudaSuccess || e2 != cudaSuccess) {
-    set_error(std::string("graph capture: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+  cudaGraph_t graph = nullptr;
+  long long nk = 0;
+  cudaError_t e = capture_iteration<R>(c, w, gscale, c.stream, &graph, &nk);
+  if (e != cudaSuccess) {
+    set_error(std::string("graph capture: ") + cudaGetErrorString(e));
     return DDA_ERR_CUDA;
   }
-  size_t nnodes = 0;
-  cudaGraphGetNodes(graph, nullptr, &nnodes);
-  w.graph_kernels = (long long)nnodes;
+  w.graph_kernels = nk;
   e = cudaGraphInstantiate(&w.gexec, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) { set_error(std::string("graph instantiate: ") + cudaGetErrorString(e)); return DDA_ERR_CUDA; }
