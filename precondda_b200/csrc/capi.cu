@@ -91,6 +91,16 @@ int dda_ctx_create(int device, dda_ctx** out) {
     delete c;
     return DDA_ERR_CUDA;
   }
+  // transient buffers (Green-build transforms, voxeliser shape lists) come
+  // from the device's stream-ordered pool; keep freed blocks in the pool
+  // instead of unmapping them at every synchronisation (dda_ctx_trim
+  // returns them)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   *out = c;
   return DDA_OK;
 }
@@ -112,6 +122,9 @@ int dda_ctx_trim(dda_ctx* ctx) {
   if (rc) return rc;
   cudaStreamSynchronize(ctx->c.stream);
   ctx->c.trim();
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, ctx->c.device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
   return DDA_OK;
 }
 

@@ -84,14 +84,14 @@ __global__ void __launch_bounds__(KNT) k_init(InstState* st, const int* act, dou
   C* zs[7] = {(C*)S.vec[V_V], (C*)S.vec[V_T], (C*)S.vec[V_S], (C*)S.vec[V_SPREV], (C*)S.vec[V_U], (C*)S.vec[V_Z],
               (C*)S.vec[V_W]};
   double acc[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C bv = b[i];
     r[i] = bv; rh[i] = bv; p[i] = bv;
     xa[i] = czero<C>();
 #pragma unroll
     for (int j = 0; j < 7; ++j) zs[j][i] = czero<C>();
     acc[0] += (double)bv.x * bv.x + (double)bv.y * bv.y;
-  }
+  });
   double tot[1];
   if (reduce_last<1>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     const double nrm = sqrt(tot[0]);
@@ -120,11 +120,11 @@ __global__ void __launch_bounds__(KNT) k_alpha(InstState* st, const int* act, do
   const C* __restrict__ rh = (const C*)S.vec[V_RHAT];
   const C* __restrict__ v = (const C*)S.vec[V_V];
   double acc[2] = {0.0, 0.0};
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C a = rh[i], b = v[i];
     acc[0] += (double)a.x * b.x + (double)a.y * b.y;
     acc[1] += (double)a.x * b.y - (double)a.y * b.x;
-  }
+  });
   double tot[2];
   if (reduce_last<2>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0)
     S.alpha = zdiv(S.rho1, make_double2(tot[0], tot[1]));
@@ -144,11 +144,11 @@ __global__ void __launch_bounds__(KNT) k_sy(InstState* st, const int* act, long 
   C* __restrict__ s = (C*)S.vec[V_S];
   C* __restrict__ y = (C*)S.vec[V_Y];
   const C al = tocr<C>(S.alpha);
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
     const C sv = csub(r[i], cmul(al, v[i]));
     s[i] = sv;
     y[i] = csub(csub(sp[i], sv), cmul(al, w[i]));
-  }
+  });
 }
 
 // zeta, eta  (Gpbicgstab.py:1038-1052, calculate_zeta_eta_twostep :239-380)
@@ -163,18 +163,18 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
   const C* __restrict__ t = (const C*)S.vec[V_T];
   const C* __restrict__ s = (const C*)S.vec[V_S];
   const C* __restrict__ y = (const C*)S.vec[V_Y];
-  double acc[KRED];
+  double acc[8];
 #pragma unroll
-  for (int k = 0; k < KRED; ++k) acc[k] = 0.0;
+  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
   if (first) {
-    for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C tv = t[i], sv = s[i];
       acc[0] += (double)tv.x * tv.x + (double)tv.y * tv.y;            // <t,t>
       acc[1] += (double)tv.x * sv.x + (double)tv.y * sv.y;            // <t,s>
       acc[2] += (double)tv.x * sv.y - (double)tv.y * sv.x;
-    }
+    });
   } else {
-    for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C tv = t[i], sv = s[i], yv = y[i];
       acc[0] += (double)yv.x * yv.x + (double)yv.y * yv.y;            // yy
       acc[1] += (double)tv.x * tv.x + (double)tv.y * tv.y;            // tt
@@ -184,10 +184,10 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
       acc[5] += (double)yv.x * sv.y - (double)yv.y * sv.x;
       acc[6] += (double)tv.x * sv.x + (double)tv.y * sv.y;            // ts
       acc[7] += (double)tv.x * sv.y - (double)tv.y * sv.x;
-    }
+    });
   }
-  double tot[KRED];
-  if (reduce_last<KRED>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
+  double tot[8];
+  if (reduce_last<8>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     if (first) {
       S.zeta = zdiv(make_double2(tot[1], tot[2]), make_double2(tot[0], 0.0));
       S.eta = make_double2(0.0, 0.0);
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
   C* __restrict__ z = (C*)S.vec[V_Z];
   const C ze = tocr<C>(S.zeta), et = tocr<C>(S.eta), al = tocr<C>(S.alpha), be = tocr<C>(S.beta);
   double acc[3] = {0.0, 0.0, 0.0};
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     C un, zn, rn;
     if (first) {
       un = cmul(ze, v[i]);
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
     acc[0] += (double)rn.x * rn.x + (double)rn.y * rn.y;
     acc[1] += (double)h.x * rn.x + (double)h.y * rn.y;
     acc[2] += (double)h.x * rn.y - (double)h.y * rn.x;
-  }
+  });
   double tot[3];
   if (reduce_last<3>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     S.cur_x = nxt;
@@ -270,12 +270,12 @@ __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, dou
   const C* __restrict__ r = (const C*)S.vec[V_R];
   const C* __restrict__ rh = (const C*)S.vec[V_RHAT];
   double acc[3] = {0.0, 0.0, 0.0};
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C rn = r[i], h = rh[i];
     acc[0] += (double)rn.x * rn.x + (double)rn.y * rn.y;
     acc[1] += (double)h.x * rn.x + (double)h.y * rn.y;
     acc[2] += (double)h.x * rn.y - (double)h.y * rn.x;
-  }
+  });
   double tot[3];
   if (reduce_last<3>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     ctrl_check(S, tot[0], make_double2(tot[1], tot[2]));
@@ -296,20 +296,20 @@ __global__ void __launch_bounds__(KNT) k_fin(InstState* st, const int* act, unsi
   C* __restrict__ p = (C*)S.vec[V_P];
   if (reset) {
     C* __restrict__ rh = (C*)S.vec[V_RHAT];
-    for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C rv = r[i];
       rh[i] = rv; p[i] = rv;
-    }
+    });
   } else {
     const C* __restrict__ t = (const C*)S.vec[V_T];
     const C* __restrict__ v = (const C*)S.vec[V_V];
     const C* __restrict__ u = (const C*)S.vec[V_U];
     C* __restrict__ w = (C*)S.vec[V_W];
     const C be = tocr<C>(S.beta);
-    for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       w[i] = cadd(t[i], cmul(be, v[i]));
       p[i] = cadd(r[i], cmul(be, csub(p[i], u[i])));
-    }
+    });
   }
   if (finish_last(cnt, inst, RB) && threadIdx.x == 0) {
     void* tmp = S.vec[V_S]; S.vec[V_S] = S.vec[V_SPREV]; S.vec[V_SPREV] = tmp;

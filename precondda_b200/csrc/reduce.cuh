@@ -11,6 +11,21 @@ constexpr int KNT = 256;
 constexpr int KNW = KNT / 32;
 constexpr int KRED = 12;   // reduction slots per CTA (6 complex dots)
 
+// Grid-stride loop over [start, n) that handles U elements per trip with
+// their loads issued together (U independent memory requests in flight per
+// thread), then the remainder one by one.  The element order of each
+// thread's work is fixed, so reductions stay deterministic.
+constexpr int KU = 4;
+template <int U, class F>
+__device__ __forceinline__ void grid_loop(long long n, long long start, long long stride, F&& f) {
+  long long i = start;
+  for (; i + (U - 1) * stride < n; i += U * stride) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) f(i + u * stride);
+  }
+  for (; i < n; i += stride) f(i);
+}
+
 __device__ __forceinline__ int kinst(const int* act) { return act ? act[blockIdx.y] : (int)blockIdx.y; }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -21,26 +36,34 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Block-reduce K doubles, publish per-CTA partials, and return true in the
 // last CTA of the instance, with `tot` holding the fixed-order grid total.
+// Both stages spread their loads over the CTA's threads so that no thread
+// walks a long dependent chain of L2 reads.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double (&sh)[K][KNW], double (&out)[K]) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const double s = warp_sum(v[k]);
+    if (lane == 0) sh[k][wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = warp_sum(lane < KNW ? sh[k][lane] : 0.0);
+  }
+}
+
 template <int K>
 __device__ __forceinline__ bool reduce_last(double (&v)[K], double (&tot)[K], double* red, unsigned* cnt, int inst,
                                             int RB) {
   __shared__ double sh[K][KNW];
   __shared__ bool last;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    double s = warp_sum(v[k]);
-    if (lane == 0) sh[k][wid] = s;
-  }
-  __syncthreads();
+  double part[K];
+  block_sum<K>(v, sh, part);
   if (threadIdx.x == 0) {
     double* dst = red + ((size_t)inst * RB + blockIdx.x) * KRED;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double s = 0.0;
-      for (int w = 0; w < KNW; ++w) s += sh[k][w];
-      dst[k] = s;
-    }
+    for (int k = 0; k < K; ++k) dst[k] = part[k];
     __threadfence();
     const unsigned prev = atomicAdd(&cnt[inst], 1u);
     last = (prev == (unsigned)RB - 1u);
@@ -48,17 +71,20 @@ __device__ __forceinline__ bool reduce_last(double (&v)[K], double (&tot)[K], do
   __syncthreads();
   if (!last) return false;
   __threadfence();
-  if (wid == 0) {
-    const double* src = red + (size_t)inst * RB * KRED;
+  // every thread gathers a fixed subset of the CTAs' partials
+  const double* src = red + (size_t)inst * RB * KRED;
+  double g[K];
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      double s = 0.0;
-      for (int b = lane; b < RB; b += 32) s += __ldcg(src + (size_t)b * KRED + k);
-      s = warp_sum(s);
-      tot[k] = s;
-    }
-    if (lane == 0) cnt[inst] = 0u;
+  for (int k = 0; k < K; ++k) g[k] = 0.0;
+  for (int b = threadIdx.x; b < RB; b += KNT) {
+    double t[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) t[k] = __ldcg(src + (size_t)b * KRED + k);
+#pragma unroll
+    for (int k = 0; k < K; ++k) g[k] += t[k];
   }
+  block_sum<K>(g, sh, tot);
+  if (threadIdx.x == 0) cnt[inst] = 0u;
   return true;   // only warp 0 holds valid totals
 }
 

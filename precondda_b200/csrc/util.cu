@@ -17,11 +17,11 @@ __global__ void __launch_bounds__(KNT) k_make_b(InstState* st, const int* act, l
   const C* __restrict__ e = (const C*)S.vec[src_id];
   const C* __restrict__ ia = (const C*)S.inva;
   C* __restrict__ b = (C*)S.vec[dst_id];
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < nsite * 3; i += (long long)gridDim.x * KNT) {
+  grid_loop<KU>(nsite * 3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
     const C a = ia[i / 3];
     const bool m = (a.x != (R)0) || (a.y != (R)0);
     b[i] = m ? e[i] : czero<C>();
-  }
+  });
 }
 
 // dst(c64).vec[did] = (complex64) src(c128).vec[sid]
@@ -53,12 +53,12 @@ __global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const 
   const float2* __restrict__ e = sol64(S);
   if (!e) return;
   double2* __restrict__ x = (double2*)st128[j].vec[xid];
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
     const float2 v = e[i];
     double2 a = x[i];
     a.x += (double)v.x; a.y += (double)v.y;
     x[i] = a;
-  }
+  });
 }
 
 // out[inst] = ||vec[id]||^2 (FP64, deterministic)
@@ -71,10 +71,10 @@ __global__ void __launch_bounds__(KNT) k_norm2(InstState* st, const int* act, in
   if (!S.active) return;
   const C* __restrict__ v = (const C*)S.vec[id];
   double acc[1] = {0.0};
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)RB * KNT) {
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C a = v[i];
     acc[0] += (double)a.x * a.x + (double)a.y * a.y;
-  }
+  });
   double tot[1];
   if (reduce_last<1>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) out[inst] = tot[0];
 }
