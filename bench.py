@@ -401,6 +401,247 @@ def run_profile_matvec(args, local):
     print(json.dumps(out))
 
 
+# --------------------------------------------------------------------------
+# other workloads (one JSON line each; the default run is the sphere64 line)
+# --------------------------------------------------------------------------
+def _line(metric, value, unit, args, ws, t, config, dtype="c64+fp64", **extra):
+    out = {"metric": metric, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 * t / max(args.steps, 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded lattices; no dataset)", "config": config}
+    out.update(extra)
+    return out
+
+
+def run_large128(args, ws, rank, local):
+    """Large single solve: 128^3 box, rotated ellipsoid with semi-axes
+    (64, 48, 40) d, m from the seed, |m|kd = 0.6; mixed precision vs plain
+    complex128 at tol 1e-6 and the C_ext / C_abs error of each against a
+    complex128 solve to 1e-10."""
+    import torch
+    import precondda_b200 as P
+    from precondda_b200 import _lib as L
+    from precondda_b200.workloads import ellipsoid128_spec, build_geometry
+    dev = torch.device("cuda", local)
+    spec = ellipsoid128_spec(seed=3 + rank)
+    ia, k, d, Es = build_geometry(spec, dev)
+    op = P.DDAOperator(ia, k, d, dtype=torch.complex128, device=dev, with_twin=True)
+    E = Es[0]
+
+    def solve(prec, tol=TOL):
+        return P.solve_many([op], [E], tol=tol, max_iter=4000, ratio=RATIO, precision=prec, inner_tol=INNER_TOL)
+
+    for _ in range(max(args.warmup, 1)):
+        solve("mixed")
+    torch.cuda.synchronize()
+    lc0 = L.lib().dda_kernel_launches()
+    stream = torch.cuda.current_stream(dev)
+    with ClockSampler(dev.index) as clk:
+        barrier(ws)
+        e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            Pm, im = solve("mixed")
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = L.lib().dda_kernel_launches() - lc0
+    t = max_over_ranks(ws, e0.elapsed_time(e1) / 1e3)
+    value = args.steps * ws / t
+    if rank != 0:
+        return
+    g0 = torch.cuda.Event(enable_timing=True); g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    Pp, ip = solve("c128")
+    g1.record(stream)
+    torch.cuda.synchronize()
+    plain = 1.0 / (g0.elapsed_time(g1) / 1e3)
+    Pf, iff = solve("c128", tol=1e-10)
+    cm, cp, cf = (op.cross_sections(Pm[0], E), op.cross_sections(Pp[0], E), op.cross_sections(Pf[0], E))
+    err = lambda a, b: abs(a - b) / abs(b)
+    nocc = int((ia != 0).sum().item())
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    t_mv = time_matvec(op.twin(torch.complex64), 10, flush)
+    peak, pk = measured_peak()
+    B = matvec_bytes(op.shape, 8)
+    line = _line(METRIC, value, "solves/s", args, ws, t,
+                 {"workload": f"large128: 128^3 box ({nocc} dipoles), ellipsoid semi-axes (64,48,40)d, seeded Euler "
+                              f"angles, m={spec['m']:.4f}, |m|kd=0.6, mixed c64 (1e-4) + FP64 refinement to 1e-6",
+                  "box": [128] * 3, "fft": list(op.L), "parallelism": "replicas" if ws > 1 else "single"},
+                 gpu_launches=int(launches),
+                 plain_c128_solves_per_s=plain, mixed_over_plain=value / ws / plain,
+                 iterations={"mixed_inner": im[0].iters, "outer": im[0].outer, "plain_c128": ip[0].iters,
+                             "true_relres_mixed": im[0].true_relres},
+                 accuracy_vs_fp64={"mixed": {"C_ext_rel_err": err(cm[0], cf[0]), "C_abs_rel_err": err(cm[1], cf[1])},
+                                   "plain_c128": {"C_ext_rel_err": err(cp[0], cf[0]),
+                                                  "C_abs_rel_err": err(cp[1], cf[1])},
+                                   "C_ext": cf[0], "C_abs": cf[1]},
+                 roofline={"bound": "hbm", "achieved": B / t_mv / 1e9, "peak": peak, "unit": "GB/s",
+                           "frac": B / t_mv / 1e9 / peak, "traffic": None, "peak_kind": pk,
+                           "kernel": "5-pass matvec, complex64, 128^3 box (FFT 256^3)", "ms": t_mv * 1e3,
+                           "algorithmic_bytes": B},
+                 clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+def run_batch64(args, ws, rank, local):
+    """64 rotated ellipsoids with box edges 16-96, 2 polarisations x 8
+    incidence directions each (1024 right-hand sides), mixed precision to
+    1e-5, autotuned padding per size bucket, buckets as concurrent slot pools."""
+    import torch
+    from precondda_b200 import _lib as L
+    from precondda_b200.batch import Geometry, PaddingTuner, solve_geometries
+    from precondda_b200.workloads import random_ellipsoid_spec, build_geometry
+    from precondda_b200.engine import cross_sections
+    dev = torch.device("cuda", local)
+    rng = np.random.default_rng(40 + rank)
+    specs = [random_ellipsoid_spec(rng) for _ in range(args.geometries)]
+    tuner = PaddingTuner("mixed", device=dev)
+    tuner.plan([tuple(s["box"]) for s in specs])          # autotune outside the timed region
+    torch.cuda.synchronize()
+    lc0 = L.lib().dda_kernel_launches()
+    with ClockSampler(dev.index) as clk:
+        barrier(ws)
+        t_all = time.perf_counter()
+        geoms = []
+        for sp in specs:
+            ia, k, d, Es = build_geometry(sp, dev)
+            geoms.append(Geometry(ia, k, d, Es))
+        torch.cuda.synchronize()
+        t_build = time.perf_counter() - t_all
+        xs = {}
+
+        def on_result(g, j, Pv, info):
+            G = geoms[g]
+            xs[(g, j)] = cross_sections(Pv.contiguous(), G.E_incs[j], G.inv_alpha, G.k)
+
+        res = solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, tuner=tuner, device=dev,
+                               keep_results=False, on_result=on_result)
+        torch.cuda.synchronize()
+        t_all = time.perf_counter() - t_all
+    launches = L.lib().dda_kernel_launches() - lc0
+    t = max_over_ranks(ws, res.seconds)
+    te = max_over_ranks(ws, t_all)
+    n = res.solves
+    if rank != 0:
+        return
+    infos = [i for gi in res.info for i in gi]
+    its = [i.iters for i in infos]
+    buckets = {}
+    for (box, L_) in res.plan:
+        key = "x".join(map(str, box))
+        buckets[key] = buckets.get(key, 0) + 1
+    line = _line(METRIC, n * ws / t, "solves/s", args, ws, t,
+                 {"workload": f"batch64: {len(specs)} rotated ellipsoids, box edges U{{16..96}}, semi-axes 0.3-0.5 x "
+                              f"edge, m Re U[1.3,2], Im U[0,0.3], lambda U[0.4,0.8] um, |m|kd=0.5, 2 pols x 8 "
+                              f"directions ({n} RHS), mixed c64 (1e-4) + FP64 refinement to 1e-5",
+                  "global_batch": n * ws, "parallelism": "replicas" if ws > 1 else "single",
+                  "buckets": buckets},
+                 e2e={"value": n * ws / te, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                      "d2h_bytes_per_step": 3 * 8 * n,
+                      "includes": "device voxelisation and incident fields from seeded specs, Green builds, padded "
+                                  "batched solves, cross sections of every RHS to the host"},
+                 gpu_launches=int(launches),
+                 solve_seconds=res.seconds, build_seconds=t_build,
+                 converged=sum(i.status == "converged" for i in infos),
+                 iterations={"mean_inner": float(np.mean(its)), "max_inner": int(max(its)),
+                             "mean_outer": float(np.mean([i.outer for i in infos]))},
+                 clocks=clk.summary())
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, ws, rank, local):
+    """Poisson request stream (20/s), 40% spheres, 40% ellipsoids, 20%
+    random-walk aggregates, boxes 16^3-128^3, 1-16 incidences each, served
+    by continuous batching with HBM admission and Green-tensor reuse."""
+    import torch
+    from precondda_b200 import _lib as L
+    from precondda_b200.serve import DDAServer, Request
+    from precondda_b200.workloads import serving_stream, build_geometry
+    dev = torch.device("cuda", local)
+    stream = serving_stream(50 + rank, rate=args.rate, duration=args.duration)
+    srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=8, device=dev)
+    # warm the kernels of every bucket outside the timed region
+    warm = sorted({srv.bucket_for(sp["box"]) for _, sp in stream})
+    for b in warm:
+        ia, k, d, Es = build_geometry({"kind": "sphere", "box": (b, b, b), "radius_d": b / 2.0, "m": 1.5 + 0.01j,
+                                       "wavelength": 0.5, "mkd": 0.5, "dirs": np.array([[0.0, 0.0, 1.0]]),
+                                       "pols": 1}, dev)
+        srv.submit(Request(inv_alpha=ia, E_inc=Es[0], k=k, d=d, tol=1e-5))
+    srv.drain()
+    srv.done.clear()
+    srv.green.hits = srv.green.misses = 0
+    torch.cuda.synchronize()
+    lc0 = L.lib().dda_kernel_launches()
+    groups = {}
+    with ClockSampler(dev.index) as clk:
+        barrier(ws)
+        t0 = time.perf_counter()
+        q = 0
+        while q < len(stream) or srv.pending():
+            now = time.perf_counter() - t0
+            while q < len(stream) and stream[q][0] <= now:
+                arr, sp = stream[q]
+                # lazy requests: the lattice and incident fields are built on
+                # the device when a request enters a slot (the lattice once
+                # per request group), so the queue holds no device memory
+                cache = {}
+
+                def make(j, sp=sp, cache=cache):
+                    def build():
+                        if "geo" not in cache:
+                            cache["geo"] = build_geometry(sp, dev)
+                        ia, k_, d_, Es = cache["geo"]
+                        E = Es[j]
+                        cache["left"] = cache.get("left", len(Es)) - 1
+                        if cache["left"] == 0:
+                            cache.clear()
+                        return ia, E
+                    return build
+
+                lam, m = sp["wavelength"], sp["m"]
+                k = 2 * math.pi / lam
+                d = sp["mkd"] / (abs(m) * k)
+                reqs = []
+                n_rhs = len(sp["dirs"]) * (len(sp["fixed_pols"]) if "fixed_pols" in sp else sp.get("pols", 2))
+                for j in range(n_rhs):
+                    r = srv.submit(Request(inv_alpha=None, E_inc=None, k=k, d=d, tol=1e-5, shape=tuple(sp["box"]),
+                                           build=make(j)))
+                    r.t_submit = t0 + arr
+                    reqs.append(r)
+                groups[q] = (t0 + arr, reqs)
+                q += 1
+            if srv.pending():
+                for r in srv.step():
+                    r.P = r.inv_alpha = r.E_inc = None          # results are not kept
+            elif q < len(stream):
+                time.sleep(min(1e-3, max(0.0, stream[q][0] - now)))
+        torch.cuda.synchronize()
+        span = time.perf_counter() - t0
+    launches = L.lib().dda_kernel_launches() - lc0
+    if rank != 0:
+        return
+    lat_req = np.array([max(r.t_done for r in reqs) - ta for ta, reqs in groups.values()])
+    rhs = [r for _, reqs in groups.values() for r in reqs]
+    lat_rhs = np.array([r.t_done - r.t_submit for r in rhs])
+    st = srv.stats(rhs)
+    line = _line(METRIC, len(rhs) / span, "solves/s", args, ws, span,
+                 {"workload": f"serve: Poisson {args.rate}/s over {args.duration} s ({len(stream)} requests, "
+                              f"{len(rhs)} RHS), 40% spheres / 40% ellipsoids / 20% aggregates (K 4-32, r 6-12 d), "
+                              f"boxes 16^3-128^3, m Re U[1.3,2] Im U[0,0.5], lambda U[0.4,0.8] um, 1-16 incidences, "
+                              f"mixed precision to 1e-5, continuous batching",
+                  "parallelism": "replicas" if ws > 1 else "single", "slots_per_bucket": args.slots,
+                  "pools": {str(k): v for k, v in st.get("pools", {}).items()}},
+                 latency_ms={"request_p50": float(np.percentile(lat_req, 50) * 1e3),
+                             "request_p99": float(np.percentile(lat_req, 99) * 1e3),
+                             "rhs_p50": float(np.percentile(lat_rhs, 50) * 1e3),
+                             "rhs_p99": float(np.percentile(lat_rhs, 99) * 1e3)},
+                 requests_per_s=len(stream) / span,
+                 green_cache={"hits": srv.green.hits, "misses": srv.green.misses},
+                 converged=sum(r.info.status == "converged" for r in rhs),
+                 gpu_launches=int(launches), clocks=clk.summary())
+    srv.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -412,6 +653,13 @@ def main():
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--time", action="store_true", help="with --profile-matvec: time 20 launches (L2 flushed)")
+    ap.add_argument("--workload", default="sphere64", choices=["sphere64", "large128", "batch64", "serve"],
+                    help="sphere64 (default): the precision configuration; large128: 128^3 ellipsoid; "
+                         "batch64: 64 geometries x 16 RHS; serve: Poisson request stream")
+    ap.add_argument("--geometries", type=int, default=64, help="batch64: number of geometries")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
+    ap.add_argument("--slots", type=int, default=16, help="serve: slots per size bucket")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     if args.profile_matvec:
@@ -420,6 +668,12 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, ws, rank)
+        elif args.workload == "large128":
+            run_large128(args, ws, rank, local)
+        elif args.workload == "batch64":
+            run_batch64(args, ws, rank, local)
+        elif args.workload == "serve":
+            run_serve(args, ws, rank, local)
         else:
             run_ours(args, ws, rank, local)
     finally:

@@ -1,0 +1,280 @@
+"""Many geometries of uneven size solved together on one GPU.
+
+Each geometry (a lattice with its own k and d) carries several right-hand
+sides (polarisations x incidence directions).  Geometries are padded into
+size buckets -- zero inverse polarizability in the padding is exactly an
+empty voxel, so the physics does not change -- and every bucket is a slot
+pool (``serve.SlotPool``) holding all right-hand sides of its geometries.
+The pools run on their own streams and are advanced round-robin, so buckets
+of different size are in flight on the device at the same time, and each
+pool retires converged right-hand sides while the rest continue (the
+reference solves one right-hand side of one lattice at a time,
+Gpbicgstab.py:879-1201).  The synthetic workloads live in workloads.py.
+
+``PaddingTuner`` picks each geometry's padded box and FFT lengths: for every
+candidate shape (per-axis padding to the next bucket edge, or the enclosing
+cube, whose kernels are specialised at compile time) it times the batched
+matvec on the device once and keeps the cheapest per right-hand side.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import time
+from collections import defaultdict
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .engine import _C64, _C128, _device, fft_lengths, green_octant_pair, compiled_fft_lengths
+from .serve import SlotPool, request_bytes, slot_bytes
+
+DEFAULT_EDGES = (8, 12, 16, 20, 24, 32, 40, 48, 64, 72, 80, 96, 128, 144, 160, 192, 256)
+
+
+@dataclass
+class Geometry:
+    """One lattice: inverse polarizability (nx,ny,nz) and its right-hand sides."""
+    inv_alpha: torch.Tensor
+    k: float
+    d: float
+    E_incs: list
+    tag: dict = field(default_factory=dict)
+
+    @property
+    def shape(self):
+        return tuple(int(v) for v in self.inv_alpha.shape)
+
+
+# --------------------------------------------------------------------------
+# padding autotuner
+# --------------------------------------------------------------------------
+def _next_edge(n, edges):
+    for e in sorted(edges):
+        if e >= n:
+            return int(e)
+    raise ValueError(f"box edge {n} exceeds the largest bucket edge {max(edges)}")
+
+
+class PaddingTuner:
+    """Chooses (padded box, FFT lengths) per geometry by timing the
+    batched matvec of each candidate shape once (results cached, optionally
+    in a JSON file)."""
+
+    def __init__(self, precision="mixed", edges=DEFAULT_EDGES, nb=16, device=None, cache_path=None, measure=True):
+        self.device = _device(device)
+        self.dtype = _C64 if precision in ("mixed", "c64") else _C128
+        self.edges = tuple(edges)
+        self.nb = int(nb)
+        self.measure = measure
+        self.cache_path = cache_path
+        self.times: dict = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.times = {tuple(json.loads(k)): v for k, v in json.load(f).items()}
+
+    def candidates(self, shape):
+        pad = tuple(_next_edge(n, self.edges) for n in shape)
+        c = _next_edge(max(shape), self.edges)
+        out = {pad, (c, c, c)}
+        return sorted(out)
+
+    def lengths(self, box):
+        sizes = compiled_fft_lengths(self.dtype)
+        return tuple(2 * b if 2 * b in sizes else min(s for s in sizes if s >= 2 * b) for b in box)
+
+    def cost(self, box):
+        """Seconds per right-hand side per matvec for a padded box."""
+        L_ = self.lengths(box)
+        key = tuple(box) + tuple(L_) + (self.nb,)
+        if key in self.times:
+            return self.times[key]
+        if not self.measure:
+            n = np.prod(L_)
+            t = 1e-12 * n * math.log2(n) * 3 + 1e-9 * np.prod(box)
+        else:
+            t = self._time(box, L_)
+        self.times[key] = t
+        if self.cache_path:
+            with open(self.cache_path, "w") as f:
+                json.dump({json.dumps(list(k)): v for k, v in self.times.items()}, f)
+        return t
+
+    def _time(self, box, L_):
+        # one matvec of a filled box of this shape (the solver's cost per
+        # iteration is two matvecs plus streaming updates over the box)
+        from .engine import DDAOperator
+        dev = self.device
+        ia = torch.full(box, 1.0 / (0.02 + 0.002j), dtype=_C128, device=dev)
+        op = DDAOperator(ia, 6.0, 0.05, dtype=self.dtype, L_=L_, device=dev)
+        x = torch.randn(*box, 3, dtype=self.dtype, device=dev)
+        for _ in range(2):
+            op.matvec(x)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        e0.record()
+        for _ in range(reps):
+            op.matvec(x)
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    def plan(self, shapes):
+        """[(box, L)] per geometry shape."""
+        out = []
+        for s in shapes:
+            best = min(self.candidates(s), key=lambda b: self.cost(b))
+            out.append((best, self.lengths(best)))
+        return out
+
+
+# --------------------------------------------------------------------------
+# execution
+# --------------------------------------------------------------------------
+def _pad(t, box, extra=()):
+    if tuple(t.shape[:3]) == tuple(box):
+        return t.contiguous()
+    out = torch.zeros(tuple(box) + tuple(extra), dtype=t.dtype, device=t.device)
+    nx, ny, nz = t.shape[:3]
+    out[:nx, :ny, :nz] = t
+    return out
+
+
+@dataclass
+class BatchResult:
+    P: list            # per geometry: list of P (cropped to the geometry's box), one per RHS
+    info: list         # per geometry: list of SolveInfo
+    plan: list         # per geometry: (box, L)
+    seconds: float     # device-synchronised wall time of the solve phase
+    solves: int
+
+
+def green_bytes(L_):
+    """Both precisions of one FFT'd interaction octant."""
+    return 6 * (L_[0] // 2 + 1) * (L_[1] // 2 + 1) * (L_[2] // 2 + 1) * (16 + 8)
+
+
+def item_bytes(box, L_, precision, nrhs, ngeom):
+    """Device bytes a bucket item holds while it runs: its slot pool, the
+    per-request tensors and padded copies, and one octant per geometry."""
+    n = box[0] * box[1] * box[2]
+    per_rhs = slot_bytes(box, L_, precision) + request_bytes(box, precision) + 3 * n * 16 + n * 8
+    return nrhs * per_rhs + ngeom * (green_bytes(L_) + n * 16)
+
+
+def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_iter=2000, max_outer=12,
+                     ratio=100.0, chunk=8, tuner=None, hbm_budget=None, device=None, keep_results=True,
+                     on_result=None):
+    """Solve every right-hand side of every geometry.
+
+    Buckets (geometries sharing a padded box and FFT lengths) become slot
+    pools; pools are started while the HBM budget (default 75% of the free
+    memory) allows, advanced round-robin on their own streams, and a new
+    bucket starts as soon as a running one finishes.  ``on_result(g, j, P,
+    info)`` is called for each finished right-hand side (P cropped to the
+    geometry's box); P is also kept in the result unless ``keep_results`` is
+    False."""
+    from collections import deque
+    dev = _device(device)
+    tuner = tuner or PaddingTuner(precision, device=dev)
+    plan = tuner.plan([g.shape for g in geoms])
+    groups = defaultdict(list)
+    for gi, (box, L_) in enumerate(plan):
+        groups[(box, L_)].append(gi)
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    if hbm_budget is None:
+        free, _ = torch.cuda.mem_get_info(dev)
+        hbm_budget = int(0.75 * free)
+    # items: buckets, largest first, split so that each fits the budget
+    items = deque()
+    for key in sorted(groups, key=lambda k: -np.prod(k[0])):
+        box, L_ = key
+        acc = []
+        for g in groups[key]:
+            trial = acc + [g]
+            if acc and item_bytes(box, L_, precision, sum(len(geoms[x].E_incs) for x in trial),
+                                  len(trial)) > hbm_budget:
+                items.append((key, acc))
+                acc = [g]
+            else:
+                acc = trial
+        if acc:
+            items.append((key, acc))
+
+    Ps = [[None] * len(g.E_incs) for g in geoms]
+    infos = [[None] * len(g.E_incs) for g in geoms]
+
+    def start(key, gl):
+        box, L_ = key
+        nrhs = sum(len(geoms[g].E_incs) for g in gl)
+        pool = SlotPool(box, L_, nrhs, precision, 1.0, dev)
+        where, slot = {}, 0
+        try:
+            for g in gl:
+                G = geoms[g]
+                g128, g64 = green_octant_pair(box, G.k, G.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dev)
+                ia = _pad(G.inv_alpha.to(_C128), box)
+                if precision == "c64":
+                    ia = ia.to(_C64)
+                gh = (g64, g128) if precision == "mixed" else (g64 if precision == "c64" else g128)
+                for j, E in enumerate(G.E_incs):
+                    Ep = _pad(E.to(_C64 if precision == "c64" else _C128), box, (3,))
+                    pool.admit(slot, gh, ia, Ep, tol=tol, inner_tol=inner_tol, max_iter=max_iter,
+                               max_outer=max_outer, ratio=ratio)
+                    where[slot] = (g, j)
+                    slot += 1
+        except BaseException:
+            pool.close()
+            raise
+        return pool, where, item_bytes(box, L_, precision, nrhs, len(gl))
+
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    active, used = [], 0
+    while items or active:
+        while items:
+            key, gl = items[0]
+            est = item_bytes(key[0], key[1], precision, sum(len(geoms[g].E_incs) for g in gl), len(gl))
+            if active and used + est > hbm_budget:
+                break
+            try:
+                entry = start(key, gl)
+            except (MemoryError, torch.cuda.OutOfMemoryError):
+                if not active:
+                    raise
+                torch.cuda.empty_cache()
+                break
+            items.popleft()
+            active.append(entry)
+            used += entry[2]
+        for pool, _, _ in active:
+            pool.run(chunk)
+        still = []
+        for pool, where, est in active:
+            for s, info, P in pool.poll():
+                g, j = where[s]
+                nx, ny, nz = geoms[g].shape
+                Pc = P[:nx, :ny, :nz]
+                infos[g][j] = info
+                if on_result is not None:
+                    on_result(g, j, Pc, info)
+                if keep_results:
+                    Ps[g][j] = Pc
+            if pool.running:
+                still.append((pool, where, est))
+            else:
+                pool.close()
+                used -= est
+        if len(still) < len(active):
+            torch.cuda.empty_cache()
+        active = still
+    torch.cuda.synchronize(dev)
+    secs = time.perf_counter() - t0
+    n = sum(len(g.E_incs) for g in geoms)
+    return BatchResult(Ps, infos, plan, secs, n)

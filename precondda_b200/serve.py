@@ -208,7 +208,12 @@ class GreenCache:
 
 @dataclass
 class Request:
-    """One solve: inv_alpha (nx,ny,nz), E_inc (nx,ny,nz,3), k, d."""
+    """One solve: inv_alpha (nx,ny,nz), E_inc (nx,ny,nz,3), k, d.
+
+    Lazy form: inv_alpha = E_inc = None with ``shape`` set and ``build`` a
+    callable returning (inv_alpha, E_inc); the arrays are then made only when
+    the request is admitted into a slot, so a queue of waiting requests holds
+    no device memory."""
     inv_alpha: object
     E_inc: object
     k: float
@@ -222,6 +227,7 @@ class Request:
     info: SolveInfo | None = None
     bucket: int = 0
     shape: tuple = ()
+    build: object = None
 
 
 @dataclass
@@ -237,8 +243,9 @@ class DDAServer:
     """Continuous-batching server (one GPU, one pool per cubic size bucket).
 
     precision: 'mixed' (complex64 sweeps + FP64 refinement, the default),
-    'c64' or 'c128'.  hbm_budget: bytes the pools may hold (default: 80% of
-    the free device memory at construction)."""
+    'c64' or 'c128'.  hbm_budget: bytes the pools may hold (default: 60% of
+    the free device memory at construction; the rest is left to Green builds,
+    the Green cache and the requests' arrays)."""
 
     def __init__(self, precision="mixed", buckets=DEFAULT_BUCKETS, slots_per_bucket=16, chunk_iters=8,
                  hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None):
@@ -251,7 +258,7 @@ class DDAServer:
         self.chunk = int(chunk_iters)
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
-            hbm_budget = int(0.8 * free)
+            hbm_budget = int(0.6 * free)      # the rest: Green builds and caches, request arrays
         self.hbm_budget = int(hbm_budget)
         self.hbm_used = 0
         self.green = GreenCache(green_budget, self.device)
@@ -283,9 +290,14 @@ class DDAServer:
 
     # -- requests -----------------------------------------------------------
     def submit(self, req: Request) -> Request:
-        """Queue a request (arrays on the host or the device)."""
+        """Queue a request (arrays on the host or the device, or lazy)."""
         ia = req.inv_alpha
-        shape = tuple(int(v) for v in (ia.shape if hasattr(ia, "shape") else np.shape(ia)))
+        if ia is None:
+            if req.build is None or len(req.shape) != 3:
+                raise ValueError("a lazy request needs build() and shape")
+            shape = tuple(int(v) for v in req.shape)
+        else:
+            shape = tuple(int(v) for v in (ia.shape if hasattr(ia, "shape") else np.shape(ia)))
         if len(shape) != 3:
             raise ValueError("inv_alpha must have shape (nx, ny, nz)")
         req.shape = shape
@@ -315,6 +327,8 @@ class DDAServer:
             if s < 0:
                 return
             req = b.queue.popleft()
+            if req.inv_alpha is None:
+                req.inv_alpha, req.E_inc = req.build()
             g64, g128 = self.green.get((b.n,) * 3, b.L, req.k, req.d)
             ghat = (g64, g128) if self.precision == "mixed" else (g64 if self.precision == "c64" else g128)
             ia, E = self._pad(req, b.n)

@@ -136,3 +136,27 @@ def test_serve_buckets_and_hbm_admission():
     assert pool_slots(box, L, "mixed", 10 * per + per // 2, 64) == 10
     assert pool_slots(box, L, "mixed", 10 * per, 4) == 4
     assert pool_slots(box, L, "mixed", per - 1, 4) == 0
+
+
+def test_workload_generators_are_seeded_and_valid():
+    from precondda_b200 import workloads as W
+    a = W.serving_stream(3, rate=20, duration=5)
+    b = W.serving_stream(3, rate=20, duration=5)
+    assert [x[0] for x in a] == [x[0] for x in b] and len(a) > 50
+    kinds = {sp["kind"] for _, sp in a}
+    assert kinds <= {"sphere", "ellipsoid", "aggregate"} and len(kinds) == 3
+    assert all(16 <= max(sp["box"]) <= 128 for _, sp in a)
+    assert all(1 <= len(sp["dirs"]) <= 16 for _, sp in a)
+    rng = np.random.default_rng(0)
+    c, r = W.random_walk_aggregate(12, (6, 12), rng)
+    assert len(c) == 12
+    for i in range(12):
+        for j in range(i):
+            assert np.linalg.norm(c[i] - c[j]) >= r[i] + r[j] - 1e-6
+    # every sphere after the first touches an earlier one
+    for i in range(1, 12):
+        assert min(abs(np.linalg.norm(c[i] - c[j]) - r[i] - r[j]) for j in range(i)) < 1e-6
+    e = W.random_ellipsoid_spec(np.random.default_rng(1))
+    assert all(16 <= b <= 96 for b in e["box"]) and len(e["dirs"]) == 8
+    k1, k2 = W.transverse_pair(np.array([0.3, -0.5, 0.81]) / np.linalg.norm([0.3, -0.5, 0.81]))
+    assert abs(k1 @ k2) < 1e-12
