@@ -102,11 +102,23 @@ struct BatchWs {
 
 enum MvMode { MV_AX = 0, MV_RESIDUAL = 1, MV_CONV = 2, MV_CONV_MASKED = 3 };
 
+// Krylov steps fused into a matvec: before the first pass (the input is
+// formed on the fly) and after the last pass (a dot product of the output
+// reduced across the grid, the scalar step run by the last CTA).
+enum MvPre { MV_PRE_NONE = 0, MV_PRE_SY = 1 };                 // s = r - alpha v, y = s_prev - s - alpha w
+enum MvPost { MV_POST_NONE = 0, MV_POST_ALPHA = 1, MV_POST_ZETA = 2 };
+struct MvFuse {
+  int pre = MV_PRE_NONE, post = MV_POST_NONE;
+  double* red = nullptr;      // >= nb * grid1 * KRED doubles
+  unsigned* cnt = nullptr;    // per-instance tickets
+};
+
 // Enqueue the 5-pass matvec for a batch of instances that share Geo.
 // Instance slots: st[act ? act[j] : j], j < nb.
 template <typename R>
 cudaError_t launch_matvec(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
-                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s);
+                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
+                          const MvFuse& fz = MvFuse());
 
 // One matvec with explicit twiddle tables (allocation-free entry point).
 template <typename R>

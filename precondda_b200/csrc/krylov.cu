@@ -20,7 +20,7 @@
 //
 // Dots and norms accumulate in FP64 whatever the vector precision.
 #include "dda_host.h"
-#include "reduce.cuh"
+#include "krylov_ctrl.cuh"
 
 namespace dda {
 
@@ -126,8 +126,7 @@ __global__ void __launch_bounds__(KNT) k_alpha(InstState* st, const int* act, do
     acc[1] += (double)a.x * b.y - (double)a.y * b.x;
   });
   double tot[2];
-  if (reduce_last<2>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0)
-    S.alpha = zdiv(S.rho1, make_double2(tot[0], tot[1]));
+  if (reduce_last<2>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) alpha_from_dot(S, tot);
 }
 
 // s = r - alpha v ; y = s_prev - s - alpha w   (Gpbicgstab.py:1020-1021)
@@ -176,32 +175,11 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
   } else {
     grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C tv = t[i], sv = s[i], yv = y[i];
-      acc[0] += (double)yv.x * yv.x + (double)yv.y * yv.y;            // yy
-      acc[1] += (double)tv.x * tv.x + (double)tv.y * tv.y;            // tt
-      acc[2] += (double)yv.x * tv.x + (double)yv.y * tv.y;            // yt = conj(y) t
-      acc[3] += (double)yv.x * tv.y - (double)yv.y * tv.x;
-      acc[4] += (double)yv.x * sv.x + (double)yv.y * sv.y;            // ys
-      acc[5] += (double)yv.x * sv.y - (double)yv.y * sv.x;
-      acc[6] += (double)tv.x * sv.x + (double)tv.y * sv.y;            // ts
-      acc[7] += (double)tv.x * sv.y - (double)tv.y * sv.x;
+      zeta_dots_acc(acc, tv, sv, yv);
     });
   }
   double tot[8];
-  if (reduce_last<8>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
-    if (first) {
-      S.zeta = zdiv(make_double2(tot[1], tot[2]), make_double2(tot[0], 0.0));
-      S.eta = make_double2(0.0, 0.0);
-    } else {
-      const double2 yy = make_double2(tot[0], 0.0), tt = make_double2(tot[1], 0.0);
-      const double2 yt = make_double2(tot[2], tot[3]);
-      const double2 ty = make_double2(tot[2], -tot[3]);   // conj(t) y = conj(conj(y) t)
-      const double2 ys = make_double2(tot[4], tot[5]);
-      const double2 ts = make_double2(tot[6], tot[7]);
-      const double2 den = zsub(zmul(tt, yy), zmul(yt, ty));
-      S.zeta = zdiv(zsub(zmul(yy, ts), zmul(ys, ty)), den);
-      S.eta = zdiv(zsub(zmul(tt, ys), zmul(yt, ts)), den);
-    }
-  }
+  if (reduce_last<8>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) zeta_eta_from_dots(S, tot, first);
 }
 
 // u, z, r, x updates (Gpbicgstab.py:1038-1057) and ||r||^2, <rhat, r>

@@ -5,6 +5,17 @@
 namespace dda {
 template <>
 bool mv_cube_set<float>(int L, int p3var, MvSet<float>& o) {
+  if (p3var == 1) {
+    // the register-tensor variant, compiled for the power-of-two lengths
+    switch (L) {
+      case 32: mv_cube_fill<float, 32, 1>(o); return true;
+      case 64: mv_cube_fill<float, 64, 1>(o); return true;
+      case 128: mv_cube_fill<float, 128, 1>(o); return true;
+      case 256: mv_cube_fill<float, 256, 1>(o); return true;
+      case 512: mv_cube_fill<float, 512, 1>(o); return true;
+    }
+    return false;
+  }
   if (p3var != 0) return false;
   switch (L) {
 #define DDA_K(n) case n: mv_cube_fill<float, n, 0>(o); return true;

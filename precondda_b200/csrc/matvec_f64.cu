@@ -8,8 +8,9 @@ bool mv_general_set<double>(int Lx, int Ly, int Lz, int p3var, MvSet<double>& ou
 }
 template <>
 cudaError_t launch_matvec<double>(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
-                                 int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
-  return launch_matvec_impl<double>(ctx, g, pc, st, act, nb, in_id, out_id, mode, cond, gscale, s);
+                                 int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
+                                 const MvFuse& fz) {
+  return launch_matvec_impl<double>(ctx, g, pc, st, act, nb, in_id, out_id, mode, cond, gscale, s, fz);
 }
 template <>
 cudaError_t launch_matvec_tw<double>(const Geo& g, const PassCfg& pc, InstState* st, const void* twx, const void* twy,

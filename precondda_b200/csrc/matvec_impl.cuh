@@ -20,6 +20,7 @@
 #pragma once
 #include "dda_host.h"
 #include "fftreg.cuh"
+#include "krylov_ctrl.cuh"
 #include "fft_sizes.h"
 #include <cstdlib>
 #include <type_traits>
@@ -71,7 +72,7 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int cond,
-                                                            int nl_) {
+                                                            int nl_, int pre) {
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
@@ -92,14 +93,36 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
   const int t = rest % SH::T, l = rest / SH::T;
   const long long line = (long long)blockIdx.x * nl + l;
   const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
-  const C* xl = x + line * nz * 3 + c;
+  const long long base = line * nz * 3 + c;
   C* tl = t1 + line * (long long)LZ * 3 + c;
   C* sl = s + l * 3 * SH::LP + c;
-  auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nz)) ? __ldcg(xl + pos * 3) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
   auto stf = [&](int, int pos, C v) { if (ok) __stcg(tl + pos * 3, v); };
   C a[P::E];
-  rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
+  if (pre == MV_PRE_SY) {
+    // the input is s = r - alpha v, formed here together with
+    // y = s_prev - s - alpha w (Gpbicgstab.py:1020-1021); both are stored
+    const C* __restrict__ r = (const C*)S.vec[V_R];
+    const C* __restrict__ v = (const C*)S.vec[V_V];
+    const C* __restrict__ sp = (const C*)S.vec[V_SPREV];
+    const C* __restrict__ w = (const C*)S.vec[V_W];
+    C* __restrict__ so = (C*)S.vec[V_S];
+    C* __restrict__ yo = (C*)S.vec[V_Y];
+    const C al = mk<C>(S.alpha.x, S.alpha.y);
+    auto ld = [&](int, int pos) -> C {
+      if (!(ok && (ZH || pos < nz))) return czero<C>();
+      const long long i = base + (long long)pos * 3;
+      const C sv = csub(__ldcg(r + i), cmul(al, __ldcg(v + i)));
+      __stcg(so + i, sv);
+      __stcg(yo + i, csub(csub(__ldcg(sp + i), sv), cmul(al, __ldcg(w + i))));
+      return sv;
+    };
+    rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
+  } else {
+    const C* xl = x + base;
+    auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nz)) ? __ldcg(xl + pos * 3) : czero<C>(); };
+    rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -187,63 +210,89 @@ __device__ __forceinline__ int pencil_ky(int p, int Ly) {
   return (p & 1) ? pr : Ly - pr;
 }
 
-// variant with the three components of a pencil in one thread:
-// thread = (kzl fastest, t); general sizes only
-template <typename R, int LX, int V>
+// variant with the three components of a pencil in one thread and the
+// tensor product in registers: thread = (kzl fastest, t)
+template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                             InstState* st, const int* act, int cond, int tz,
-                                                             int ntz, R gscale) {
+                                                             InstState* st, const int* act, int cond, int tz_,
+                                                             int ntz_, R gscale) {
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
   typedef typename SH::P P;
   typedef RevPlan<P> Q;
+  constexpr bool CUBE = NC > 0;
+  static_assert(!CUBE || LX == 2 * NC, "cubic kernels need L = 2n");
+  constexpr int TZC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), LX) : 1;
+  constexpr int NTZC = (LX + TZC - 1) / TZC;
+  constexpr bool ZH = CUBE && P::r[0] % 2 == 0;
+  constexpr bool DH = CUBE && half_store_ok<Q>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t2 = (C*)S.t2;
   const C* __restrict__ gh = (const C*)S.ghat;
+  const int tz = CUBE ? TZC : tz_;
+  const int ntz = CUBE ? NTZC : ntz_;
+  const int Ly = CUBE ? LX : g.Ly, Lz = CUBE ? LX : g.Lz;
+  const int hy = CUBE ? LX / 2 + 1 : g.hy, hz = CUBE ? LX / 2 + 1 : g.hz;
+  const int H = CUBE ? (LX / 2 + 1) * (LX / 2 + 1) * (LX / 2 + 1) : g.hx * g.hy * g.hz;
+  const int nx = CUBE ? NC : g.nx;
   const int kzl = threadIdx.x % tz, t = threadIdx.x / tz;
   const int p = blockIdx.x / ntz, kzt = blockIdx.x - p * ntz;
-  const int ky = pencil_ky(p, g.Ly);
+  const int ky = pencil_ky(p, Ly);
   const int kz0 = kzt * tz;
   const int kz = kz0 + kzl;
-  const bool ok = kz < g.Lz;
-  const int nx = g.nx;
-  const long long rs = (long long)g.Ly * g.Lz * 3;          // x-row stride of T2
-  C* col = t2 + ((long long)ky * g.Lz + kz) * 3;
+  const bool ok = (CUBE && LX % TZC == 0) || kz < Lz;
+  const long long rs = (long long)Ly * Lz * 3;          // x-row stride of T2
+  C* col = t2 + ((long long)ky * Lz + kz) * 3;
   const int W = 3 * tz;
   C* sw = s + 3 * kzl;
-  auto ld = [&](int c, int pos) -> C { return (ok && pos < nx) ? __ldcg(col + pos * rs + c) : czero<C>(); };
+  auto ld = [&](int c, int pos) -> C { return (ok && (ZH || pos < nx)) ? __ldcg(col + pos * rs + c) : czero<C>(); };
   auto sm = [&](int c, int pp) -> C& { return sw[pp * W + c]; };
   C a[3 * P::E];
-  rload<P, 3>(a, t, ld);
+  rload<P, 3, ZH>(a, t, ld);
 #pragma unroll
-  for (int c = 0; c < 3; ++c) rstage<P, 0>(a + c * P::E, t, tw);
+  for (int c = 0; c < 3; ++c) rstage<P, 0, ZH>(a + c * P::E, t, tw);
   rrest<P, 3, 0>(a, t, sm, tw);
   // tensor product at the positions this thread owns after the last stage
   constexpr int RL = P::r[P::S - 1];
-  const bool fy = ky > g.Ly / 2;
-  const int my = fy ? g.Ly - ky : ky;
+  const bool fy = ky > Ly / 2, fz = kz > Lz / 2;
+  const int my = fy ? Ly - ky : ky;
+  const int mz = fz ? Lz - kz : kz;
+  const C* __restrict__ q0 = gh + my * hz + mz;
   if (ok) {
 #pragma unroll
     for (int b = 0; b < P::E / RL; ++b)
 #pragma unroll
       for (int q = 0; q < RL; ++q) {
         const int i = b * RL + q;
-        tensor3(gh, g, LX, rout_pos<P, P::S - 1>(t, b, q), my, fy, kz, gscale, a[i], a[P::E + i], a[2 * P::E + i]);
+        const int kx = rout_pos<P, P::S - 1>(t, b, q);
+        const bool fx = kx > LX / 2;
+        const int mx = fx ? LX - kx : kx;
+        const C* qp = q0 + mx * (hy * hz);
+        const R sxy = (fx != fy) ? -gscale : gscale, sxz = (fx != fz) ? -gscale : gscale;
+        const R syz = (fy != fz) ? -gscale : gscale;
+        const C gxx = cscale(__ldg(qp), gscale), gxy = cscale(__ldg(qp + H), sxy);
+        const C gxz = cscale(__ldg(qp + 2 * H), sxz), gyy = cscale(__ldg(qp + 3 * H), gscale);
+        const C gyz = cscale(__ldg(qp + 4 * H), syz), gzz = cscale(__ldg(qp + 5 * H), gscale);
+        const C a0 = a[i], a1 = a[P::E + i], a2 = a[2 * P::E + i];
+        a[i] = cadd(cadd(cmul(gxx, a0), cmul(gxy, a1)), cmul(gxz, a2));
+        a[P::E + i] = cadd(cadd(cmul(gxy, a0), cmul(gyy, a1)), cmul(gyz, a2));
+        a[2 * P::E + i] = cadd(cadd(cmul(gxz, a0), cmul(gyz, a1)), cmul(gzz, a2));
       }
   }
-  // inverse transform with the reversed plan: its stage 0 owns the same positions
+  // inverse transform with the reversed plan: its stage 0 owns the same
+  // positions; run as swap(FFT(swap(.)))
   const int ti = opaque(t);
   C* colo = opaque_ptr(col);
-  auto stf = [&](int c, int pos, C v) { if (ok && pos < nx) __stcg(colo + pos * rs + c, cswap(v)); };
+  auto stf = [&](int c, int pos, C v) { if (ok && (DH || pos < nx)) __stcg(colo + pos * rs + c, cswap(v)); };
 #pragma unroll
   for (int i = 0; i < 3 * P::E; ++i) a[i] = cswap(a[i]);
 #pragma unroll
   for (int c = 0; c < 3; ++c) rstage<Q, 0>(a + c * P::E, ti, tw);
   rrest<Q, 3, 0>(a, ti, sm, tw);
-  rstore<Q, 3>(a, ti, stf);
+  rstore<Q, 3, DH>(a, ti, stf);
 }
 
 // variant with one component per thread and the tensor product through
@@ -373,7 +422,8 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
 template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int out_id,
-                                                            int mode, int cond, int nl_) {
+                                                            int mode, int cond, int nl_, int post, double* red,
+                                                            unsigned* cnt) {
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
@@ -383,7 +433,8 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
   constexpr bool DH = CUBE && half_store_ok<P>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* s = reinterpret_cast<C*>(smem_raw);
-  InstState& S = st[inst_of(act)];
+  const int inst = inst_of(act);
+  InstState& S = st[inst];
   if (!cond_ok(S, cond)) return;
   const C* __restrict__ t1 = (const C*)S.t1;
   const int nl = CUBE ? NLC : nl_;
@@ -411,26 +462,57 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
   C* __restrict__ yg = (C*)S.vec[out_id] + site_base * 3;
   const C* __restrict__ iag = (const C*)S.inva + site_base;
   const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site_base * 3 : nullptr;
+  // fused dot products of the output (post): <rhat, v> for alpha, or the
+  // zeta / eta dots of t with s and y
+  const bool first = (S.iter == 0) || S.was_reset;
+  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT] + site_base * 3
+                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] + site_base * 3 : nullptr);
+  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] + site_base * 3 : nullptr;
+  double acc[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
   int ll = threadIdx.x / per, j = threadIdx.x - (threadIdx.x / per) * per;
   for (int idx = threadIdx.x; idx < nv; idx += blockDim.x) {
     const int pos = j / 3, cc = j - 3 * pos;
     C v = s[ll * 3 * SH::LP + ppad(pos) * 3 + cc];
+    C r;
     if (mode == MV_CONV) {
-      __stcg(yg + idx, v);
+      r = v;
     } else {
       const C a_ = __ldg(iag + ll * nz + pos);     // shared by 3 lanes: keep it in L1
       const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
       if (!msk) v = czero<C>();
       if (mode == MV_CONV_MASKED) {
-        __stcg(yg + idx, v);
+        r = v;
       } else {
-        C r = csub(cmul(a_, __ldcg(xg + idx)), v);
+        r = csub(cmul(a_, __ldcg(xg + idx)), v);
         if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + idx), r);
-        __stcg(yg + idx, r);
+      }
+    }
+    __stcg(yg + idx, r);
+    if (post == MV_POST_ALPHA) {
+      const C h = __ldcg(d0 + idx);
+      acc[0] += (double)h.x * r.x + (double)h.y * r.y;
+      acc[1] += (double)h.x * r.y - (double)h.y * r.x;
+    } else if (post == MV_POST_ZETA) {
+      const C sv = __ldcg(d0 + idx);
+      if (first) {
+        acc[0] += (double)r.x * r.x + (double)r.y * r.y;
+        acc[1] += (double)r.x * sv.x + (double)r.y * sv.y;
+        acc[2] += (double)r.x * sv.y - (double)r.y * sv.x;
+      } else {
+        const C yv = __ldcg(d1 + idx);
+        zeta_dots_acc(acc, r, sv, yv);
       }
     }
     j += blockDim.x;
     while (j >= per) { j -= per; ++ll; }
+  }
+  if (post == MV_POST_NONE) return;
+  double tot[8];
+  if (reduce_last_n<8>(acc, tot, red, cnt, inst, (int)gridDim.x, blockDim.x) && threadIdx.x == 0) {
+    if (post == MV_POST_ALPHA) alpha_from_dot(S, tot);
+    else zeta_eta_from_dots(S, tot, first);
   }
 }
 
@@ -439,10 +521,10 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
 // ---------------------------------------------------------------------------
 template <typename R> struct MvSet {
   typedef typename CT<R>::T C;
-  typedef void (*P1)(Geo, const C*, InstState*, const int*, int, int, int);
+  typedef void (*P1)(Geo, const C*, InstState*, const int*, int, int, int, int);
   typedef void (*PY)(Geo, const C*, InstState*, const int*, int, int, int);
   typedef void (*P3)(Geo, const C*, InstState*, const int*, int, int, int, R);
-  typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int);
+  typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int, int, double*, unsigned*);
   P1 k1 = nullptr; PY k2 = nullptr; P3 k3 = nullptr; PY k4 = nullptr; P5 k5 = nullptr;
   // tile sizes the kernels were compiled for (cubic set only; 0 = any)
   int nl = 0, tz2 = 0, tz3 = 0;
@@ -476,7 +558,7 @@ bool mv_general_set_impl(int Lx, int Ly, int Lz, int p3var, MvSet<R>& o) {
   switch (Lx) {
 #define DDA_K(n)                                                                                   \
   case n:                                                                                          \
-    o.k3 = p3var == 1 ? (typename M::P3)k_mv_pass3r<R, n, 1>                                       \
+    o.k3 = p3var == 1 ? (typename M::P3)k_mv_pass3r<R, n, 1, 0>                                    \
                       : (p3var == 2 ? (typename M::P3)k_mv_pass3s<R, n, 2, 0>                      \
                                     : (typename M::P3)k_mv_pass3s<R, n, 0, 0>);                    \
     break;
@@ -493,7 +575,8 @@ void mv_cube_fill(MvSet<R>& o) {
   constexpr int NC = L / 2;
   o.k1 = k_mv_pass1<R, L, NC>;
   o.k2 = (typename M::PY)k_mv_pass_y<R, false, L, NC>;
-  o.k3 = (typename M::P3)k_mv_pass3s<R, L, V, NC>;
+  if constexpr (V == 1) o.k3 = (typename M::P3)k_mv_pass3r<R, L, V, NC>;
+  else o.k3 = (typename M::P3)k_mv_pass3s<R, L, V, NC>;
   o.k4 = (typename M::PY)k_mv_pass_y<R, true, L, NC>;
   o.k5 = k_mv_pass5<R, L, NC>;
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
@@ -519,23 +602,26 @@ cudaError_t mv_prepare(const void* const* ks, int n);
 template <typename R>
 cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                           const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
-                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
+                          int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
+                          const MvFuse& fz = MvFuse()) {
   const void* ks[5] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
                        (const void*)k.k5};
   cudaError_t e = mv_prepare(ks, 5);
   if (e != cudaSuccess) return e;
-  k.k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl);
+  k.k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl, fz.pre);
   k.k2<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
   k.k3<<<dim3((unsigned)pc.grid3, nb), pc.th3, pc.smem3, s>>>(g, twx, st, act, cond, pc.tz3, pc.ntz3, (R)gscale);
   k.k4<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
-  k.k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl);
+  k.k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl,
+                                                              fz.post, fz.red, fz.cnt);
   note_launch(s, 5);
   return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
-                               int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s) {
+                               int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
+                               const MvFuse& fz) {
   typedef typename CT<R>::T C;
   constexpr bool dbl = sizeof(R) == 8;
   MvSet<R> k;
@@ -544,7 +630,7 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
   const C* twy = (const C*)ctx.twiddles(g.Ly, dbl);
   const C* twz = (const C*)ctx.twiddles(g.Lz, dbl);
   if (!twx || !twy || !twz) return cudaErrorMemoryAllocation;
-  return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, out_id, mode, cond, gscale, s);
+  return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, out_id, mode, cond, gscale, s, fz);
 }
 
 // Same five launches with caller-provided twiddle tables (used by the

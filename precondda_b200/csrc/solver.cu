@@ -82,7 +82,7 @@ int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
       cudaMalloc((void**)&d_st, nb * sizeof(InstState)) != cudaSuccess ||
       cudaMallocHost((void**)&h_st[0], nb * sizeof(InstState)) != cudaSuccess ||
       cudaMallocHost((void**)&h_st[1], nb * sizeof(InstState)) != cudaSuccess ||
-      cudaMalloc((void**)&red, (size_t)nb * RB * KRED * sizeof(double)) != cudaSuccess ||
+      cudaMalloc((void**)&red, (size_t)nb * std::max<long long>(RB, pc.grid1) * KRED * sizeof(double)) != cudaSuccess ||
       cudaMalloc((void**)&cnt, nb * sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc((void**)&d_out, nb * sizeof(double)) != cudaSuccess ||
       cudaMallocHost((void**)&h_out, nb * sizeof(double)) != cudaSuccess) {
@@ -130,16 +130,43 @@ void Ctx::trim() {
 // ---------------------------------------------------------------------------
 // one GPBiCGSTAB iteration for every instance of the workspace
 // ---------------------------------------------------------------------------
+// DDA_FUSE_KRYLOV=1 lets the Krylov steps alpha (<rhat, v>), s / y and
+// zeta / eta ride on the two matvecs (dot products in the last pass, s and y
+// formed in the first) instead of three separate kernels.  Measured on B200
+// it is no faster (64^3 x 16 RHS: equal; 128^3: 7 % slower), so the separate
+// kernels are the default.
+static bool fuse_krylov() {
+  const char* e = getenv("DDA_FUSE_KRYLOV");
+  return e && *e == '1';
+}
+
+template <typename R>
+static cudaError_t enqueue_front(Ctx& c, BatchWs& w, double gscale, cudaStream_t s, const KrylovLaunch& k) {
+  cudaError_t e;
+  if (fuse_krylov()) {
+    MvFuse f1, f2;
+    f1.post = MV_POST_ALPHA; f1.red = w.red; f1.cnt = w.cnt;
+    f2.pre = MV_PRE_SY; f2.post = MV_POST_ZETA; f2.red = w.red; f2.cnt = w.cnt;
+    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s, f1)))
+      return e;
+    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s, f2)))
+      return e;
+  } else {
+    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
+    launch_alpha<R>(k, s);
+    launch_sy<R>(k, s);
+    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return e;
+    launch_zeta<R>(k, s);
+  }
+  launch_uzrx<R>(k, s);
+  return cudaGetLastError();
+}
+
 template <typename R>
 cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s) {
   KrylovLaunch k{w.d_st, nullptr, w.nb, w.red, w.cnt, (long long)w.n3, w.RB};
   cudaError_t e;
-  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
-  launch_alpha<R>(k, s);
-  launch_sy<R>(k, s);
-  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return e;
-  launch_zeta<R>(k, s);
-  launch_uzrx<R>(k, s);
+  if ((e = enqueue_front<R>(c, w, gscale, s, k))) return e;
   if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s)))
     return e;
   launch_norm<R>(k, s);
@@ -205,16 +232,7 @@ cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s,
     k.cond_reset = hR;
     std::vector<cudaGraphNode_t> none, d1, d2, d3;
     cudaGraphNode_t n1 = nullptr, n2 = nullptr;
-    e = capture_segment(s, G, none, d1, [&]() -> cudaError_t {
-      cudaError_t r;
-      if ((r = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return r;
-      launch_alpha<R>(k, s);
-      launch_sy<R>(k, s);
-      if ((r = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return r;
-      launch_zeta<R>(k, s);
-      launch_uzrx<R>(k, s);
-      return cudaGetLastError();
-    });
+    e = capture_segment(s, G, none, d1, [&]() -> cudaError_t { return enqueue_front<R>(c, w, gscale, s, k); });
     if (e == cudaSuccess)
       e = add_if(s, G, hT, d1, &n1, [&]() -> cudaError_t {
         return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s);
@@ -235,7 +253,8 @@ cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s,
       });
     if (e == cudaSuccess) {
       *out = G;
-      *kernels = 5 + 5 + 6;      // kernels every launch runs (conditional bodies excluded)
+      // kernels every launch runs (conditional bodies excluded)
+      *kernels = fuse_krylov() ? 5 + 5 + 3 : 5 + 5 + 6;
       return cudaSuccess;
     }
     cudaGetLastError();
