@@ -40,7 +40,7 @@ REF_ITERS_64 = 123
 # DRAM bytes (read + write) of one complex64 64^3 matvec (five passes), from
 # the ncu capture summarised in profiles/matvec_c64_sphere64_passes.md; the
 # passes' intermediates stay in L2, so this is below the algorithmic bytes.
-MATVEC64_C64_DRAM_BYTES = 103.5e6
+MATVEC64_C64_DRAM_BYTES = 103.9e6
 
 
 def problem(n=N_BOX, m=M_REF):
@@ -157,13 +157,21 @@ def barrier(ws):
 
 
 def max_over_ranks(ws, v):
+    """Largest value over the ranks (the slowest rank's time)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_value(ws, units_per_rank, seconds):
+    """Whole-job throughput of independent replicas: all ranks' units over
+    the slowest rank's time."""
+    return units_per_rank * ws / max_over_ranks(ws, seconds)
 
 
 # --------------------------------------------------------------------------

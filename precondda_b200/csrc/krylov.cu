@@ -183,7 +183,9 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
 }
 
 // u, z, r, x updates (Gpbicgstab.py:1038-1057) and ||r||^2, <rhat, r>
-template <typename R>
+// SETC: the kernel switches the graph's conditional residual matvecs (a
+// separate instantiation, so the plain one stays visible to profilers)
+template <typename R, bool SETC>
 __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB, unsigned long long cond_true, unsigned long long cond_reset) {
   typedef typename CT<R>::T C;
@@ -232,13 +234,15 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
     S.cur_x = nxt;
     S.vec[V_X] = S.vec[V_XA + nxt];
     if (!S.flag_true_res) ctrl_check(S, tot[0], make_double2(tot[1], tot[2]));
-    if (cond_true && S.flag_true_res && !S.done) cudaGraphSetConditional(cond_true, 1);
-    if (cond_reset && S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
+    if constexpr (SETC) {
+      if (S.flag_true_res && !S.done) cudaGraphSetConditional(cond_true, 1);
+      if (S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
+    }
   }
 }
 
 // ||r||^2, <rhat, r> after the i == 1 true residual (Gpbicgstab.py:1059-1076)
-template <typename R>
+template <typename R, bool SETC>
 __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB, unsigned long long cond_reset) {
   typedef typename CT<R>::T C;
@@ -257,7 +261,9 @@ __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, dou
   double tot[3];
   if (reduce_last<3>(acc, tot, red, cnt, inst, RB) && threadIdx.x == 0) {
     ctrl_check(S, tot[0], make_double2(tot[1], tot[2]));
-    if (cond_reset && S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
+    if constexpr (SETC) {
+      if (S.flag_reset && S.flag_reset_res && !S.done) cudaGraphSetConditional(cond_reset, 1);
+    }
   }
 }
 
@@ -324,11 +330,17 @@ template <typename R> void launch_zeta(const KrylovLaunch& k, cudaStream_t s) {
   note_launch(s, 1);
 }
 template <typename R> void launch_uzrx(const KrylovLaunch& k, cudaStream_t s) {
-  k_uzrx<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_true, k.cond_reset);
+  if (k.cond_true && k.cond_reset)
+    k_uzrx<R, true><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_true, k.cond_reset);
+  else
+    k_uzrx<R, false><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0, 0);
   note_launch(s, 1);
 }
 template <typename R> void launch_norm(const KrylovLaunch& k, cudaStream_t s) {
-  k_norm<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_reset);
+  if (k.cond_reset)
+    k_norm<R, true><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_reset);
+  else
+    k_norm<R, false><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0);
   note_launch(s, 1);
 }
 template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s) {

@@ -222,3 +222,20 @@ def test_device_incident_field_matches_host():
     got = incident_field_device((9, 7, 5), 0.03, k * kdir, pol).cpu().numpy()
     ref = O.incident_field((9, 7, 5), 0.03, k, kdir, pol)
     assert np.abs(got - ref).max() < 1e-13
+
+
+@pytest.mark.parametrize("n", [11, 20])
+def test_fused_krylov_steps_match_oracle(n, monkeypatch):
+    """alpha, s/y and zeta/eta carried by the matvec passes (DDA_FUSE_KRYLOV=1)
+    follow the reference's recurrence like the separate kernels do."""
+    P = _pkg()
+    monkeypatch.setenv("DDA_FUSE_KRYLOV", "1")
+    k, d, alpha, E = _sphere_problem(n, 1.6 + 0.05j)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    it_ref, P_ref, low_ref, _ = O.solve_gpbicgstab((n, n, n), ia, G, E, mask, 100, 500, target=1e-6)
+    op = P.DDAOperator(ia, k, d, dtype=C128, L_=(2 * n,) * 3 if n == 20 else None)
+    Pg, info = op.solve(E, tol=1e-6, max_iter=500, ratio=100)
+    assert info.iters == it_ref
+    assert _rel(Pg.cpu().numpy(), P_ref) < 1e-8
+    Pm, im = op.solve(E, tol=1e-6, max_iter=500, ratio=100, precision="mixed")
+    assert im.status == "converged" and im.true_relres <= 1e-6

@@ -177,3 +177,27 @@ def test_mixed_pool_matches_batched_mixed_solve():
     Pn = r.P.cpu().numpy()
     assert np.linalg.norm(Pn - Pb.cpu().numpy()) / np.linalg.norm(Pn) < 1e-5
     srv.close()
+
+
+def test_slot_pool_argument_errors():
+    import precondda_b200 as P
+    from precondda_b200.serve import SlotPool
+    from precondda_b200._lib import DDAError
+    n = 8
+    k, d, alpha, E = _sphere(n, 1.5 + 0.01j)
+    ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    L = (16, 16, 16)
+    g = P.green_octant((n, n, n), k, d, L, 1.0 / 4096, C128, layout="engine")
+    pool = SlotPool((n, n, n), L, 2, "c128")
+    assert pool.poll() == [] and pool.running == 0
+    pool.admit(0, g, torch.tensor(ia, device="cuda"), torch.tensor(E, device="cuda"), tol=1e-6)
+    with pytest.raises(DDAError):
+        pool.admit(0, g, torch.tensor(ia, device="cuda"), torch.tensor(E, device="cuda"))   # occupied
+    with pytest.raises(DDAError):
+        pool.admit(5, g, torch.tensor(ia, device="cuda"), torch.tensor(E, device="cuda"))   # no such slot
+    assert pool.free_slot() == 1
+    res = _run_pool(pool)
+    assert res[0][0].status == "converged"
+    pool.close()
+    with pytest.raises(Exception):
+        SlotPool((n, n, n), (14, 16, 16), 1, "c128")       # FFT length < 2n
