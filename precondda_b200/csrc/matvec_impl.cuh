@@ -446,68 +446,59 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
   const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
   const C* tl = t1 + line * (long long)LZ * 3 + c;
   C* sl = s + l * 3 * SH::LP + c;
-  auto ld = [&](int, int pos) -> C { return ok ? __ldcg(tl + pos * 3) : czero<C>(); };
-  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
-  auto stf = [&](int, int pos, C v) { if (DH || pos < nz) sl[ppad(pos) * 3] = v; };
-  C a[P::E];
-  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
-  __syncthreads();
-  // combine: consecutive threads take consecutive (site, component); the
-  // (line, offset) split of idx advances without divisions
-  const long long site_base = (long long)blockIdx.x * nl * nz;
-  const int nlb = (int)min((long long)nl, nlines - (long long)blockIdx.x * nl);
-  const int per = nz * 3;
-  const int nv = nlb * per;
-  const C* __restrict__ xg = (const C*)S.vec[in_id] + site_base * 3;
-  C* __restrict__ yg = (C*)S.vec[out_id] + site_base * 3;
-  const C* __restrict__ iag = (const C*)S.inva + site_base;
-  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site_base * 3 : nullptr;
+  // the combine runs on the last stage's registers: for a fixed leg the
+  // lanes (component fastest, then t) hold consecutive sites of a line, so
+  // the stores below are contiguous
+  const long long site0 = line * nz;
+  const C* __restrict__ xg = (const C*)S.vec[in_id] + site0 * 3 + c;
+  C* __restrict__ yg = (C*)S.vec[out_id] + site0 * 3 + c;
+  const C* __restrict__ iag = (const C*)S.inva + site0;
+  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site0 * 3 + c : nullptr;
   // fused dot products of the output (post): <rhat, v> for alpha, or the
   // zeta / eta dots of t with s and y
   const bool first = (S.iter == 0) || S.was_reset;
-  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT] + site_base * 3
-                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] + site_base * 3 : nullptr);
-  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] + site_base * 3 : nullptr;
+  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT] + site0 * 3 + c
+                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] + site0 * 3 + c : nullptr);
+  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] + site0 * 3 + c : nullptr;
   double acc[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc[k] = 0.0;
-  int ll = threadIdx.x / per, j = threadIdx.x - (threadIdx.x / per) * per;
-  for (int idx = threadIdx.x; idx < nv; idx += blockDim.x) {
-    const int pos = j / 3, cc = j - 3 * pos;
-    C v = s[ll * 3 * SH::LP + ppad(pos) * 3 + cc];
+  auto ld = [&](int, int pos) -> C { return ok ? __ldcg(tl + pos * 3) : czero<C>(); };
+  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
+  auto stf = [&](int, int pos, C v) {
+    if (!(ok && (DH || pos < nz))) return;
     C r;
     if (mode == MV_CONV) {
       r = v;
     } else {
-      const C a_ = __ldg(iag + ll * nz + pos);     // shared by 3 lanes: keep it in L1
+      const C a_ = __ldg(iag + pos);        // shared by the 3 component lanes
       const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
       if (!msk) v = czero<C>();
       if (mode == MV_CONV_MASKED) {
         r = v;
       } else {
-        r = csub(cmul(a_, __ldcg(xg + idx)), v);
-        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + idx), r);
+        r = csub(cmul(a_, __ldcg(xg + pos * 3)), v);
+        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + pos * 3), r);
       }
     }
-    __stcg(yg + idx, r);
+    __stcg(yg + pos * 3, r);
     if (post == MV_POST_ALPHA) {
-      const C h = __ldcg(d0 + idx);
+      const C h = __ldcg(d0 + pos * 3);
       acc[0] += (double)h.x * r.x + (double)h.y * r.y;
       acc[1] += (double)h.x * r.y - (double)h.y * r.x;
     } else if (post == MV_POST_ZETA) {
-      const C sv = __ldcg(d0 + idx);
+      const C sv = __ldcg(d0 + pos * 3);
       if (first) {
         acc[0] += (double)r.x * r.x + (double)r.y * r.y;
         acc[1] += (double)r.x * sv.x + (double)r.y * sv.y;
         acc[2] += (double)r.x * sv.y - (double)r.y * sv.x;
       } else {
-        const C yv = __ldcg(d1 + idx);
-        zeta_dots_acc(acc, r, sv, yv);
+        zeta_dots_acc(acc, r, sv, __ldcg(d1 + pos * 3));
       }
     }
-    j += blockDim.x;
-    while (j >= per) { j -= per; ++ll; }
-  }
+  };
+  C a[P::E];
+  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
   if (post == MV_POST_NONE) return;
   double tot[8];
   if (reduce_last_n<8>(acc, tot, red, cnt, inst, (int)gridDim.x, blockDim.x) && threadIdx.x == 0) {
