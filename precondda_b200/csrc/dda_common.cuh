@@ -95,6 +95,16 @@ struct InstState {
   const void* inva;    // inverse polarizability per site (N complex)
   void* t1;            // scratch (nx,ny,Lz,3)
   void* t2;            // scratch (nx,Ly,Lz,3)
+  // Occupied-site storage: when cidx is set, every vector of the instance
+  // holds only the M sites with inv_alpha != 0 (site-major, component
+  // fastest) and cidx[site] is the site's rank among them, -1 for an empty
+  // site.  Empty sites carry zero in every Krylov vector of the reference's
+  // recurrence (the right-hand side and every operator row are masked), so
+  // dropping them changes no value.  nv = vector length in complex elements
+  // (3M, or 3N when cidx is null).
+  const int* cidx;
+  long long nv;
+  void* out;           // solution destination (dense (nx,ny,nz,3))
   // scalars (complex double)
   double2 rho1, rho0, alpha, beta, zeta, eta;
   double initial_norm, lowest, current, prev_lowest, first, target, ratio;

@@ -90,13 +90,17 @@ struct BatchWs {
   InstState* h_st[2] = {nullptr, nullptr};   // pinned status buffers
   double* red = nullptr;
   unsigned* cnt = nullptr;
+  int* cidx = nullptr;           // nb * nsite occupied-site maps (full workspaces)
+  int* bcount = nullptr;         // nb * site_blocks(nsite) block offsets
   double* d_out = nullptr;
   double* h_out = nullptr;
   cudaGraphExec_t gexec = nullptr;
   double graph_gscale = 0.0;
   long long graph_kernels = 0;
   int alloc(Ctx& c, int dtype, const Geo& g, int nb, bool full);
-  void base_state(int j, InstState& S) const;
+  // state of instance j: vector slots and scratch; with `sites` the
+  // instance stores occupied sites only (its map is built on the device)
+  void base_state(int j, InstState& S, bool sites = false) const;
   ~BatchWs();
 };
 
@@ -172,6 +176,15 @@ template <typename R>
 void launch_norm2(InstState* st, int id, int nb, long long n3, double* red, unsigned* cnt, int RB, double* out,
                   cudaStream_t s, const int* act);
 int grid_for(long long n, int nb, int num_sms);
+// occupied-site maps of the instances (S.cidx set on the host beforehand)
+int site_blocks(long long nsite);
+template <typename R>
+void launch_site_map(InstState* st, int nb, long long nsite, int* bcount, cudaStream_t s, const int* act);
+// dense solution of each finished instance into S.out
+template <typename R>
+void launch_store_solution(InstState* st, int nb, long long n3, int num_sms, cudaStream_t s, const int* act);
+// whether solver workspaces store occupied sites only (DDA_NO_COMPRESS=1: dense)
+bool compress_sites();
 
 // Lattice setup kernels (lattice.cu).
 int voxelize(const dda_shape* shapes_dev, int nshape, int nx, int ny, int nz, double d, const double* origin,

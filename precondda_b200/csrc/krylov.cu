@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(KNT) k_init(InstState* st, const int* act, dou
   C* zs[7] = {(C*)S.vec[V_V], (C*)S.vec[V_T], (C*)S.vec[V_S], (C*)S.vec[V_SPREV], (C*)S.vec[V_U], (C*)S.vec[V_Z],
               (C*)S.vec[V_W]};
   double acc[1] = {0.0};
-  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+  grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C bv = b[i];
     r[i] = bv; rh[i] = bv; p[i] = bv;
     xa[i] = czero<C>();
@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(KNT) k_alpha(InstState* st, const int* act, do
   const C* __restrict__ rh = (const C*)S.vec[V_RHAT];
   const C* __restrict__ v = (const C*)S.vec[V_V];
   double acc[2] = {0.0, 0.0};
-  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+  grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C a = rh[i], b = v[i];
     acc[0] += (double)a.x * b.x + (double)a.y * b.y;
     acc[1] += (double)a.x * b.y - (double)a.y * b.x;
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(KNT) k_sy(InstState* st, const int* act, long 
   C* __restrict__ s = (C*)S.vec[V_S];
   C* __restrict__ y = (C*)S.vec[V_Y];
   const C al = tocr<C>(S.alpha);
-  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
+  grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
     const C sv = csub(r[i], cmul(al, v[i]));
     s[i] = sv;
     y[i] = csub(csub(sp[i], sv), cmul(al, w[i]));
@@ -166,14 +166,14 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc[k] = 0.0;
   if (first) {
-    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+    grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C tv = t[i], sv = s[i];
       acc[0] += (double)tv.x * tv.x + (double)tv.y * tv.y;            // <t,t>
       acc[1] += (double)tv.x * sv.x + (double)tv.y * sv.y;            // <t,s>
       acc[2] += (double)tv.x * sv.y - (double)tv.y * sv.x;
     });
   } else {
-    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+    grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C tv = t[i], sv = s[i], yv = y[i];
       zeta_dots_acc(acc, tv, sv, yv);
     });
@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
   C* __restrict__ z = (C*)S.vec[V_Z];
   const C ze = tocr<C>(S.zeta), et = tocr<C>(S.eta), al = tocr<C>(S.alpha), be = tocr<C>(S.beta);
   double acc[3] = {0.0, 0.0, 0.0};
-  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+  grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     C un, zn, rn;
     if (first) {
       un = cmul(ze, v[i]);
@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, dou
   const C* __restrict__ r = (const C*)S.vec[V_R];
   const C* __restrict__ rh = (const C*)S.vec[V_RHAT];
   double acc[3] = {0.0, 0.0, 0.0};
-  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+  grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
     const C rn = r[i], h = rh[i];
     acc[0] += (double)rn.x * rn.x + (double)rn.y * rn.y;
     acc[1] += (double)h.x * rn.x + (double)h.y * rn.y;
@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(KNT) k_fin(InstState* st, const int* act, unsi
   C* __restrict__ p = (C*)S.vec[V_P];
   if (reset) {
     C* __restrict__ rh = (C*)S.vec[V_RHAT];
-    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+    grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       const C rv = r[i];
       rh[i] = rv; p[i] = rv;
     });
@@ -290,7 +290,7 @@ __global__ void __launch_bounds__(KNT) k_fin(InstState* st, const int* act, unsi
     const C* __restrict__ u = (const C*)S.vec[V_U];
     C* __restrict__ w = (C*)S.vec[V_W];
     const C be = tocr<C>(S.beta);
-    grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
+    grid_loop<KU>(S.nv, (long long)blockIdx.x * KNT + threadIdx.x, (long long)RB * KNT, [&](long long i) {
       w[i] = cadd(t[i], cmul(be, v[i]));
       p[i] = cadd(r[i], cmul(be, csub(p[i], u[i])));
     });

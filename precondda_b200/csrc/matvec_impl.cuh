@@ -94,6 +94,13 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
   const long long line = (long long)blockIdx.x * nl + l;
   const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
   const long long base = line * nz * 3 + c;
+  // occupied-site vectors: element (site, c) lives at 3 cidx[site] + c
+  const int* __restrict__ cid = S.cidx ? S.cidx + line * nz : nullptr;
+  auto eidx = [&](int pos) -> long long {
+    if (!cid) return base + (long long)pos * 3;
+    const int k = cid[pos];
+    return k < 0 ? -1 : 3LL * k + c;
+  };
   C* tl = t1 + line * (long long)LZ * 3 + c;
   C* sl = s + l * 3 * SH::LP + c;
   auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
@@ -111,7 +118,8 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
     const C al = mk<C>(S.alpha.x, S.alpha.y);
     auto ld = [&](int, int pos) -> C {
       if (!(ok && (ZH || pos < nz))) return czero<C>();
-      const long long i = base + (long long)pos * 3;
+      const long long i = eidx(pos);
+      if (i < 0) return czero<C>();
       const C sv = csub(__ldcg(r + i), cmul(al, __ldcg(v + i)));
       __stcg(so + i, sv);
       __stcg(yo + i, csub(csub(__ldcg(sp + i), sv), cmul(al, __ldcg(w + i))));
@@ -119,8 +127,11 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
     };
     rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
   } else {
-    const C* xl = x + base;
-    auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nz)) ? __ldcg(xl + pos * 3) : czero<C>(); };
+    auto ld = [&](int, int pos) -> C {
+      if (!(ok && (ZH || pos < nz))) return czero<C>();
+      const long long i = eidx(pos);
+      return i < 0 ? czero<C>() : __ldcg(x + i);
+    };
     rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
   }
 }
@@ -450,16 +461,18 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
   // lanes (component fastest, then t) hold consecutive sites of a line, so
   // the stores below are contiguous
   const long long site0 = line * nz;
-  const C* __restrict__ xg = (const C*)S.vec[in_id] + site0 * 3 + c;
-  C* __restrict__ yg = (C*)S.vec[out_id] + site0 * 3 + c;
+  const C* __restrict__ xg = (const C*)S.vec[in_id];
+  C* __restrict__ yg = (C*)S.vec[out_id];
   const C* __restrict__ iag = (const C*)S.inva + site0;
-  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] + site0 * 3 + c : nullptr;
+  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] : nullptr;
+  // occupied-site vectors: element (site, c) lives at 3 cidx[site] + c
+  const int* __restrict__ cid = S.cidx ? S.cidx + site0 : nullptr;
   // fused dot products of the output (post): <rhat, v> for alpha, or the
   // zeta / eta dots of t with s and y
   const bool first = (S.iter == 0) || S.was_reset;
-  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT] + site0 * 3 + c
-                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] + site0 * 3 + c : nullptr);
-  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] + site0 * 3 + c : nullptr;
+  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT]
+                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] : nullptr);
+  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] : nullptr;
   double acc[8];
 #pragma unroll
   for (int k = 0; k < 8; ++k) acc[k] = 0.0;
@@ -467,6 +480,12 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
   auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
   auto stf = [&](int, int pos, C v) {
     if (!(ok && (DH || pos < nz))) return;
+    long long e = (site0 + pos) * 3 + c;
+    if (cid) {
+      const int k = cid[pos];
+      if (k < 0) return;               // empty site: not stored
+      e = 3LL * k + c;
+    }
     C r;
     if (mode == MV_CONV) {
       r = v;
@@ -477,23 +496,23 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
       if (mode == MV_CONV_MASKED) {
         r = v;
       } else {
-        r = csub(cmul(a_, __ldcg(xg + pos * 3)), v);
-        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + pos * 3), r);
+        r = csub(cmul(a_, __ldcg(xg + e)), v);
+        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + e), r);
       }
     }
-    __stcg(yg + pos * 3, r);
+    __stcg(yg + e, r);
     if (post == MV_POST_ALPHA) {
-      const C h = __ldcg(d0 + pos * 3);
+      const C h = __ldcg(d0 + e);
       acc[0] += (double)h.x * r.x + (double)h.y * r.y;
       acc[1] += (double)h.x * r.y - (double)h.y * r.x;
     } else if (post == MV_POST_ZETA) {
-      const C sv = __ldcg(d0 + pos * 3);
+      const C sv = __ldcg(d0 + e);
       if (first) {
         acc[0] += (double)r.x * r.x + (double)r.y * r.y;
         acc[1] += (double)r.x * sv.x + (double)r.y * sv.y;
         acc[2] += (double)r.x * sv.y - (double)r.y * sv.x;
       } else {
-        zeta_dots_acc(acc, r, sv, __ldcg(d1 + pos * 3));
+        zeta_dots_acc(acc, r, sv, __ldcg(d1 + e));
       }
     }
   };

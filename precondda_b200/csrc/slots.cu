@@ -70,9 +70,10 @@ static int put_state(dda_slots* p, BatchWs& w, int j, const InstState& S) {
 // (Re)initialise the complex64 / complex128 Krylov state of slot j from its
 // right-hand side (already in V_B for mixed pools, in V_TMP otherwise).
 static int arm_solver(dda_slots* p, int j, const void* ghat, const void* inva, const void* e_inc, double target,
-                      int max_iter, double ratio, bool from_tmp) {
+                      int max_iter, double ratio, bool from_tmp, void* out) {
   InstState S;
-  p->w.base_state(j, S);
+  p->w.base_state(j, S, compress_sites());
+  S.out = out;
   S.ghat = ghat;
   S.inva = inva;
   if (from_tmp) S.vec[V_TMP] = (void*)e_inc;
@@ -205,12 +206,16 @@ int dda_slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_in
   Ctx& c = p->ctx->c;
   if (p->prec != DDA_PREC_MIXED) {
     I.p_out = in->p_out;
-    if ((rc = arm_solver(p, slot, in->ghat, in->inv_alpha, in->e_inc, tol, max_iter, ratio, true))) return rc;
+    if ((rc = arm_solver(p, slot, in->ghat, in->inv_alpha, in->e_inc, tol, max_iter, ratio, true, in->p_out)))
+      return rc;
     KrylovLaunch k{p->w.d_st, act, 1, p->w.red, p->w.cnt, (long long)p->w.n3, p->w.RB};
+    const bool sites = compress_sites();
     if (p->prec == DDA_PREC_C128) {
+      if (sites) launch_site_map<double>(p->w.d_st, 1, p->g.nsite, p->w.bcount, p->s, act);
       launch_make_b<double>(p->w.d_st, 1, p->g.nsite, V_TMP, V_B, c.num_sms, p->s, act);
       launch_init<double>(k, p->s);
     } else {
+      if (sites) launch_site_map<float>(p->w.d_st, 1, p->g.nsite, p->w.bcount, p->s, act);
       launch_make_b<float>(p->w.d_st, 1, p->g.nsite, V_TMP, V_B, c.num_sms, p->s, act);
       launch_init<float>(k, p->s);
     }
@@ -229,7 +234,9 @@ int dda_slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_in
     launch_norm2<double>(p->w128.d_st, V_B, 1, (long long)p->w128.n3, p->w128.red, p->w128.cnt, p->w128.RB,
                          p->d_bnorm, p->s, act);
     cudaMemcpyAsync(H.vec[V_R], H.vec[V_B], bytes, cudaMemcpyDeviceToDevice, p->s);
-    if ((rc = arm_solver(p, slot, lo->ghat, lo->inv_alpha, nullptr, inner_tol, max_iter, ratio, false))) return rc;
+    if ((rc = arm_solver(p, slot, lo->ghat, lo->inv_alpha, nullptr, inner_tol, max_iter, ratio, false, nullptr)))
+      return rc;
+    if (compress_sites()) launch_site_map<float>(p->w.d_st, 1, p->g.nsite, p->w.bcount, p->s, act);
     launch_down(p->w.d_st, V_B, p->w128.d_st, V_R, 1, (long long)p->w.n3, c.num_sms, p->s, act);
     KrylovLaunch k{p->w.d_st, act, 1, p->w.red, p->w.cnt, (long long)p->w.n3, p->w.RB};
     launch_init<float>(k, p->s);
@@ -278,15 +285,17 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
     I.state = 0;
   };
   if (p->prec != DDA_PREC_MIXED) {
-    const size_t bytes = p->w.n3 * p->w.esz;
+    if (!done.empty()) {
+      int rc = set_act(p, 0, done);
+      if (rc) return rc;
+      if (p->prec == DDA_PREC_C128)
+        launch_store_solution<double>(p->w.d_st, (int)done.size(), (long long)p->w.n3, c.num_sms, p->s, p->d_act);
+      else
+        launch_store_solution<float>(p->w.d_st, (int)done.size(), (long long)p->w.n3, c.num_sms, p->s, p->d_act);
+    }
     for (int j : done) {
       const InstState& S = p->w.h_st[1][j];
       SlotInfo& I = p->info[j];
-      const void* src = nullptr;
-      if (S.status == ST_CONVERGED) src = S.vec[V_X];
-      else if (S.best_x >= 0) src = S.vec[V_XA + S.best_x];
-      if (src) cudaMemcpyAsync(I.p_out, src, bytes, cudaMemcpyDeviceToDevice, p->s);
-      else cudaMemsetAsync(I.p_out, 0, bytes, p->s);
       I.iters = S.ret_iters;
       I.resets = S.reset_count;
       I.first_rel = S.initial_norm > 0 ? S.first / S.initial_norm : NAN;
@@ -330,11 +339,12 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
         SlotInfo& I = p->info[j];
         const InstState& S = p->w.h_st[1][j];
         const double tj = std::max(I.inner_tol, std::min(0.5, 0.3 * I.tol / I.relres));
-        if ((rc = arm_solver(p, j, S.ghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false))) return rc;
+        if ((rc = arm_solver(p, j, S.ghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false, nullptr))) return rc;
       }
       if ((rc = set_act(p, 1, rearm))) return rc;
       const int* act2 = p->d_act + p->n;
       const int r = (int)rearm.size();
+      if (compress_sites()) launch_site_map<float>(p->w.d_st, r, p->g.nsite, p->w.bcount, p->s, act2);
       launch_down(p->w.d_st, V_B, p->w128.d_st, V_R, r, (long long)p->w.n3, c.num_sms, p->s, act2);
       KrylovLaunch k{p->w.d_st, act2, r, p->w.red, p->w.cnt, (long long)p->w.n3, p->w.RB};
       launch_init<float>(k, p->s);

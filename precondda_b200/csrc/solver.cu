@@ -66,6 +66,7 @@ BatchWs::~BatchWs() {
   if (gexec) cudaGraphExecDestroy(gexec);
   cudaFree(vecs); cudaFree(scratch); cudaFree(d_st); cudaFreeHost(h_st[0]); cudaFreeHost(h_st[1]);
   cudaFree(red); cudaFree(cnt); cudaFree(d_out); cudaFreeHost(h_out);
+  cudaFree(cidx); cudaFree(bcount);
 }
 
 int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
@@ -85,7 +86,9 @@ int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
       cudaMalloc((void**)&red, (size_t)nb * std::max<long long>(RB, pc.grid1) * KRED * sizeof(double)) != cudaSuccess ||
       cudaMalloc((void**)&cnt, nb * sizeof(unsigned)) != cudaSuccess ||
       cudaMalloc((void**)&d_out, nb * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost((void**)&h_out, nb * sizeof(double)) != cudaSuccess) {
+      cudaMallocHost((void**)&h_out, nb * sizeof(double)) != cudaSuccess ||
+      (full && (cudaMalloc((void**)&cidx, (size_t)nb * g.nsite * sizeof(int)) != cudaSuccess ||
+                cudaMalloc((void**)&bcount, (size_t)nb * site_blocks(g.nsite) * sizeof(int)) != cudaSuccess))) {
     cudaGetLastError();
     set_error("solver workspace: out of device memory");
     return DDA_ERR_OOM;
@@ -95,9 +98,16 @@ int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
   return DDA_OK;
 }
 
+bool compress_sites() {
+  const char* e = getenv("DDA_NO_COMPRESS");
+  return !(e && *e == '1');
+}
+
 // base InstState of instance j: vector slots and scratch
-void BatchWs::base_state(int j, InstState& S) const {
+void BatchWs::base_state(int j, InstState& S, bool sites) const {
   std::memset(&S, 0, sizeof(S));
+  S.nv = (long long)n3;
+  S.cidx = (sites && cidx) ? cidx + (size_t)j * g.nsite : nullptr;
   const int* slots = full ? kFullSlots : kLightSlots;
   char* v0 = (char*)vecs + (size_t)j * nslot * n3 * esz;
   for (int q = 0; q < nslot; ++q) S.vec[slots[q]] = v0 + (size_t)q * n3 * esz;
@@ -354,11 +364,13 @@ int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, i
   BatchWs* w = c.workspace(dtype, g, nb, true, &err);
   if (!w) return err;
   InstState* H = w->h_st[0];
+  const bool sites = compress_sites();
   for (int j = 0; j < nb; ++j) {
-    w->base_state(j, H[j]);
+    w->base_state(j, H[j], sites);
     H[j].ghat = inst[j].ghat;
     H[j].inva = inst[j].inv_alpha;
     H[j].vec[V_TMP] = (void*)inst[j].e_inc;
+    H[j].out = inst[j].p_out;
     H[j].target = target;
     H[j].ratio = ratio;
     H[j].max_iter = max_iter;
@@ -368,22 +380,17 @@ int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, i
   DDA_CUDA_OK(cudaEventRecord(c.ev_user, user));
   DDA_CUDA_OK(cudaStreamWaitEvent(s, c.ev_user, 0));
   DDA_CUDA_OK(cudaMemcpyAsync(w->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+  if (sites) launch_site_map<R>(w->d_st, nb, g.nsite, w->bcount, s, nullptr);
   launch_make_b<R>(w->d_st, nb, g.nsite, V_TMP, V_B, c.num_sms, s, nullptr);
   KrylovLaunch k{w->d_st, nullptr, nb, w->red, w->cnt, (long long)w->n3, w->RB};
   launch_init<R>(k, s);
   DDA_CUDA_OK(cudaGetLastError());
   int rc = run_iterations<R>(c, *w, gscale, 4);
   if (rc) return rc;
-  const size_t bytes = w->n3 * w->esz;
-  for (int j = 0; j < nb; ++j) {
-    const InstState& S = w->h_st[0][j];
-    const void* src = nullptr;
-    if (S.status == ST_CONVERGED) src = S.vec[V_X];
-    else if (S.best_x >= 0) src = S.vec[V_XA + S.best_x];
-    if (src) DDA_CUDA_OK(cudaMemcpyAsync(inst[j].p_out, src, bytes, cudaMemcpyDeviceToDevice, s));
-    else DDA_CUDA_OK(cudaMemsetAsync(inst[j].p_out, 0, bytes, s));
-    if (res) fill_result(S, res[j]);
-  }
+  launch_store_solution<R>(w->d_st, nb, (long long)w->n3, c.num_sms, s, nullptr);
+  DDA_CUDA_OK(cudaGetLastError());
+  for (int j = 0; j < nb; ++j)
+    if (res) fill_result(w->h_st[0][j], res[j]);
   DDA_CUDA_OK(cudaEventRecord(c.ev_done, s));
   DDA_CUDA_OK(cudaStreamWaitEvent(user, c.ev_done, 0));
   return DDA_OK;
@@ -436,12 +443,13 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
   for (int j = 0; j < nb; ++j)
     DDA_CUDA_OK(cudaMemcpyAsync(H[j].vec[V_R], H[j].vec[V_B], bytes128, cudaMemcpyDeviceToDevice, s));
   InstState* H64 = w64->h_st[0];
+  const bool sites = compress_sites();
   for (int sweep = 0; sweep < max_outer; ++sweep) {
     int nact = 0;
     for (int j = 0; j < nb; ++j) nact += active[j];
     if (!nact) break;
     for (int j = 0; j < nb; ++j) {
-      w64->base_state(j, H64[j]);
+      w64->base_state(j, H64[j], sites);
       H64[j].ghat = i64[j].ghat;
       H64[j].inva = i64[j].inv_alpha;
       // inner target: inner_tol, relaxed on later sweeps to what the FP64
@@ -456,6 +464,7 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
     }
     DDA_CUDA_OK(cudaMemcpyAsync(w64->d_st, H64, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
     DDA_CUDA_OK(cudaMemcpyAsync(w128->d_st, H, nb * sizeof(InstState), cudaMemcpyHostToDevice, s));
+    if (sites) launch_site_map<float>(w64->d_st, nb, g.nsite, w64->bcount, s, nullptr);
     launch_down(w64->d_st, V_B, w128->d_st, V_R, nb, (long long)w64->n3, c.num_sms, s, nullptr);
     KrylovLaunch k{w64->d_st, nullptr, nb, w64->red, w64->cnt, (long long)w64->n3, w64->RB};
     launch_init<float>(k, s);

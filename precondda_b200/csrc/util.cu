@@ -17,10 +17,17 @@ __global__ void __launch_bounds__(KNT) k_make_b(InstState* st, const int* act, l
   const C* __restrict__ e = (const C*)S.vec[src_id];
   const C* __restrict__ ia = (const C*)S.inva;
   C* __restrict__ b = (C*)S.vec[dst_id];
+  const int* __restrict__ cid = S.cidx;
   grid_loop<KU>(nsite * 3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
-    const C a = ia[i / 3];
-    const bool m = (a.x != (R)0) || (a.y != (R)0);
-    b[i] = m ? e[i] : czero<C>();
+    const long long site = i / 3;
+    if (cid) {
+      const int k = cid[site];
+      if (k >= 0) b[3LL * k + (i - 3 * site)] = e[i];
+    } else {
+      const C a = ia[site];
+      const bool m = (a.x != (R)0) || (a.y != (R)0);
+      b[i] = m ? e[i] : czero<C>();
+    }
   });
 }
 
@@ -32,8 +39,17 @@ __global__ void __launch_bounds__(KNT) k_down(InstState* dst, int did, const Ins
   if (!D.active) return;
   const double2* __restrict__ s = (const double2*)src[j].vec[sid];
   float2* __restrict__ d = (float2*)D.vec[did];
-  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT)
-    d[i] = make_float2((float)s[i].x, (float)s[i].y);
+  const int* __restrict__ cid = D.cidx;
+  for (long long i = (long long)blockIdx.x * KNT + threadIdx.x; i < n3; i += (long long)gridDim.x * KNT) {
+    const float2 v = make_float2((float)s[i].x, (float)s[i].y);
+    if (cid) {
+      const long long site = i / 3;
+      const int k = cid[site];
+      if (k >= 0) d[3LL * k + (i - 3 * site)] = v;
+    } else {
+      d[i] = v;
+    }
+  }
 }
 
 // solution of a finished complex64 solve: the current iterate when it
@@ -53,12 +69,149 @@ __global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const 
   const float2* __restrict__ e = sol64(S);
   if (!e) return;
   double2* __restrict__ x = (double2*)st128[j].vec[xid];
+  const int* __restrict__ cid = S.cidx;
   grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
-    const float2 v = e[i];
+    long long src = i;
+    if (cid) {
+      const long long site = i / 3;
+      const int k = cid[site];
+      if (k < 0) return;
+      src = 3LL * k + (i - 3 * site);
+    }
+    const float2 v = e[src];
     double2 a = x[i];
     a.x += (double)v.x; a.y += (double)v.y;
     x[i] = a;
   });
+}
+
+// P (dense, S.out) = solution of a finished solve: the current iterate when
+// it converged, else the best one, else zero (Gpbicgstab.py:1162-1201);
+// expanded from occupied-site storage when the instance uses it
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_store_solution(const InstState* st, const int* act, long long n3) {
+  typedef typename CT<R>::T C;
+  const InstState& S = st[kinst(act)];
+  if (!S.active || !S.out) return;
+  const C* __restrict__ e = nullptr;
+  if (S.status == ST_CONVERGED) e = (const C*)S.vec[V_X];
+  else if (S.best_x >= 0) e = (const C*)S.vec[V_XA + S.best_x];
+  C* __restrict__ out = (C*)S.out;
+  const int* __restrict__ cid = S.cidx;
+  grid_loop<KU>(n3, (long long)blockIdx.x * KNT + threadIdx.x, (long long)gridDim.x * KNT, [&](long long i) {
+    C v = czero<C>();
+    if (e) {
+      if (cid) {
+        const long long site = i / 3;
+        const int k = cid[site];
+        if (k >= 0) v = e[3LL * k + (i - 3 * site)];
+      } else {
+        v = e[i];
+      }
+    }
+    out[i] = v;
+  });
+}
+
+// ---------------------------------------------------------------------------
+// occupied-site map: cidx[site] = rank of the site among the sites with
+// inv_alpha != 0 (site order), -1 for an empty site; S.nv = 3 x count.
+// Three passes over blocks of kSiteBlock sites: count, scan the block
+// counts, write the ranks.  Every step has a fixed order (deterministic).
+// ---------------------------------------------------------------------------
+constexpr int kSitePer = 4;                      // sites per thread
+constexpr int kSiteBlock = KNT * kSitePer;       // sites per CTA
+
+template <typename R>
+__device__ __forceinline__ int site_flags(const InstState& S, long long base, long long nsite, bool* f) {
+  typedef typename CT<R>::T C;
+  const C* __restrict__ ia = (const C*)S.inva;
+  int n = 0;
+#pragma unroll
+  for (int j = 0; j < kSitePer; ++j) {
+    const long long site = base + j;
+    bool m = false;
+    if (site < nsite) {
+      const C a = ia[site];
+      m = (a.x != (R)0) || (a.y != (R)0);
+    }
+    f[j] = m;
+    n += m;
+  }
+  return n;
+}
+
+// exclusive prefix sum of v over the CTA (KNT threads); *total = CTA sum
+__device__ __forceinline__ int block_excl_scan(int v, int* total) {
+  __shared__ int wsum[KNW];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  int woff = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < KNW; ++w) {
+    if (w < wid) woff += wsum[w];
+    tot += wsum[w];
+  }
+  __syncthreads();
+  *total = tot;
+  return woff + x - v;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_site_count(InstState* st, const int* act, long long nsite, int nblk,
+                                                    int* bcount) {
+  const int inst = kinst(act);
+  const InstState& S = st[inst];
+  if (!S.active || !S.cidx) return;
+  bool f[kSitePer];
+  const int n = site_flags<R>(S, (long long)blockIdx.x * kSiteBlock + (long long)threadIdx.x * kSitePer, nsite, f);
+  int total;
+  block_excl_scan(n, &total);
+  if (threadIdx.x == 0) bcount[(size_t)inst * nblk + blockIdx.x] = total;
+}
+
+// one CTA per instance: block counts -> exclusive block offsets, nv = 3 M
+__global__ void __launch_bounds__(KNT) k_site_scan(InstState* st, const int* act, int nblk, int* bcount) {
+  const int inst = kinst(act);
+  InstState& S = st[inst];
+  if (!S.active || !S.cidx) return;
+  int* bc = bcount + (size_t)inst * nblk;
+  int carry = 0;
+  for (int b0 = 0; b0 < nblk; b0 += KNT) {
+    const int b = b0 + threadIdx.x;
+    const int v = b < nblk ? bc[b] : 0;
+    int total;
+    const int ex = block_excl_scan(v, &total);
+    if (b < nblk) bc[b] = carry + ex;
+    carry += total;
+  }
+  if (threadIdx.x == 0) S.nv = 3LL * carry;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(KNT) k_site_index(InstState* st, const int* act, long long nsite, int nblk,
+                                                    const int* bcount) {
+  const int inst = kinst(act);
+  const InstState& S = st[inst];
+  if (!S.active || !S.cidx) return;
+  const long long base = (long long)blockIdx.x * kSiteBlock + (long long)threadIdx.x * kSitePer;
+  bool f[kSitePer];
+  const int n = site_flags<R>(S, base, nsite, f);
+  int total;
+  int r = bcount[(size_t)inst * nblk + blockIdx.x] + block_excl_scan(n, &total);
+  int* cid = const_cast<int*>(S.cidx);
+#pragma unroll
+  for (int j = 0; j < kSitePer; ++j) {
+    if (base + j < nsite) cid[base + j] = f[j] ? r : -1;
+    r += f[j];
+  }
 }
 
 // out[inst] = ||vec[id]||^2 (FP64, deterministic)
@@ -138,6 +291,27 @@ void launch_accum(InstState* st128, int xid, const InstState* st64, int nb, long
   k_accum<<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(st128, xid, st64, act, n3);
   note_launch(s, 1);
 }
+
+int site_blocks(long long nsite) { return (int)((nsite + kSiteBlock - 1) / kSiteBlock); }
+
+template <typename R>
+void launch_site_map(InstState* st, int nb, long long nsite, int* bcount, cudaStream_t s, const int* act) {
+  const int nblk = site_blocks(nsite);
+  k_site_count<R><<<dim3(nblk, nb), KNT, 0, s>>>(st, act, nsite, nblk, bcount);
+  k_site_scan<<<dim3(1, nb), KNT, 0, s>>>(st, act, nblk, bcount);
+  k_site_index<R><<<dim3(nblk, nb), KNT, 0, s>>>(st, act, nsite, nblk, bcount);
+  note_launch(s, 3);
+}
+template void launch_site_map<float>(InstState*, int, long long, int*, cudaStream_t, const int*);
+template void launch_site_map<double>(InstState*, int, long long, int*, cudaStream_t, const int*);
+
+template <typename R>
+void launch_store_solution(InstState* st, int nb, long long n3, int num_sms, cudaStream_t s, const int* act) {
+  k_store_solution<R><<<dim3(grid_for(n3, nb, num_sms), nb), KNT, 0, s>>>(st, act, n3);
+  note_launch(s, 1);
+}
+template void launch_store_solution<float>(InstState*, int, long long, int, cudaStream_t, const int*);
+template void launch_store_solution<double>(InstState*, int, long long, int, cudaStream_t, const int*);
 
 template <typename R>
 void launch_norm2(InstState* st, int id, int nb, long long n3, double* red, unsigned* cnt, int RB, double* out,
