@@ -249,6 +249,16 @@ int dda_incident_field(dda_ctx* ctx, int dtype, int nx, int ny, int nz, double d
 int dda_cross_sections(dda_ctx* ctx, int dtype, long long nsite, const void* p, const void* e_inc,
                        const void* inv_alpha, double k, double e0, double* out3, void* stream);
 
+/* Far-field scattering amplitude (not in the reference; Draine 1988):
+ *   F(n) = k^2 sum_j [P_j - n (n . P_j)] exp(-i k n . r_j),  r_j = (i,j,k) d
+ * for ndir (1..65535) directions dirs3 (host, 3 doubles each, normalised here); out6
+ * (host, 6 doubles per direction) = (Re F_x, Im F_x, Re F_y, Im F_y, Re F_z,
+ * Im F_z).  dC_sca/dOmega = |F|^2 / |E0|^2; F at the incidence direction
+ * gives C_ext = 4 pi / k Im(E0* . F) / |E0|^2.  Sums in FP64, phases
+ * from FP64 sincos; blocks until the result is on the host. */
+int dda_far_field(dda_ctx* ctx, int dtype, int nx, int ny, int nz, double d, double k, const void* p, int ndir,
+                  const double* dirs3, double* out6, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

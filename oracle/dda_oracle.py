@@ -454,6 +454,23 @@ def cross_sections(P, E_inc, inv_alpha, k, E0=1.0):
 # --------------------------------------------------------------------------
 # Mie theory (Bohren & Huffman 1983, appendix A: BHMIE recurrences)
 # --------------------------------------------------------------------------
+def far_field(P, d, k, directions):
+    """Far-field amplitude F(n) = k^2 sum_j [P_j - n (n.P_j)] exp(-i k n.r_j),
+    r_j = (i, j, k) d (the incident field's origin, ddaforgit.py:1626-1632);
+    the standard DDA far field (Draine 1988), not present in the reference."""
+    P = np.asarray(P)
+    nx, ny, nz, _ = P.shape
+    idx = np.stack(np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij"), -1).reshape(-1, 3) * d
+    Pf = P.reshape(-1, 3)
+    out = []
+    for n in np.asarray(directions, float).reshape(-1, 3):
+        n = n / np.linalg.norm(n)
+        ph = np.exp(-1j * k * (idx @ n))
+        S = (Pf * ph[:, None]).sum(0)
+        out.append(k * k * (S - n * (n @ S)))
+    return np.array(out)
+
+
 def mie_qext_qsca(m, x):
     """Extinction and scattering efficiencies of a homogeneous sphere with
     relative index ``m`` and size parameter ``x`` (Bohren & Huffman BHMIE:

@@ -370,6 +370,36 @@ def solve_many(ops, E_incs, tol=1e-5, max_iter=2000, ratio=100.0, precision=None
     return P128, [_info(res[j]) for j in range(nb)]
 
 
+def far_field(P, d, k, directions):
+    """Far-field scattering amplitude F(n) (ndir, 3) complex128 of the
+    polarisation P (nx,ny,nz,3) for unit directions n:
+    F = k^2 sum_j [P_j - n (n.P_j)] exp(-i k n.r_j), r_j = (i,j,k) d.
+    dC_sca/dOmega = |F|^2 / |E0|^2."""
+    if not isinstance(P, torch.Tensor):
+        P = as_device(P, _C128, _device())
+    dev = _device(P.device)
+    dt = P.dtype if P.dtype in (_C64, _C128) else _C128
+    P = as_device(P, dt, dev)
+    if P.dim() != 4 or P.shape[3] != 3:
+        raise ValueError("P must have shape (nx, ny, nz, 3)")
+    dirs = np.ascontiguousarray(np.asarray(directions, dtype=np.float64).reshape(-1, 3))
+    nd = dirs.shape[0]
+    out = np.empty(nd * 6, dtype=np.float64)
+    ctx = L.context(dev.index)
+    with torch.cuda.device(dev):
+        L.check(L.lib().dda_far_field(ctx.handle, _dt_code(dt), *P.shape[:3], float(d), float(k), P.data_ptr(), nd,
+                                      dirs.ctypes.data_as(C.POINTER(C.c_double)),
+                                      out.ctypes.data_as(C.POINTER(C.c_double)), stream_handle(dev)))
+    o = out.reshape(nd, 3, 2)
+    return o[..., 0] + 1j * o[..., 1]
+
+
+def differential_cross_section(P, d, k, directions, E0=1.0):
+    """dC_sca/dOmega = |F(n)|^2 / |E0|^2 for each direction."""
+    F = far_field(P, d, k, directions)
+    return (np.abs(F) ** 2).sum(axis=1) / abs(E0) ** 2
+
+
 def cross_sections(P, E_inc, inv_alpha, k, E0=1.0):
     """(C_ext, C_abs, C_sca) reduced in FP64 on the device (Draine & Flatau
     1994); arrays are brought to the precision of P."""

@@ -160,3 +160,24 @@ def test_workload_generators_are_seeded_and_valid():
     assert all(16 <= b <= 96 for b in e["box"]) and len(e["dirs"]) == 8
     k1, k2 = W.transverse_pair(np.array([0.3, -0.5, 0.81]) / np.linalg.norm([0.3, -0.5, 0.81]))
     assert abs(k1 @ k2) < 1e-12
+
+
+def test_results_file_layout(tmp_path):
+    from precondda_b200.results import save_results_to_file
+    P = (np.arange(2 * 3 * 4 * 3) + 1j).reshape(2, 3, 4, 3).astype(np.complex64)
+    problem = {"grid_size": (2, 3, 4), "lattice_spacing": 0.02, "wavelength": 0.5, "k_direction": [0, 0, 1],
+               "E_polarization": [1, 0, 0], "k": 12.566370614359172}
+    shapes = [{"type": "sphere", "center": [0.1, 0.1, 0.1], "n": 1.5, "radius": 0.08},
+              {"type": "prism", "center": [0, 0, 0], "n": 2.0, "radius": 0.05, "height": 0.1, "sides": 6,
+               "axis": "z"}]
+    fn = str(tmp_path / "run.txt")
+    files = save_results_to_file(fn, problem, [np.nan, np.nan], shapes, (17, P, 3.2e-7), (1.0, 0.25, 0.75))
+    assert files == [fn, fn.replace(".txt", "_polarization.npy")]
+    txt = open(fn).read().splitlines()
+    assert txt[0] == "DDA Problem Analysis Results" and txt[1] == "=" * 50
+    assert "Grid size: (2, 3, 4)" in txt and "Lattice spacing: 0.020000" in txt
+    assert "Shape 1: sphere" in txt and "  Radius: 0.08" in txt and "  Sides: 6" in txt
+    assert "AI PREDICTION: Failed" in txt
+    assert "Iterations: 17" in txt and "Final norm: 3.200000e-07" in txt and "Status: Converged" in txt
+    assert "Polarization array shape: (2, 3, 4, 3)" in txt and "C_sca: 7.500000000e-01" in txt
+    assert np.array_equal(np.load(files[1]), P)

@@ -239,3 +239,45 @@ def test_fused_krylov_steps_match_oracle(n, monkeypatch):
     assert _rel(Pg.cpu().numpy(), P_ref) < 1e-8
     Pm, im = op.solve(E, tol=1e-6, max_iter=500, ratio=100, precision="mixed")
     assert im.status == "converged" and im.true_relres <= 1e-6
+
+
+@pytest.mark.parametrize("dtype,tol", [(C128, 1e-11), (C64, 2e-5)])
+def test_far_field_matches_oracle(dtype, tol):
+    P = _pkg()
+    rng = np.random.default_rng(11)
+    shape = (5, 7, 6)
+    Pv = rng.standard_normal(shape + (3,)) + 1j * rng.standard_normal(shape + (3,))
+    dirs = rng.standard_normal((17, 3))
+    k, d = 9.0, 0.07
+    ref = O.far_field(Pv, d, k, dirs)
+    got = P.far_field(torch.tensor(Pv, device="cuda").to(dtype), d, k, dirs)
+    assert np.abs(got - ref).max() / np.abs(ref).max() < tol
+
+
+def test_far_field_optical_theorem_and_energy():
+    """F at the incidence direction gives C_ext (optical theorem), and the
+    integral of |F|^2 over the sphere equals C_ext - C_abs (energy balance of
+    the dipole system with the radiative-reaction polarizability)."""
+    P = _pkg()
+    n, m = 10, 1.5 + 0.02j
+    k, d, alpha, E = _sphere_problem(n, m)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    Pg, info = op.solve(E, tol=1e-11, max_iter=800, ratio=100)
+    ce, ca, cs = op.cross_sections(Pg, E)
+    E0 = np.array([1.0, 0.0, 0.0])
+    Ff = P.far_field(Pg, d, k, [[0.0, 0.0, 1.0]])[0]
+    c_ext_ot = 4 * np.pi / k * np.imag(np.conj(E0) @ Ff)
+    assert abs(c_ext_ot - ce) / abs(ce) < 1e-10
+    # Gauss-Legendre in cos(theta) x uniform phi
+    xg, wg = np.polynomial.legendre.leggauss(24)
+    nphi = 48
+    phi = 2 * np.pi * np.arange(nphi) / nphi
+    ct = np.repeat(xg, nphi)
+    st = np.sqrt(1 - ct ** 2)
+    ph = np.tile(phi, len(xg))
+    dirs = np.stack([st * np.cos(ph), st * np.sin(ph), ct], -1)
+    w = np.repeat(wg, nphi) * (2 * np.pi / nphi)
+    dcs = P.differential_cross_section(Pg, d, k, dirs)
+    c_sca_int = float((dcs * w).sum())
+    assert abs(c_sca_int - cs) / cs < 1e-6
