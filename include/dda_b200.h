@@ -122,6 +122,14 @@ void dda_op_destroy(dda_op* op);
  * DDA_MV_RESIDUAL.  x and y must not alias. */
 int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void* stream);
 
+/* dda_matvec for nb operators / vectors in one launch sequence (every kernel
+ * has gridDim.y = nb): operators sharing context, dtype, box, FFT lengths and
+ * tensor scale (they may have different ghat / inv_alpha).  Arrays of nb
+ * device pointers on the host; b may be NULL unless mode is DDA_MV_RESIDUAL.
+ * Uses transform scratch cached in the context per (shape, nb). */
+int dda_matvec_batch(dda_op* const* ops, int nb, int mode, const void* const* x, void* const* y,
+                     const void* const* b, void* stream);
+
 /* Allocation-free A.x.  No counterpart in the reference: it exists for
  * callers that cannot allocate device memory where they need the product --
  * code recording into a CUDA graph (cudaMalloc cannot be captured), serving

@@ -43,7 +43,7 @@ EXPORTS = (
     "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
     "dda_voxelize", "dda_incident_field", "dda_slots_create", "dda_slots_destroy", "dda_slots_capacity",
     "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
-    "dda_far_field",
+    "dda_far_field", "dda_matvec_batch",
 )
 
 
@@ -112,6 +112,7 @@ def _declare(lib):
     lib.dda_slots_poll.argtypes = [vp, C.POINTER(i), C.POINTER(dda_result), C.POINTER(i), C.POINTER(i)]
     lib.dda_slots_release.argtypes = [vp, i]
     lib.dda_far_field.argtypes = [vp, i, i, i, i, d, d, vp, i, C.POINTER(d), C.POINTER(d), vp]
+    lib.dda_matvec_batch.argtypes = [C.POINTER(vp), i, i, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
     return lib
 
 

@@ -1,6 +1,7 @@
 // extern "C" entry points of include/dda_b200.h.
 #include <cmath>
 #include <cstring>
+#include <vector>
 #include <new>
 
 #include "../../include/dda_b200.h"
@@ -226,6 +227,54 @@ int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void
   else
     e = launch_matvec<float>(op->ctx->c, op->g, op->pc, op->d_st, nullptr, 1, V_R, V_RHAT, mode, C_ALWAYS,
                              op->gscale, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  return DDA_OK;
+}
+
+int dda_matvec_batch(dda_op* const* ops, int nb, int mode, const void* const* x, void* const* y,
+                     const void* const* b, void* stream) {
+  if (!ops || nb < 1 || !x || !y) { set_error("bad batch arguments"); return DDA_ERR_ARG; }
+  if (mode < 0 || mode > 3 || (mode == DDA_MV_RESIDUAL && !b)) { set_error("bad matvec mode"); return DDA_ERR_ARG; }
+  const dda_op* o0 = ops[0];
+  if (!o0) { set_error("null operator"); return DDA_ERR_ARG; }
+  int rc = check_ctx(o0->ctx);
+  if (rc) return rc;
+  for (int j = 0; j < nb; ++j) {
+    const dda_op* o = ops[j];
+    if (!o || o->ctx != o0->ctx || o->dtype != o0->dtype || o->gscale != o0->gscale || o->g.nx != o0->g.nx ||
+        o->g.ny != o0->g.ny || o->g.nz != o0->g.nz || o->g.Lx != o0->g.Lx || o->g.Ly != o0->g.Ly ||
+        o->g.Lz != o0->g.Lz) {
+      set_error("batched operators must share context, dtype, box, FFT lengths and tensor scale");
+      return DDA_ERR_ARG;
+    }
+    if (!x[j] || !y[j] || x[j] == y[j] || (mode == DDA_MV_RESIDUAL && !b[j])) {
+      set_error("null or aliased vector");
+      return DDA_ERR_ARG;
+    }
+  }
+  Ctx& c = o0->ctx->c;
+  cudaSetDevice(c.device);
+  int err = DDA_OK;
+  BatchWs* w = c.workspace(o0->dtype, o0->g, nb, false, &err, 1);
+  if (!w) return err;
+  std::vector<InstState> H(nb);
+  for (int j = 0; j < nb; ++j) {
+    w->base_state(j, H[j]);
+    H[j].vec[V_R] = (void*)x[j];
+    H[j].vec[V_RHAT] = y[j];
+    H[j].vec[V_B] = b ? (void*)b[j] : nullptr;
+    H[j].ghat = ops[j]->ghat;
+    H[j].inva = ops[j]->inva;
+    H[j].active = 1;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  // pageable source: the copy is staged before the call returns
+  cudaError_t e = cudaMemcpyAsync(w->d_st, H.data(), nb * sizeof(InstState), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
+  if (o0->dtype == DDA_C128)
+    e = launch_matvec<double>(c, o0->g, w->pc, w->d_st, nullptr, nb, V_R, V_RHAT, mode, C_ALWAYS, o0->gscale, s);
+  else
+    e = launch_matvec<float>(c, o0->g, w->pc, w->d_st, nullptr, nb, V_R, V_RHAT, mode, C_ALWAYS, o0->gscale, s);
   if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
   return DDA_OK;
 }

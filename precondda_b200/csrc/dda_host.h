@@ -59,7 +59,8 @@ struct Ctx {
   // returns device twiddles for length L (builds on first use)
   const void* twiddles(int L, bool dbl);
   // cached solver workspace for (dtype, geometry, batch size)
-  BatchWs* workspace(int dtype, const Geo& g, int nb, bool full, int* err);
+  // (tag separates workspaces of different users of the same shape)
+  BatchWs* workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag = 0);
   void trim();
   ~Ctx();
 };

@@ -118,9 +118,10 @@ void BatchWs::base_state(int j, InstState& S, bool sites) const {
   S.best_x = -1;
 }
 
-BatchWs* Ctx::workspace(int dtype, const Geo& g, int nb, bool full, int* err) {
+BatchWs* Ctx::workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag) {
   char key[160];
-  snprintf(key, sizeof(key), "%d:%d,%d,%d:%d,%d,%d:%d:%d", dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, nb, full ? 1 : 0);
+  snprintf(key, sizeof(key), "%d:%d,%d,%d:%d,%d,%d:%d:%d:%d", dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, nb,
+           full ? 1 : 0, tag);
   std::lock_guard<std::mutex> lk(mu);
   auto it = ws.find(key);
   if (it != ws.end()) return it->second;

@@ -304,6 +304,28 @@ class DDAOperator:
         return cross_sections(P, E_inc, self.inv_alpha, self.k, E0)
 
 
+def matvec_batch(ops, xs, mode=L.MV_AX, bs=None):
+    """[A_j x_j] for operators sharing box, FFT lengths, dtype and scale, in
+    one batched launch sequence (mode: L.MV_AX, MV_RESIDUAL with bs,
+    MV_CONV, MV_CONV_MASKED)."""
+    ops = list(ops)
+    if len(ops) != len(xs):
+        raise ValueError("one vector per operator")
+    _same_bucket(ops)
+    o0 = ops[0]
+    X = [o._vec(x) for o, x in zip(ops, xs)]
+    Y = [torch.empty_like(x) for x in X]
+    B = [o._vec(b) for o, b in zip(ops, bs)] if bs is not None else None
+    nb = len(ops)
+    arr = lambda v: (C.c_void_p * nb)(*v)
+    with torch.cuda.device(o0.device):
+        L.check(L.lib().dda_matvec_batch(arr([o._op.value for o in ops]), nb, int(mode),
+                                         arr([x.data_ptr() for x in X]), arr([y.data_ptr() for y in Y]),
+                                         arr([b.data_ptr() for b in B]) if B is not None else None,
+                                         stream_handle(o0.device)))
+    return Y
+
+
 def _same_bucket(ops):
     o0 = ops[0]
     for o in ops[1:]:

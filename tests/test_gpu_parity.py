@@ -281,3 +281,22 @@ def test_far_field_optical_theorem_and_energy():
     dcs = P.differential_cross_section(Pg, d, k, dirs)
     c_sca_int = float((dcs * w).sum())
     assert abs(c_sca_int - cs) / cs < 1e-6
+
+
+def test_matvec_batch_equals_single_launches():
+    P = _pkg()
+    from precondda_b200 import _lib as L
+    shape = (12, 12, 12)
+    ops, xs = [], []
+    for seed in (1, 2, 3):
+        k, d, alpha, x = _rand_problem(shape, seed=seed)
+        ia, _, _, _ = O.prepare_interaction_matrices(alpha, k / (1 + 0 * seed), d)
+        ops.append(P.DDAOperator(ia, k, d, dtype=C64, L_=(24, 24, 24)))
+        xs.append(x)
+    ys = P.engine.matvec_batch(ops, xs)
+    for op, x, y in zip(ops, xs, ys):
+        assert torch.equal(y, op.matvec(x))
+    bs = [x[::-1].copy() for x in xs]
+    rs = P.engine.matvec_batch(ops, xs, L.MV_RESIDUAL, bs)
+    for op, x, b, r in zip(ops, xs, bs, rs):
+        assert torch.equal(r, op._mv(L.MV_RESIDUAL, x, b))
