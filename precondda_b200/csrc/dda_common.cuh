@@ -43,6 +43,19 @@ __device__ __forceinline__ float2 csub(float2 a, float2 b) { return __ffma2_rn(b
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 #endif
 
+// Programmatic dependent launch: a kernel launched with the
+// programmatic-stream-serialization attribute may start while its
+// predecessor drains; grid_dep_begin() waits until the predecessor has
+// completed and its memory is visible, then lets this kernel's own successor
+// start launching (every CTA of this grid is resident by then).  Without the
+// attribute both instructions return at once.
+__device__ __forceinline__ void grid_dep_begin() {
+#if defined(__CUDA_ARCH__) && (__CUDA_ARCH__ >= 900)
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
 // complex double helpers used by the scalar control logic
 __device__ __forceinline__ double2 zmul(double2 a, double2 b) { return cmul(a, b); }
 __device__ __forceinline__ double2 zdiv(double2 a, double2 b) {

@@ -5,6 +5,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "dda_common.cuh"
@@ -13,6 +14,24 @@
 namespace dda {
 
 void set_error(const std::string& msg);
+
+// Launch with programmatic stream serialization (the kernel must begin with
+// grid_dep_begin()); DDA_NO_PDL=1 launches plainly.
+bool pdl_enabled();
+template <typename... KArgs, typename... Args>
+cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
 // Counts kernels this library enqueues (launches made while a stream is being
 // captured into a graph are counted when the graph is launched instead).
 void note_launch(cudaStream_t s, long long n);

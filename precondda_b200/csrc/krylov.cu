@@ -74,6 +74,7 @@ __device__ void ctrl_check(InstState& S, double norm2, double2 rho_new) {
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_init(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -113,6 +114,7 @@ __global__ void __launch_bounds__(KNT) k_init(InstState* st, const int* act, dou
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_alpha(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                                int RB) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -132,6 +134,7 @@ __global__ void __launch_bounds__(KNT) k_alpha(InstState* st, const int* act, do
 // s = r - alpha v ; y = s_prev - s - alpha w   (Gpbicgstab.py:1020-1021)
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_sy(InstState* st, const int* act, long long n3) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -154,6 +157,7 @@ __global__ void __launch_bounds__(KNT) k_sy(InstState* st, const int* act, long 
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -188,6 +192,7 @@ __global__ void __launch_bounds__(KNT) k_zeta(InstState* st, const int* act, dou
 template <typename R, bool SETC>
 __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB, unsigned long long cond_true, unsigned long long cond_reset) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -245,6 +250,7 @@ __global__ void __launch_bounds__(KNT) k_uzrx(InstState* st, const int* act, dou
 template <typename R, bool SETC>
 __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, double* red, unsigned* cnt, long long n3,
                                               int RB, unsigned long long cond_reset) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -271,6 +277,7 @@ __global__ void __launch_bounds__(KNT) k_norm(InstState* st, const int* act, dou
 // (Gpbicgstab.py:1139-1158)
 template <typename R>
 __global__ void __launch_bounds__(KNT) k_fin(InstState* st, const int* act, unsigned* cnt, long long n3, int RB) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   const int inst = kinst(act);
   InstState& S = st[inst];
@@ -314,37 +321,38 @@ __global__ void __launch_bounds__(KNT) k_fin(InstState* st, const int* act, unsi
 
 
 template <typename R> void launch_init(const KrylovLaunch& k, cudaStream_t s) {
-  k_init<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB);
+  launch_pdl(k_init<R>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB);
   note_launch(s, 1);
 }
 template <typename R> void launch_alpha(const KrylovLaunch& k, cudaStream_t s) {
-  k_alpha<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB);
+  launch_pdl(k_alpha<R>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB);
   note_launch(s, 1);
 }
 template <typename R> void launch_sy(const KrylovLaunch& k, cudaStream_t s) {
-  k_sy<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.n3);
+  launch_pdl(k_sy<R>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.n3);
   note_launch(s, 1);
 }
 template <typename R> void launch_zeta(const KrylovLaunch& k, cudaStream_t s) {
-  k_zeta<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB);
+  launch_pdl(k_zeta<R>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB);
   note_launch(s, 1);
 }
 template <typename R> void launch_uzrx(const KrylovLaunch& k, cudaStream_t s) {
   if (k.cond_true && k.cond_reset)
-    k_uzrx<R, true><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_true, k.cond_reset);
+    launch_pdl(k_uzrx<R, true>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_true,
+               k.cond_reset);
   else
-    k_uzrx<R, false><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0, 0);
+    launch_pdl(k_uzrx<R, false>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0ull, 0ull);
   note_launch(s, 1);
 }
 template <typename R> void launch_norm(const KrylovLaunch& k, cudaStream_t s) {
   if (k.cond_reset)
-    k_norm<R, true><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_reset);
+    launch_pdl(k_norm<R, true>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB, k.cond_reset);
   else
-    k_norm<R, false><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0);
+    launch_pdl(k_norm<R, false>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.red, k.cnt, k.n3, k.RB, 0ull);
   note_launch(s, 1);
 }
 template <typename R> void launch_fin(const KrylovLaunch& k, cudaStream_t s) {
-  k_fin<R><<<dim3(k.RB, k.nb), KNT, 0, s>>>(k.st, k.act, k.cnt, k.n3, k.RB);
+  launch_pdl(k_fin<R>, dim3(k.RB, k.nb), dim3(KNT), 0, s, k.st, k.act, k.cnt, k.n3, k.RB);
   note_launch(s, 1);
 }
 

@@ -1,11 +1,20 @@
 // Tile shapes of the five matvec passes (see matvec_impl.cuh).
 #include "matvec_impl.cuh"
 
+#include <cstdlib>
 #include <mutex>
 #include <set>
 #include <utility>
 
 namespace dda {
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("DDA_NO_PDL");
+    return !(e && *e == '1');
+  }();
+  return on;
+}
 
 cudaError_t mv_prepare(const void* const* ks, int n) {
   static std::mutex mu;

@@ -73,6 +73,7 @@ template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int cond,
                                                             int nl_, int pre) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
@@ -145,6 +146,7 @@ template <typename R, bool INV, int LY, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
                                                              int ntz_) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef MvShape<R, LY> SH;
   typedef typename SH::P P;
@@ -227,6 +229,7 @@ template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
                                                              int ntz_, R gscale) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
   typedef typename SH::P P;
@@ -321,6 +324,7 @@ template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
                                                              int ntz_, R gscale) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
   typedef typename SH::P P;
@@ -435,6 +439,7 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
                                                             InstState* st, const int* act, int in_id, int out_id,
                                                             int mode, int cond, int nl_, int post, double* red,
                                                             unsigned* cnt) {
+  grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef MvShape<R, LZ> SH;
   typedef typename SH::P P;
@@ -618,12 +623,21 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                        (const void*)k.k5};
   cudaError_t e = mv_prepare(ks, 5);
   if (e != cudaSuccess) return e;
-  k.k1<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, cond, pc.nl, fz.pre);
-  k.k2<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
-  k.k3<<<dim3((unsigned)pc.grid3, nb), pc.th3, pc.smem3, s>>>(g, twx, st, act, cond, pc.tz3, pc.ntz3, (R)gscale);
-  k.k4<<<dim3((unsigned)pc.grid2, nb), pc.th2, pc.smem2, s>>>(g, twy, st, act, cond, pc.tz2, pc.ntz2);
-  k.k5<<<dim3((unsigned)pc.grid1, nb), pc.th1, pc.smem1, s>>>(g, twz, st, act, in_id, out_id, mode, cond, pc.nl,
-                                                              fz.post, fz.red, fz.cnt);
+  if ((e = launch_pdl(k.k1, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, cond,
+                      pc.nl, fz.pre)))
+    return e;
+  if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
+                      pc.ntz2)))
+    return e;
+  if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond, pc.tz3,
+                      pc.ntz3, (R)gscale)))
+    return e;
+  if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
+                      pc.ntz2)))
+    return e;
+  if ((e = launch_pdl(k.k5, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, out_id,
+                      mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
+    return e;
   note_launch(s, 5);
   return cudaGetLastError();
 }
