@@ -16,6 +16,16 @@ bool pdl_enabled() {
   return on;
 }
 
+bool fused_zy_enabled(bool inverse) {
+  const char* e = getenv("DDA_NO_FUSED_ZY");
+  if (e && *e == '1') return false;
+  if (inverse) {
+    e = getenv("DDA_NO_FUSED_INV");
+    if (e && *e == '1') return false;
+  }
+  return true;
+}
+
 cudaError_t mv_prepare(const void* const* ks, int n) {
   static std::mutex mu;
   static std::set<std::pair<int, const void*>> done;
@@ -24,7 +34,7 @@ cudaError_t mv_prepare(const void* const* ks, int n) {
   if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(mu);
   for (int i = 0; i < n; ++i) {
-    if (done.count({dev, ks[i]})) continue;
+    if (!ks[i] || done.count({dev, ks[i]})) continue;
     if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024))) return e;
     if ((e = cudaFuncSetAttribute(ks[i], cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
     done.insert({dev, ks[i]});

@@ -22,10 +22,13 @@
 #include "fftreg.cuh"
 #include "krylov_ctrl.cuh"
 #include "fft_sizes.h"
+#include <cooperative_groups.h>
 #include <cstdlib>
 #include <type_traits>
 
 namespace dda {
+
+namespace cg = cooperative_groups;
 
 constexpr int kMvMaxThreads = 384;
 
@@ -532,6 +535,193 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typenam
 }
 
 // ---------------------------------------------------------------------------
+// Passes 1+2 and 4+5 fused over a thread-block cluster (cubic boxes; the
+// z/y transforms keep T1 on chip).  The CL CTAs of a cluster share one x
+// slab ix:
+//   forward  CTA r runs the z transforms of rows y in [r YR, (r+1) YR) and
+//            writes each output kz into the shared memory of the CTA owning
+//            kz's block (kz / KB) through distributed shared memory; after the
+//            cluster barrier every CTA runs the y transforms of its KB kz
+//            columns straight from that buffer into T2.
+//   inverse  CTA r runs the y inverse transforms of its kz block from T2 and
+//            writes each kept row y into the buffer of row owner y / YR;
+//            after the barrier every CTA runs the z inverse transforms of its
+//            YR rows with the pass-5 combine.
+// T1 is neither written nor read and one launch replaces two.  Every value
+// goes through the same arithmetic as in the separate passes, so the results
+// are equal bit for bit.  All CTAs of a cluster share blockIdx.y (the
+// instance), so the condition test exits whole clusters or none.
+// ---------------------------------------------------------------------------
+template <typename R, int L>
+struct FusedZY {
+  typedef MvShape<R, L> SH;
+  typedef typename SH::P P;
+  static constexpr int CL = 4;                  // CTAs per cluster (one x slab)
+  static constexpr int NC = L / 2;              // box edge
+  static constexpr int YR = NC / CL;            // z lines (rows y) per CTA
+  static constexpr int KB = L / CL;             // kz columns per CTA
+  static constexpr int TH = 3 * SH::T * YR;     // z phase: thread = (c, t, row)
+  static constexpr int TZ = YR;                 // y phase: kz columns per round, thread = (3 kz + c, t)
+  static constexpr int ROUNDS = KB / TZ;
+  static constexpr int BWF = 3 * KB;            // forward buffer: NC rows of KB kz x 3
+  static constexpr int BWI = 3 * L + 1;         // inverse buffer: YR rows of L kz x 3 (+1 bank pad)
+  static constexpr int XS = 3 * YR * SH::LP;    // exchange scratch of either phase
+  typedef typename CT<R>::T C;
+  static constexpr size_t smem_fwd = (size_t)(NC * BWF + XS) * sizeof(C);
+  static constexpr size_t smem_inv = (size_t)(YR * BWI + XS) * sizeof(C);
+  static_assert(NC % CL == 0 && KB % TZ == 0 && TH <= kMvMaxThreads, "cluster tiling");
+  static_assert(P::r[0] % 2 == 0 && half_store_ok<P>(), "zero-half loads and half stores");
+  // two CTAs per SM: shared memory for both, registers capped by the launch bounds
+  static_assert(smem_fwd <= 110 * 1024 && smem_inv <= 110 * 1024, "two CTAs per SM");
+};
+
+template <typename R, int L>
+__global__ void __launch_bounds__(FusedZY<R, L>::TH, 2) k_mv_fwd_zy(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                                 InstState* st, const int* act, int in_id,
+                                                                 int cond) {
+  grid_dep_begin();
+  typedef typename CT<R>::T C;
+  typedef FusedZY<R, L> F;
+  typedef typename F::P P;
+  constexpr int NC = F::NC, LP = F::SH::LP, T = F::SH::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);     // [NC][BWF], filled by the whole cluster
+  C* xs = buf + NC * F::BWF;                    // exchange scratch
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int ix = (int)blockIdx.x / F::CL;
+  cluster.sync();                               // every peer runs before its buffer is written
+  {
+    const C* __restrict__ x = (const C*)S.vec[in_id];
+    const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
+    const int t = rest % T, l = rest / T;
+    const int y = r * F::YR + l;
+    const long long line = (long long)ix * NC + y;
+    const long long base = line * NC * 3 + c;
+    const int* __restrict__ cid = S.cidx ? S.cidx + line * NC : nullptr;
+    auto ld = [&](int, int pos) -> C {
+      long long i = base + (long long)pos * 3;
+      if (cid) {
+        const int k = cid[pos];
+        if (k < 0) return czero<C>();
+        i = 3LL * k + c;
+      }
+      return __ldcg(x + i);
+    };
+    C* sl = xs + l * 3 * LP + c;
+    auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
+    C* brow = buf + y * F::BWF + c;
+    auto stf = [&](int, int kz, C v) { *cluster.map_shared_rank(brow + 3 * (kz % F::KB), kz / F::KB) = v; };
+    C a[P::E];
+    rfft<P, 1, false, true, false>(a, t, ld, sm, stf, tw);
+  }
+  cluster.sync();                               // all NC rows of this CTA's kz block are in
+  {
+    C* __restrict__ t2 = (C*)S.t2;
+    constexpr int W = 3 * F::TZ;
+    constexpr long long rs = (long long)L * 3;
+    const int w = threadIdx.x % W, t = threadIdx.x / W;
+    C* sw = xs + w;
+    auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
+#pragma unroll 1
+    for (int q = 0; q < F::ROUNDS; ++q) {
+      const C* src = buf + q * W + w;
+      C* dst = t2 + (long long)ix * L * rs + (r * F::KB + q * F::TZ) * 3 + w;
+      auto ld = [&](int, int pos) -> C { return src[pos * F::BWF]; };
+      auto stf = [&](int, int pos, C v) { __stcg(dst + pos * rs, v); };
+      C a[P::E];
+      rfft<P, 1, false, true, false>(a, t, ld, sm, stf, tw);
+    }
+  }
+}
+
+template <typename R, int L>
+__global__ void __launch_bounds__(FusedZY<R, L>::TH, 2) k_mv_inv_yz(Geo g, const typename CT<R>::T* __restrict__ tw,
+                                                                 InstState* st, const int* act, int in_id,
+                                                                 int out_id, int mode, int cond) {
+  grid_dep_begin();
+  typedef typename CT<R>::T C;
+  typedef FusedZY<R, L> F;
+  typedef typename F::P P;
+  constexpr int NC = F::NC, LP = F::SH::LP, T = F::SH::T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);     // [YR][BWI], filled by the whole cluster
+  C* xs = buf + F::YR * F::BWI;                 // exchange scratch
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int ix = (int)blockIdx.x / F::CL;
+  cluster.sync();
+  {
+    const C* __restrict__ t2 = (const C*)S.t2;
+    constexpr int W = 3 * F::TZ;
+    constexpr long long rs = (long long)L * 3;
+    const int w = threadIdx.x % W, t = threadIdx.x / W;
+    C* sw = xs + w;
+    auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
+#pragma unroll 1
+    for (int q = 0; q < F::ROUNDS; ++q) {
+      const int col = (r * F::KB + q * F::TZ) * 3 + w;
+      const C* src = t2 + (long long)ix * L * rs + col;
+      C* bcol = buf + col;
+      auto ld = [&](int, int pos) -> C { return __ldcg(src + pos * rs); };
+      auto stf = [&](int, int y, C v) { *cluster.map_shared_rank(bcol + (y % F::YR) * F::BWI, y / F::YR) = v; };
+      C a[P::E];
+      rfft<P, 1, true, false, true>(a, t, ld, sm, stf, tw);
+    }
+  }
+  cluster.sync();                               // all L kz of this CTA's rows are in
+  {
+    // fresh copies keep the y phase's address arithmetic out of this one
+    const int tid = opaque((int)threadIdx.x);
+    const int c = tid % 3, rest = tid / 3;
+    const int t = rest % T, l = rest / T;
+    const long long line = (long long)opaque(ix * NC + r * F::YR) + l;
+    buf = opaque_ptr(buf);
+    xs = opaque_ptr(xs);
+    const long long site0 = line * NC;
+    const C* __restrict__ xg = (const C*)S.vec[in_id];
+    C* __restrict__ yg = (C*)S.vec[out_id];
+    const C* __restrict__ iag = (const C*)S.inva + site0;
+    const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] : nullptr;
+    const int* __restrict__ cid = S.cidx ? S.cidx + site0 : nullptr;
+    const C* brow = buf + l * F::BWI + c;
+    auto ld = [&](int, int pos) -> C { return brow[pos * 3]; };
+    C* sl = xs + l * 3 * LP + c;
+    auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
+    // the combine of pass 5 (y = ia x - mask conv and its variants)
+    auto stf = [&](int, int pos, C v) {
+      long long e = (site0 + pos) * 3 + c;
+      if (cid) {
+        const int k = cid[pos];
+        if (k < 0) return;
+        e = 3LL * k + c;
+      }
+      C o;
+      if (mode == MV_CONV) {
+        o = v;
+      } else {
+        const C a_ = __ldg(iag + pos);
+        const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
+        if (!msk) v = czero<C>();
+        if (mode == MV_CONV_MASKED) {
+          o = v;
+        } else {
+          o = csub(cmul(a_, __ldcg(xg + e)), v);
+          if (mode == MV_RESIDUAL) o = csub(__ldcg(bg + e), o);
+        }
+      }
+      __stcg(yg + e, o);
+    };
+    C a[P::E];
+    rfft<P, 1, true, false, true>(a, t, ld, sm, stf, tw);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host dispatch over the compiled lengths
 // ---------------------------------------------------------------------------
 template <typename R> struct MvSet {
@@ -540,9 +730,16 @@ template <typename R> struct MvSet {
   typedef void (*PY)(Geo, const C*, InstState*, const int*, int, int, int);
   typedef void (*P3)(Geo, const C*, InstState*, const int*, int, int, int, R);
   typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int, int, double*, unsigned*);
+  typedef void (*PF)(Geo, const C*, InstState*, const int*, int, int);
+  typedef void (*PI)(Geo, const C*, InstState*, const int*, int, int, int, int);
   P1 k1 = nullptr; PY k2 = nullptr; P3 k3 = nullptr; PY k4 = nullptr; P5 k5 = nullptr;
   // tile sizes the kernels were compiled for (cubic set only; 0 = any)
   int nl = 0, tz2 = 0, tz3 = 0;
+  // cluster-fused passes 1+2 (kf) and 4+5 (ki), cubic sets only: cluster
+  // size, threads, CTAs per instance and dynamic shared memory
+  PF kf = nullptr; PI ki = nullptr;
+  int cl = 0, thf = 0, gridf = 0;
+  size_t smemf = 0, smemi = 0;
 };
 
 // General kernels (sizes from Geo), defined with the instantiations.
@@ -597,6 +794,17 @@ void mv_cube_fill(MvSet<R>& o) {
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
   o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
   o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+  if constexpr (sizeof(R) == 4 && L == 128) {
+    // complex64 64^3: both fused buffers fit two CTAs per SM
+    typedef FusedZY<R, L> F;
+    o.kf = k_mv_fwd_zy<R, L>;
+    o.ki = k_mv_inv_yz<R, L>;
+    o.cl = F::CL;
+    o.thf = F::TH;
+    o.gridf = NC * F::CL;
+    o.smemf = F::smem_fwd;
+    o.smemi = F::smem_inv;
+  }
 }
 
 // The kernel set for a geometry: the cubic one when the box is n^3 on a
@@ -611,34 +819,82 @@ bool mv_select(const Geo& g, const PassCfg& pc, MvSet<R>& o) {
   return mv_general_set<R>(g.Lx, g.Ly, g.Lz, pc.p3var, o);
 }
 
-// Raise the dynamic shared-memory limit of each kernel once per device.
+// Raise the dynamic shared-memory limit of each kernel once per device
+// (null entries are skipped).
 cudaError_t mv_prepare(const void* const* ks, int n);
+// Whether the cluster-fused z/y passes run (DDA_NO_FUSED_ZY=1 turns both
+// off, DDA_NO_FUSED_INV=1 the inverse one only); read at every launch.
+bool fused_zy_enabled(bool inverse);
+
+// Launch on clusters of `cl` CTAs along x, with programmatic stream
+// serialization unless DDA_NO_PDL=1.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_cluster(void (*k)(KArgs...), int cl, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                           Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[2];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[1].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl_enabled() ? 2 : 1;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+}
 
 template <typename R>
 cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                           const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
                           const MvFuse& fz = MvFuse()) {
-  const void* ks[5] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
-                       (const void*)k.k5};
-  cudaError_t e = mv_prepare(ks, 5);
+  const void* ks[7] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
+                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki};
+  cudaError_t e = mv_prepare(ks, 7);
   if (e != cudaSuccess) return e;
-  if ((e = launch_pdl(k.k1, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, cond,
-                      pc.nl, fz.pre)))
-    return e;
-  if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
-                      pc.ntz2)))
-    return e;
+  // The fused z/y kernels take the place of passes 1+2 / 4+5 in launches of
+  // one instance with no Krylov step fused into those passes (cubic sets use
+  // one twiddle table).  Measured on B200 at 64^3 complex64: one instance
+  // 0.0768 -> 0.0748 ms per matvec; two instances in one launch 0.132 ->
+  // 0.138 ms (the separate passes already fill the GPU there and the fused
+  // kernels hold two CTAs per SM), so batched launches keep the separate
+  // passes.
+  const bool one = nb == 1;
+  const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false);
+  const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true);
+  if (ff) {
+    if ((e = launch_cluster(k.kf, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemf, s, g, twz, st, act,
+                            in_id, cond)))
+      return e;
+  } else {
+    if ((e = launch_pdl(k.k1, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, cond,
+                        pc.nl, fz.pre)))
+      return e;
+    if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
+                        pc.ntz2)))
+      return e;
+  }
   if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond, pc.tz3,
                       pc.ntz3, (R)gscale)))
     return e;
-  if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
-                      pc.ntz2)))
-    return e;
-  if ((e = launch_pdl(k.k5, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, out_id,
-                      mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
-    return e;
-  note_launch(s, 5);
+  if (fi) {
+    if ((e = launch_cluster(k.ki, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemi, s, g, twz, st, act,
+                            in_id, out_id, mode, cond)))
+      return e;
+  } else {
+    if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
+                        pc.ntz2)))
+      return e;
+    if ((e = launch_pdl(k.k5, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id,
+                        out_id, mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
+      return e;
+  }
+  note_launch(s, 5 - (ff ? 1 : 0) - (fi ? 1 : 0));
   return cudaGetLastError();
 }
 

@@ -300,3 +300,45 @@ def test_matvec_batch_equals_single_launches():
     rs = P.engine.matvec_batch(ops, xs, L.MV_RESIDUAL, bs)
     for op, x, b, r in zip(ops, xs, bs, rs):
         assert torch.equal(r, op._mv(L.MV_RESIDUAL, x, b))
+
+
+def test_cluster_fused_zy_passes_equal_separate(monkeypatch):
+    """At 64^3 in complex64 the matvec runs passes 1+2 and 4+5 as
+    thread-block-cluster kernels (the z/y intermediate stays in distributed
+    shared memory).  They give the separate passes' results bit for bit --
+    dense vectors in every combine mode, occupied-site vectors inside c64 and
+    mixed solves -- and the product matches the oracle."""
+    P = _pkg()
+    from precondda_b200 import _lib as L
+    shape = (64, 64, 64)
+    k, d, alpha, x = _rand_problem(shape, seed=11)
+    ia = np.where(alpha != 0, 1.0 / np.where(alpha != 0, alpha, 1), 0)
+    op = P.DDAOperator(ia, k, d, dtype=C64)
+    assert tuple(op.L) == (128, 128, 128)
+    b = x[::-1].copy()
+    modes = [(L.MV_AX, None), (L.MV_RESIDUAL, b), (L.MV_CONV, None), (L.MV_CONV_MASKED, None)]
+    k2, d2, alpha2, E = _sphere_problem(64, 1.7 + 0.1j)
+    ia2 = np.where(alpha2 != 0, 1.0 / np.where(alpha2 != 0, alpha2, 1), 0)
+    op2 = P.DDAOperator(ia2, k2, d2, dtype=C128)
+
+    def run():
+        op._ctx.trim()                      # cached iteration graphs hold the kernels of their capture
+        mv = [op._mv(m, x, bb).clone() for m, bb in modes]
+        Pc, ic = op2.solve(E, tol=1e-4, max_iter=400, precision="c64")
+        Pm, im = op2.solve(E, tol=1e-6, max_iter=400, precision="mixed")
+        return mv, (Pc.clone(), ic), (Pm.clone(), im)
+
+    fused = run()
+    for env in ("DDA_NO_FUSED_INV", "DDA_NO_FUSED_ZY"):
+        monkeypatch.setenv(env, "1")
+        other = run()
+        for f, s in zip(fused[0], other[0]):
+            assert torch.equal(f, s)
+        for (Pf, inf), (Ps, ins) in zip(fused[1:], other[1:]):
+            assert inf.iters == ins.iters and inf.outer == ins.outer
+            assert torch.equal(Pf, Ps)
+    assert fused[2][1].status == "converged" and fused[2][1].true_relres <= 1e-6
+    mask = ia != 0
+    Gref = O.generate_interaction_row(*shape, k, d, L=op.L)
+    ref = O.interaction_mult(x, Gref, ia, mask, L=op.L)
+    assert _rel(fused[0][0].cpu().numpy(), ref) < 2e-5
