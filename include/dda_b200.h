@@ -172,6 +172,58 @@ int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, 
                           double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
                           void* stream);
 
+/* ---- preconditioned solves (precon=True) ---------------------------------- */
+/* The reference's right-preconditioned GPBiCGSTAB (Gpbicgstab.py:1002-1199,
+ * precon=True): A is applied to M p and M s, the residual replacements use
+ * A M x and the solution is M x, where
+ *   M x = mask * scale * IFFT[ P . FFT(pad x) ]  cropped to the box
+ * on the preconditioner's own grid L >= n per axis, P an octant
+ * (L/2+1)^3 x 6 read through the interaction octant's mirror rule
+ * (fft_matvec3 + optimized_dot_product_reduced_kernel, Gpbicgstab.py:633-668,
+ * :36-103; scale = 1/(Lx Ly Lz) for its normalised inverse FFT).  The
+ * reference calls preconditioner builders it does not define
+ * (ddaforgit.py:1118-1136, pre_preconditioner / circulant_approximation);
+ * dda_precond_build is this engine's replacement:
+ *   P(q) = [abar I - FFT_L(-c)(q)]^-1,  c(t) = sum_{j = t mod L} w(j) G(j),
+ * abar = mean inverse polarizability of the occupied sites, G the lattice
+ * Green tensor at offsets j in (-n, n)^3, w(j) the fraction of occupied
+ * sites whose neighbour at offset j is occupied (averaged over the 8 axis
+ * reflections): the inverse of T. Chan's optimal circulant approximation of
+ * the masked operator, folded onto the L-periodic grid (L = n is the
+ * cheapest to apply; L = 2n unfolded).  Computed in FP64 from the complex128
+ * inverse polarizability; layout DDA_GHAT_REFERENCE (hx,hy,hz,6) or
+ * DDA_GHAT_ENGINE (6,hx,hy,hz); either output may be null.  Enqueued on
+ * `stream`. */
+int dda_precond_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d,
+                      const void* inv_alpha128, int layout, void* out_c128, void* out_c64, void* stream);
+
+/* The preconditioner as an operator (engine-layout octant `phat` on the grid
+ * Lx,Ly,Lz >= the box): dda_matvec(pre, DDA_MV_CONV_MASKED, ...) is M x,
+ * the reference's fft_matvec3 (Gpbicgstab.py:633-668); inv_alpha supplies
+ * the mask.  Destroy with dda_op_destroy. */
+int dda_precond_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* phat,
+                          double scale, const void* inv_alpha, dda_op** out);
+
+/* dda_gpbicgstab with the preconditioner `pre` (same context, dtype and box
+ * as `op`): solve_gpbicgstab(..., precon=True) (Gpbicgstab.py:879-1201). */
+int dda_gpbicgstab_pre(dda_op* op, const dda_op* pre, const void* e_inc, double target, int max_iter, double ratio,
+                       void* p_out, dda_result* res, void* stream);
+
+/* dda_solve_batch with one preconditioner octant per instance (phat[j],
+ * engine layout, dtype of the solve) on the grid Px,Py,Pz, applied with
+ * pscale. */
+int dda_solve_batch_pre(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                        int Px, int Py, int Pz, double pscale, const void* const* phat, const dda_instance* inst,
+                        int nb, double target, int max_iter, double ratio, dda_result* res, void* stream);
+
+/* dda_solve_mixed_batch whose complex64 sweeps are preconditioned
+ * (phat64[j]: complex64 engine-layout octants); the FP64 refinement
+ * residual is unpreconditioned. */
+int dda_solve_mixed_batch_pre(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale, int Px,
+                              int Py, int Pz, double pscale, const void* const* phat64, const dda_instance* inst64,
+                              const dda_instance* inst128, int nb, double tol, double inner_tol, int max_iter,
+                              int max_outer, double ratio, dda_result* res, void* stream);
+
 /* ---- slot pool: continuous batching ------------------------------------- */
 /* A pool of `nslots` solver instances of one box / FFT size that requests
  * enter and leave independently: a request is admitted into a free slot

@@ -247,6 +247,82 @@ def fft_convolve(x, Ghat_oct, L=None):
     return y[:nx, :ny, :nz]
 
 
+def precondition_apply(x, P_oct, mask):
+    """M.x = mask * IFFT[ P . FFT(pad x) ] on the preconditioner's own grid
+    (2 (octant extent - 1) per axis; x placed at the origin, the result
+    cropped to the box): fft_matvec3 with optimized_dot_product_reduced_kernel,
+    Gpbicgstab.py:633-668 and :36-103 (same mirror rule as the interaction
+    octant)."""
+    x = np.asarray(x, dtype=np.complex128)
+    L = tuple(2 * (int(s) - 1) for s in P_oct.shape[:3])
+    y = fft_convolve(x, P_oct, L)
+    return y * np.asarray(mask, dtype=bool)[..., None]
+
+
+def occupancy_weights(occ):
+    """w(j) for lattice offsets j in (-n, n)^3, on the (2nx,2ny,2nz) grid
+    (offset j at index j mod 2n): the fraction of occupied sites whose
+    neighbour at offset j is occupied, R(j)/R(0), R the autocorrelation of the
+    occupancy, averaged over the 8 axis reflections of j so the weighted
+    kernel keeps the per-axis parity of G (and its octant storage)."""
+    occ = np.asarray(occ, dtype=bool)
+    nx, ny, nz = occ.shape
+    La = (2 * nx, 2 * ny, 2 * nz)
+    m = np.zeros(La)
+    m[:nx, :ny, :nz] = occ
+    R = np.real(sfft.ifftn(np.abs(sfft.fftn(m)) ** 2))
+    R = np.clip(R, 0.0, None) / max(R[0, 0, 0], 1e-300)
+    idx = [np.arange(L_) for L_ in La]
+    ref = [(-i) % L_ for i, L_ in zip(idx, La)]
+    W = np.zeros(La)
+    for sx in (idx[0], ref[0]):
+        for sy in (idx[1], ref[1]):
+            for sz in (idx[2], ref[2]):
+                W += R[np.ix_(sx, sy, sz)]
+    return W / 8.0
+
+
+def circulant_preconditioner(inv_alpha, k, d, L=None):
+    """Octant (hx,hy,hz,6) of the engine's preconditioner on the L grid
+    (n <= L per axis; default L = n):
+
+        P(q) = [abar I - FFT_L(-c)(q)]^-1,   c(t) = sum_{j = t mod L} w(j) G(j)
+
+    abar = mean inverse polarizability of the occupied sites, G the lattice
+    Green tensor at offsets j in (-n, n)^3 (zero at j = 0), w the occupancy
+    weights (``occupancy_weights``).  c is T. Chan's optimal circulant of the
+    masked interaction operator, folded onto the L-periodic grid; applied by
+    ``precondition_apply`` (which scales by 1/(Lx Ly Lz) through its
+    normalised inverse FFT) it is the inverse of that circulant.  The
+    reference calls preconditioner builders it does not define
+    (ddaforgit.py:1118-1136); this construction is the engine's own, written
+    for the reference's application format (Gpbicgstab.py:36-103, :633-668).
+    """
+    ia = np.asarray(inv_alpha, dtype=np.complex128)
+    nx, ny, nz = ia.shape
+    occ = ia != 0
+    abar = ia[occ].mean() if occ.any() else 1.0
+    if L is None:
+        L = (nx, ny, nz)
+    La = (2 * nx, 2 * ny, 2 * nz)
+    Gw = green_embedded(nx, ny, nz, k, d, La) * occupancy_weights(occ)[..., None]
+    F = np.zeros(tuple(L) + (6,), dtype=np.complex128)
+    tgt = []
+    for n_, La_, L_ in zip((nx, ny, nz), La, L):
+        i = np.arange(La_)
+        tgt.append(np.where(i < n_, i, i - La_) % L_)
+    np.add.at(F, np.ix_(*tgt), Gw)
+    Gh = sfft.fftn(-F, axes=(0, 1, 2), workers=_WORKERS)
+    Gh = Gh[:L[0] // 2 + 1, :L[1] // 2 + 1, :L[2] // 2 + 1]
+    T = np.empty(Gh.shape[:3] + (3, 3), dtype=np.complex128)
+    for a in range(3):
+        for b in range(3):
+            T[..., a, b] = -Gh[..., _COMP[a, b]]
+        T[..., a, a] += abar
+    Ti = np.linalg.inv(T)
+    return np.ascontiguousarray(np.stack([Ti[..., a, b] for a, b in _PAIRS], axis=-1))
+
+
 def prepare_interaction_matrices(alpha_array, k, d, cutoff=False, L=None):
     """(inv_alpha, mask, Ghat, None): ddaforgit.py:1085-1159 without the
     missing preconditioner builders."""
@@ -317,12 +393,16 @@ def _vdot(a, b):
 
 
 def solve_gpbicgstab(grid_size, inv_alpha, Ghat_oct, E_inc, mask, ratio,
-                     max_iter, target=1e-5, L=None, matvec=None):
+                     max_iter, target=1e-5, L=None, matvec=None, preconditioner=None):
     """GPBiCGSTAB with the reference's recurrence, resets, true-residual
     replacement at i==1, best-iterate tracking and return codes.
 
     Returns (iters, P (nx,ny,nz,3), lowest/initial, first/initial).
-    Gpbicgstab.py:957-1201 (precon=False: M = I, :634-635).
+    Gpbicgstab.py:957-1201.  ``preconditioner`` (an octant for
+    ``precondition_apply``) gives the reference's right-preconditioned form,
+    precon=True: A is applied to M p and M s (:1008, :1026), the residual
+    replacements use A M x (:1061-1064, :1143-1144) and the result is M x
+    (:1171-1199); without it M = I (:634-635).
     """
     nx, ny, nz = grid_size
     mask = np.asarray(mask).astype(bool).reshape(nx, ny, nz)
@@ -331,6 +411,16 @@ def solve_gpbicgstab(grid_size, inv_alpha, Ghat_oct, E_inc, mask, ratio,
         def matvec(v):
             return interaction_mult(v.reshape(nx, ny, nz, 3), Ghat_oct,
                                     inv_alpha, mask, L).ravel()
+    if preconditioner is None:
+        def msolve(v):
+            return v
+    else:
+        def msolve(v):
+            return precondition_apply(v.reshape(nx, ny, nz, 3), preconditioner, mask).ravel()
+    amul = matvec
+
+    def matvec(v):            # noqa: F811 -- A M
+        return amul(msolve(v))
     b = (np.asarray(E_inc, dtype=np.complex128).reshape(nx, ny, nz, 3)
          * mask[..., None]).ravel()
     r = b.copy()
@@ -416,12 +506,12 @@ def solve_gpbicgstab(grid_size, inv_alpha, Ghat_oct, E_inc, mask, ratio,
             p = r + beta * (p - u)
     shp = (nx, ny, nz, 3)
     if np.isnan(current) or last_change >= 5000:
-        return -(i + 1), best.reshape(shp), lowest / initial_norm, first / initial_norm
+        return -(i + 1), msolve(best).reshape(shp), lowest / initial_norm, first / initial_norm
     if i < max_iter - 1 and current >= target * initial_norm:
-        return -(i + 1), best.reshape(shp), lowest / initial_norm, first / initial_norm
+        return -(i + 1), msolve(best).reshape(shp), lowest / initial_norm, first / initial_norm
     if current >= target * initial_norm:
-        return max_iter, best.reshape(shp), lowest / initial_norm, first / initial_norm
-    return i + 1, x.reshape(shp), lowest / initial_norm, first / initial_norm
+        return max_iter, msolve(best).reshape(shp), lowest / initial_norm, first / initial_norm
+    return i + 1, msolve(x).reshape(shp), lowest / initial_norm, first / initial_norm
 
 
 def true_relative_residual(P, E_inc, Ghat_oct, inv_alpha, mask, L=None):

@@ -9,16 +9,16 @@ from .lattice import (Shape, Sphere, Cylinder, Ellipsoid, Rectangle, Prism, Shap
                       mark_shapes, trim_zero_faces, create_alpha_and_n_arrays, incident_field,
                       build_problem_from_shapes, sphere_occupancy, ellipsoid_occupancy, euler_rotation)
 from .engine import (DDAOperator, SolveInfo, solve_many, cross_sections, green_octant, fft_lengths,
-                     compiled_fft_lengths, far_field, differential_cross_section)
+                     compiled_fft_lengths, far_field, differential_cross_section, Preconditioner, precond_lengths)
 from .reference_api import (generate_interaction_row, prepare_interaction_matrices, interaction_mult, fft_matvec,
-                            E_field_solver, solve_gpbicgstab, Gpbicgstab, run_solver, expand_octant)
+                            fft_matvec3, E_field_solver, solve_gpbicgstab, Gpbicgstab, run_solver, expand_octant)
 
 __all__ = [
     "Shape", "Sphere", "Cylinder", "Ellipsoid", "Rectangle", "Prism", "ShapeManager", "calculate_alpha",
     "mark_shapes", "trim_zero_faces", "create_alpha_and_n_arrays", "incident_field", "build_problem_from_shapes",
     "sphere_occupancy", "ellipsoid_occupancy", "euler_rotation",
     "DDAOperator", "SolveInfo", "solve_many", "cross_sections", "green_octant", "fft_lengths",
-    "compiled_fft_lengths", "far_field", "differential_cross_section",
-    "generate_interaction_row", "prepare_interaction_matrices", "interaction_mult", "fft_matvec",
+    "compiled_fft_lengths", "far_field", "differential_cross_section", "Preconditioner", "precond_lengths",
+    "generate_interaction_row", "prepare_interaction_matrices", "interaction_mult", "fft_matvec", "fft_matvec3",
     "E_field_solver", "solve_gpbicgstab", "Gpbicgstab", "run_solver", "expand_octant",
 ]

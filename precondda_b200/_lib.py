@@ -43,7 +43,8 @@ EXPORTS = (
     "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
     "dda_voxelize", "dda_incident_field", "dda_slots_create", "dda_slots_destroy", "dda_slots_capacity",
     "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
-    "dda_far_field", "dda_matvec_batch",
+    "dda_far_field", "dda_matvec_batch", "dda_precond_build", "dda_precond_op_create", "dda_gpbicgstab_pre",
+    "dda_solve_batch_pre", "dda_solve_mixed_batch_pre",
 )
 
 
@@ -113,6 +114,14 @@ def _declare(lib):
     lib.dda_slots_release.argtypes = [vp, i]
     lib.dda_far_field.argtypes = [vp, i, i, i, i, d, d, vp, i, C.POINTER(d), C.POINTER(d), vp]
     lib.dda_matvec_batch.argtypes = [C.POINTER(vp), i, i, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
+    lib.dda_precond_build.argtypes = [vp, i, i, i, i, i, i, d, d, vp, i, vp, vp, vp]
+    lib.dda_precond_op_create.argtypes = [vp, i, i, i, i, i, i, i, vp, d, vp, C.POINTER(vp)]
+    lib.dda_gpbicgstab_pre.argtypes = [vp, vp, vp, d, i, d, vp, C.POINTER(dda_result), vp]
+    lib.dda_solve_batch_pre.argtypes = [vp, i, i, i, i, i, i, i, d, i, i, i, d, C.POINTER(vp),
+                                        C.POINTER(dda_instance), i, d, i, d, C.POINTER(dda_result), vp]
+    lib.dda_solve_mixed_batch_pre.argtypes = [vp, i, i, i, i, i, i, d, i, i, i, d, C.POINTER(vp),
+                                              C.POINTER(dda_instance), C.POINTER(dda_instance), i, d, d, i, i, d,
+                                              C.POINTER(dda_result), vp]
     return lib
 
 

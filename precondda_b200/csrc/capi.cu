@@ -42,10 +42,14 @@ static bool length_ok(int L, int dtype) {
   return fft_size_compiled(L);
 }
 
-static int make_geo(int nx, int ny, int nz, int Lx, int Ly, int Lz, int dtype, Geo* g) {
+// minmul = 2: an operator's grid (linear convolution, L >= 2n); 1: a
+// preconditioner's grid (the reference places x at the origin of any grid
+// L >= n and crops, Gpbicgstab.py:636-666)
+static int make_geo(int nx, int ny, int nz, int Lx, int Ly, int Lz, int dtype, Geo* g, int minmul = 2) {
   if (nx < 1 || ny < 1 || nz < 1) { set_error("box dimensions must be >= 1"); return DDA_ERR_BAD_SHAPE; }
-  if (Lx < 2 * nx || Ly < 2 * ny || Lz < 2 * nz) {
-    set_error("FFT lengths must be >= twice the box dimensions");
+  if (Lx < minmul * nx || Ly < minmul * ny || Lz < minmul * nz) {
+    set_error(minmul == 2 ? "FFT lengths must be >= twice the box dimensions"
+                          : "preconditioner FFT lengths must be >= the box dimensions");
     return DDA_ERR_BAD_SHAPE;
   }
   if (!length_ok(Lx, dtype) || !length_ok(Ly, dtype) || !length_ok(Lz, dtype)) {
@@ -279,6 +283,64 @@ int dda_matvec_batch(dda_op* const* ops, int nb, int mode, const void* const* x,
   return DDA_OK;
 }
 
+int dda_precond_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d,
+                      const void* inv_alpha128, int layout, void* out_c128, void* out_c64, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, DDA_C128, &g, 1))) return rc;
+  if (!(k > 0) || !(d > 0)) { set_error("k and d must be positive"); return DDA_ERR_ARG; }
+  if (!inv_alpha128) { set_error("null inverse polarizability"); return DDA_ERR_ARG; }
+  if (!out_c128 && !out_c64) { set_error("no output"); return DDA_ERR_ARG; }
+  if (layout != DDA_GHAT_REFERENCE && layout != DDA_GHAT_ENGINE) { set_error("bad octant layout"); return DDA_ERR_ARG; }
+  return precond_build(ctx->c, g, k, d, inv_alpha128, layout, out_c128, out_c64, (cudaStream_t)stream);
+}
+
+int dda_precond_op_create(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* phat,
+                          double scale, const void* inv_alpha, dda_op** out) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!out || !phat || !inv_alpha) { set_error("null argument"); return DDA_ERR_ARG; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  *out = nullptr;
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g, 1))) return rc;
+  dda_op* op = new (std::nothrow) dda_op();
+  if (!op) { set_error("host allocation failed"); return DDA_ERR_OOM; }
+  op->ctx = ctx; op->dtype = dtype; op->g = g; op->gscale = scale; op->ghat = phat; op->inva = inv_alpha;
+  op->pc = make_pass_cfg(g, dtype == DDA_C128);
+  *out = op;
+  return DDA_OK;
+}
+
+static int pre_spec(const dda_ctx* ctx, int nx, int ny, int nz, int Px, int Py, int Pz, double pscale,
+                    const void* const* phat, int nb, int dtype, PreSpec* ps) {
+  (void)ctx;
+  if (!phat) { set_error("null preconditioner list"); return DDA_ERR_ARG; }
+  for (int j = 0; j < nb; ++j)
+    if (!phat[j]) { set_error("null preconditioner octant"); return DDA_ERR_ARG; }
+  int rc = make_geo(nx, ny, nz, Px, Py, Pz, dtype, &ps->g, 1);
+  if (rc) return rc;
+  ps->scale = pscale;
+  ps->phat = phat;
+  return DDA_OK;
+}
+
+int dda_gpbicgstab_pre(dda_op* op, const dda_op* pre, const void* e_inc, double target, int max_iter, double ratio,
+                       void* p_out, dda_result* res, void* stream) {
+  if (!op || !pre) { set_error("null operator"); return DDA_ERR_ARG; }
+  if (pre->ctx != op->ctx || pre->dtype != op->dtype || pre->g.nx != op->g.nx || pre->g.ny != op->g.ny ||
+      pre->g.nz != op->g.nz) {
+    set_error("preconditioner must share the operator's context, dtype and box");
+    return DDA_ERR_ARG;
+  }
+  dda_instance in{op->ghat, op->inva, e_inc, p_out};
+  const void* ph[1] = {pre->ghat};
+  return dda_solve_batch_pre(op->ctx, op->dtype, op->g.nx, op->g.ny, op->g.nz, op->g.Lx, op->g.Ly, op->g.Lz,
+                             op->gscale, pre->g.Lx, pre->g.Ly, pre->g.Lz, pre->gscale, ph, &in, 1, target, max_iter,
+                             ratio, res, stream);
+}
+
 int dda_gpbicgstab(dda_op* op, const void* e_inc, double target, int max_iter, double ratio, void* p_out,
                    dda_result* res, void* stream) {
   if (!op) { set_error("null operator"); return DDA_ERR_ARG; }
@@ -304,6 +366,48 @@ int dda_solve_batch(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int
   if (dtype == DDA_C128)
     return solve_batch<double>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream);
   return solve_batch<float>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream);
+}
+
+int dda_solve_batch_pre(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                        int Px, int Py, int Pz, double pscale, const void* const* phat, const dda_instance* inst,
+                        int nb, double target, int max_iter, double ratio, dda_result* res, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!inst || nb < 1) { set_error("no instances"); return DDA_ERR_ARG; }
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g))) return rc;
+  PreSpec ps;
+  if ((rc = pre_spec(ctx, nx, ny, nz, Px, Py, Pz, pscale, phat, nb, dtype, &ps))) return rc;
+  for (int j = 0; j < nb; ++j)
+    if (!inst[j].ghat || !inst[j].inv_alpha || !inst[j].e_inc || !inst[j].p_out) {
+      set_error("null instance pointer");
+      return DDA_ERR_ARG;
+    }
+  if (dtype == DDA_C128)
+    return solve_batch<double>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream, &ps);
+  return solve_batch<float>(ctx->c, g, gscale, inst, nb, target, max_iter, ratio, res, (cudaStream_t)stream, &ps);
+}
+
+int dda_solve_mixed_batch_pre(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale, int Px,
+                              int Py, int Pz, double pscale, const void* const* phat64, const dda_instance* inst64,
+                              const dda_instance* inst128, int nb, double tol, double inner_tol, int max_iter,
+                              int max_outer, double ratio, dda_result* res, void* stream) {
+  int rc = check_ctx(ctx);
+  if (rc) return rc;
+  if (!inst64 || !inst128 || nb < 1) { set_error("no instances"); return DDA_ERR_ARG; }
+  Geo g;
+  if ((rc = make_geo(nx, ny, nz, Lx, Ly, Lz, DDA_C128, &g))) return rc;
+  PreSpec ps;
+  if ((rc = pre_spec(ctx, nx, ny, nz, Px, Py, Pz, pscale, phat64, nb, DDA_C64, &ps))) return rc;
+  for (int j = 0; j < nb; ++j)
+    if (!inst64[j].ghat || !inst64[j].inv_alpha || !inst128[j].ghat || !inst128[j].inv_alpha || !inst128[j].e_inc ||
+        !inst128[j].p_out) {
+      set_error("null instance pointer");
+      return DDA_ERR_ARG;
+    }
+  return solve_mixed(ctx->c, g, gscale, inst64, inst128, nb, tol, inner_tol, max_iter, max_outer, ratio, res,
+                     (cudaStream_t)stream, &ps);
 }
 
 int dda_solve_mixed_batch(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,

@@ -91,11 +91,13 @@ constexpr int kMaxStages = 12;
 // ---------------------------------------------------------------------------
 enum VecId {
   V_R = 0, V_RHAT, V_P, V_V, V_T, V_S, V_SPREV, V_U, V_Z, V_W, V_Y,
-  V_X, V_B, V_TMP, V_XA, V_XB, V_XC, kNumVec
+  V_X, V_B, V_TMP, V_XA, V_XB, V_XC,
+  V_MH,             // preconditioned vector M p / M s / M x (preconditioned solves only)
+  kNumVec
 };
 
 // control condition under which a (matvec / update) kernel does work
-enum Cond { C_ALWAYS = 0, C_ACTIVE = 1, C_TRUE_RES = 2, C_RESET_RES = 3, C_RESET = 4 };
+enum Cond { C_ALWAYS = 0, C_ACTIVE = 1, C_TRUE_RES = 2, C_RESET_RES = 3, C_RESET = 4, C_LIVE = 5 };
 
 // solver status codes (mirrors the sign convention of the reference's
 // iteration return value)
@@ -105,6 +107,7 @@ struct InstState {
   // vector table (device pointers, element type given by the batch dtype)
   void* vec[kNumVec];
   const void* ghat;    // octant of FFT(-G), engine layout (6,hx,hy,hz)
+  const void* pghat;   // preconditioner octant, engine layout, on its own grid (or null)
   const void* inva;    // inverse polarizability per site (N complex)
   void* t1;            // scratch (nx,ny,Lz,3)
   void* t2;            // scratch (nx,Ly,Lz,3)
@@ -146,6 +149,7 @@ __device__ __forceinline__ bool cond_ok(const InstState& s, int cond) {
     case C_TRUE_RES: return s.active && !s.done && s.flag_true_res;
     case C_RESET_RES: return s.active && !s.done && s.flag_reset && s.flag_reset_res;
     case C_RESET: return s.active && !s.done;
+    case C_LIVE: return s.active != 0;
   }
   return false;
 }

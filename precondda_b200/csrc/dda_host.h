@@ -79,7 +79,7 @@ struct Ctx {
   const void* twiddles(int L, bool dbl);
   // cached solver workspace for (dtype, geometry, batch size)
   // (tag separates workspaces of different users of the same shape)
-  BatchWs* workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag = 0);
+  BatchWs* workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag = 0, const Geo* gp = nullptr);
   void trim();
   ~Ctx();
 };
@@ -97,12 +97,28 @@ struct PassCfg {
 
 PassCfg make_pass_cfg(const Geo& g, bool dbl);
 
+// Preconditioner of a batched solve (the reference's right-preconditioned
+// GPBiCGSTAB, precon=True): per-instance octants (engine layout) on the grid
+// g.Lx/Ly/Lz (box g.nx/ny/nz, the solve's), applied as
+//   M x = mask * scale * IFFT[ P . FFT(pad x) ]   (cropped to the box)
+// i.e. the matvec passes in MV_CONV_MASKED mode with the x pass on
+// InstState::pghat.
+struct PreSpec {
+  Geo g{};
+  double scale = 1.0;
+  const void* const* phat = nullptr;
+};
+
 // Device memory of a batch of solver instances sharing one geometry.
 struct BatchWs {
   int dtype = 0, nb = 0, nslot = 0, RB = 1;
   bool full = true;
+  bool pre = false;              // preconditioned solve: gp / pcp / pscale and the V_MH slot
   Geo g{};
   PassCfg pc{};
+  Geo gp{};
+  PassCfg pcp{};
+  double pscale = 1.0, graph_pscale = 0.0;
   size_t esz = 8, n3 = 0, t1n = 0, t2n = 0;
   void* vecs = nullptr;          // nb * nslot * n3 complex
   void* scratch = nullptr;       // nb * (t1n + t2n) complex
@@ -117,7 +133,9 @@ struct BatchWs {
   cudaGraphExec_t gexec = nullptr;
   double graph_gscale = 0.0;
   long long graph_kernels = 0;
-  int alloc(Ctx& c, int dtype, const Geo& g, int nb, bool full);
+  int alloc(Ctx& c, int dtype, const Geo& g, int nb, bool full, const Geo* gp = nullptr);
+  // vector slots the workspace allocates, in storage order
+  const int* slots() const;
   // state of instance j: vector slots and scratch; with `sites` the
   // instance stores occupied sites only (its map is built on the device)
   void base_state(int j, InstState& S, bool sites = false) const;
@@ -135,6 +153,7 @@ struct MvFuse {
   int pre = MV_PRE_NONE, post = MV_POST_NONE;
   double* red = nullptr;      // >= nb * grid1 * KRED doubles
   unsigned* cnt = nullptr;    // per-instance tickets
+  int tensor = 0;             // octant of the x pass: 0 InstState::ghat, 1 InstState::pghat
 };
 
 // Enqueue the 5-pass matvec for a batch of instances that share Geo.
@@ -176,10 +195,11 @@ cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s,
 
 template <typename R>
 int solve_batch(Ctx& c, const Geo& g, double gscale, const struct dda_instance* inst, int nb, double target,
-                int max_iter, double ratio, struct dda_result* res, cudaStream_t user);
+                int max_iter, double ratio, struct dda_result* res, cudaStream_t user, const PreSpec* pre = nullptr);
+// pre (optional) preconditions the complex64 sweeps; its octants are complex64
 int solve_mixed(Ctx& c, const Geo& g, double gscale, const struct dda_instance* i64,
                 const struct dda_instance* i128, int nb, double tol, double inner_tol, int max_iter, int max_outer,
-                double ratio, struct dda_result* res, cudaStream_t user);
+                double ratio, struct dda_result* res, cudaStream_t user, const PreSpec* pre = nullptr);
 template <typename R>
 void launch_xsec(const void* P, const void* E, const void* ia, long long nsite, double k, double* red, unsigned* cnt,
                  int RB, double* out, cudaStream_t s);
@@ -203,6 +223,19 @@ void launch_site_map(InstState* st, int nb, long long nsite, int* bcount, cudaSt
 // dense solution of each finished instance into S.out
 template <typename R>
 void launch_store_solution(InstState* st, int nb, long long n3, int num_sms, cudaStream_t s, const int* act);
+// S.vec[V_TMP] := the iterate the solution store / refinement accumulate
+// reads (converged: x; else the best iterate; else x)
+void launch_pick_solution(InstState* st, int nb, cudaStream_t s, const int* act);
+
+// Preconditioner builder (precond.cu): octant (engine or reference layout)
+// of the occupancy-weighted circulant inverse on the grid g.Lx/Ly/Lz; see
+// dda_precond_build.
+int precond_build(Ctx& ctx, const Geo& g, double k, double d, const void* inv_alpha128, int layout, void* out128,
+                  void* out64, cudaStream_t s);
+// The y and x passes of the Green build from the z pass's output b1
+// (Lx,Ly,hz,6) FP64: octant of -scale * FFT (green.cu).
+int green_yx(Ctx& ctx, const Geo& g, const void* b1, double scale, void* out128, void* out64, int soa,
+             cudaStream_t s);
 // whether solver workspaces store occupied sites only (DDA_NO_COMPRESS=1: dense)
 bool compress_sites();
 

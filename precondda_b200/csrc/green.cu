@@ -161,35 +161,31 @@ int ghat_to_soa(const void* src, void* dst, long long H, bool dbl, cudaStream_t 
   return cudaGetLastError() == cudaSuccess ? 0 : 6;
 }
 
-int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64, int soa,
-                cudaStream_t s) {
+int green_yx(Ctx& ctx, const Geo& g, const void* b1v, double scale, void* out128, void* out64, int soa,
+             cudaStream_t s) {
   const int cap = GEPT * GNT;
-  if (6 * g.Lz > cap || 6 * g.Ly > cap || 6 * g.Lx > cap) {
+  if (6 * g.Ly > cap || 6 * g.Lx > cap) {
     set_error("green_build: FFT length too large (max 512)");
     return 7;
   }
-  GZ kz = green_z_kernel(g.Lz);
   GC ky = green_col_kernel(g.Ly, 1), kx = green_col_kernel(g.Lx, 0);
-  if (!kz || !ky || !kx) {
+  if (!ky || !kx) {
     set_error("green_build: FFT length has no compiled kernel");
     return 7;
   }
-  DDA_CUDA_OK(cudaFuncSetAttribute((const void*)kz, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   DDA_CUDA_OK(cudaFuncSetAttribute((const void*)ky, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   DDA_CUDA_OK(cudaFuncSetAttribute((const void*)kx, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
   const double2* twx = (const double2*)ctx.twiddles(g.Lx, true);
   const double2* twy = (const double2*)ctx.twiddles(g.Ly, true);
-  const double2* twz = (const double2*)ctx.twiddles(g.Lz, true);
-  if (!twx || !twy || !twz) { set_error("green_build: twiddle allocation failed"); return 2; }
-  const size_t n1 = (size_t)g.Lx * g.Ly * g.hz * 6, n2 = (size_t)g.Lx * g.hy * g.hz * 6;
-  double2 *b1 = nullptr, *b2 = nullptr;
-  DDA_CUDA_OK(cudaMallocAsync((void**)&b1, n1 * sizeof(double2), s));
-  cudaError_t e = cudaMallocAsync((void**)&b2, n2 * sizeof(double2), s);
-  if (e != cudaSuccess) { cudaFreeAsync(b1, s); set_error("green_build: out of memory"); return 2; }
-  // G1: z with G evaluated in place
-  const int NL = cap / (6 * g.Lz);
-  const long long grid1 = ((long long)g.Lx * g.Ly + NL - 1) / NL;
-  kz<<<(unsigned)grid1, GNT, (size_t)NL * 6 * g.Lz * sizeof(double2), s>>>(g, twz, k, d, NL, b1);
+  if (!twx || !twy) { set_error("green_build: twiddle allocation failed"); return 2; }
+  const double2* b1 = (const double2*)b1v;
+  const size_t n2 = (size_t)g.Lx * g.hy * g.hz * 6;
+  double2* b2 = nullptr;
+  if (cudaMallocAsync((void**)&b2, n2 * sizeof(double2), s) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("green_build: out of memory");
+    return 2;
+  }
   // G2: y
   int Tz = cap / (6 * g.Ly);
   if (Tz > g.hz) Tz = g.hz;
@@ -203,12 +199,50 @@ int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* 
   kx<<<(unsigned)(g.hy * ntz), GNT, (size_t)g.Lx * 6 * Tz * sizeof(double2), s>>>(g, twx, Tz, ntz, b2,
                                                                                   (double2*)out128, (float2*)out64,
                                                                                   scale, soa);
-  note_launch(s, 3);
-  e = cudaGetLastError();
-  cudaFreeAsync(b1, s);
+  note_launch(s, 2);
+  const cudaError_t e = cudaGetLastError();
   cudaFreeAsync(b2, s);
   if (e != cudaSuccess) { set_error(std::string("green_build: ") + cudaGetErrorString(e)); return 6; }
   return 0;
+}
+
+int green_build(Ctx& ctx, const Geo& g, double k, double d, double scale, void* out128, void* out64, int soa,
+                cudaStream_t s) {
+  const int cap = GEPT * GNT;
+  if (6 * g.Lz > cap) {
+    set_error("green_build: FFT length too large (max 512)");
+    return 7;
+  }
+  GZ kz = green_z_kernel(g.Lz);
+  if (!kz) {
+    set_error("green_build: FFT length has no compiled kernel");
+    return 7;
+  }
+  DDA_CUDA_OK(cudaFuncSetAttribute((const void*)kz, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  const double2* twz = (const double2*)ctx.twiddles(g.Lz, true);
+  if (!twz) { set_error("green_build: twiddle allocation failed"); return 2; }
+  const size_t n1 = (size_t)g.Lx * g.Ly * g.hz * 6;
+  double2* b1 = nullptr;
+  if (cudaMallocAsync((void**)&b1, n1 * sizeof(double2), s) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("green_build: out of memory");
+    return 2;
+  }
+  // G1: z with G evaluated in place
+  const int NL = cap / (6 * g.Lz);
+  const long long grid1 = ((long long)g.Lx * g.Ly + NL - 1) / NL;
+  kz<<<(unsigned)grid1, GNT, (size_t)NL * 6 * g.Lz * sizeof(double2), s>>>(g, twz, k, d, NL, b1);
+  note_launch(s, 1);
+  cudaError_t e = cudaGetLastError();
+  int rc = 0;
+  if (e != cudaSuccess) {
+    set_error(std::string("green_build: ") + cudaGetErrorString(e));
+    rc = 6;
+  } else {
+    rc = green_yx(ctx, g, b1, scale, out128, out64, soa, s);
+  }
+  cudaFreeAsync(b1, s);
+  return rc;
 }
 
 }  // namespace dda

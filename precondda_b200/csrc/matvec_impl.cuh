@@ -231,7 +231,7 @@ __device__ __forceinline__ int pencil_ky(int p, int Ly) {
 template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
-                                                             int ntz_, R gscale) {
+                                                             int ntz_, R gscale, int op) {
   grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
@@ -248,7 +248,8 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t2 = (C*)S.t2;
-  const C* __restrict__ gh = (const C*)S.ghat;
+  // op 0: the interaction octant; op 1: the preconditioner octant
+  const C* __restrict__ gh = (const C*)(op ? S.pghat : S.ghat);
   const int tz = CUBE ? TZC : tz_;
   const int ntz = CUBE ? NTZC : ntz_;
   const int Ly = CUBE ? LX : g.Ly, Lz = CUBE ? LX : g.Lz;
@@ -326,7 +327,7 @@ constexpr int p3_min_blocks() {
 template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
-                                                             int ntz_, R gscale) {
+                                                             int ntz_, R gscale, int op) {
   grid_dep_begin();
   typedef typename CT<R>::T C;
   typedef P3Shape<R, LX, V> SH;
@@ -343,7 +344,8 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   InstState& S = st[inst_of(act)];
   if (!cond_ok(S, cond)) return;
   C* __restrict__ t2 = (C*)S.t2;
-  const C* __restrict__ gh = (const C*)S.ghat;
+  // op 0: the interaction octant; op 1: the preconditioner octant
+  const C* __restrict__ gh = (const C*)(op ? S.pghat : S.ghat);
   const int tz = CUBE ? TZC : tz_;
   const int ntz = CUBE ? NTZC : ntz_;
   const int Ly = CUBE ? LX : g.Ly, Lz = CUBE ? LX : g.Lz;
@@ -728,7 +730,7 @@ template <typename R> struct MvSet {
   typedef typename CT<R>::T C;
   typedef void (*P1)(Geo, const C*, InstState*, const int*, int, int, int, int);
   typedef void (*PY)(Geo, const C*, InstState*, const int*, int, int, int);
-  typedef void (*P3)(Geo, const C*, InstState*, const int*, int, int, int, R);
+  typedef void (*P3)(Geo, const C*, InstState*, const int*, int, int, int, R, int);
   typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int, int, double*, unsigned*);
   typedef void (*PF)(Geo, const C*, InstState*, const int*, int, int);
   typedef void (*PI)(Geo, const C*, InstState*, const int*, int, int, int, int);
@@ -880,7 +882,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
       return e;
   }
   if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond, pc.tz3,
-                      pc.ntz3, (R)gscale)))
+                      pc.ntz3, (R)gscale, fz.tensor)))
     return e;
   if (fi) {
     if ((e = launch_cluster(k.ki, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemi, s, g, twz, st, act,

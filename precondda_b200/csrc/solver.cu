@@ -18,9 +18,15 @@ static thread_local std::string g_err;
 void set_error(const std::string& m) { g_err = m; }
 
 static std::atomic<long long> g_launches{0};
+// kernels this thread enqueued into a stream capture (counted per captured
+// segment by capture_iteration)
+static thread_local long long g_captured = 0;
 void note_launch(cudaStream_t s, long long n) {
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) return;
+  if (cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone) {
+    g_captured += n;
+    return;
+  }
   g_launches.fetch_add(n, std::memory_order_relaxed);
 }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
@@ -60,7 +66,11 @@ Ctx::~Ctx() {
 // ---------------------------------------------------------------------------
 static const int kFullSlots[] = {V_R, V_RHAT, V_P, V_V, V_T, V_S, V_SPREV, V_U, V_Z, V_W, V_Y, V_B, V_TMP,
                                  V_XA, V_XB, V_XC};
+static const int kPreSlots[] = {V_R, V_RHAT, V_P, V_V, V_T, V_S, V_SPREV, V_U, V_Z, V_W, V_Y, V_B, V_TMP,
+                                V_XA, V_XB, V_XC, V_MH};
 static const int kLightSlots[] = {V_R, V_B};
+
+const int* BatchWs::slots() const { return full ? (pre ? kPreSlots : kFullSlots) : kLightSlots; }
 
 BatchWs::~BatchWs() {
   if (gexec) cudaGraphExecDestroy(gexec);
@@ -69,15 +79,24 @@ BatchWs::~BatchWs() {
   cudaFree(cidx); cudaFree(bcount);
 }
 
-int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_) {
+int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_, const Geo* gp_) {
   dtype = dtype_; g = g_; nb = nb_; full = full_;
+  pre = full && gp_ != nullptr;
   esz = dtype == DDA_C128 ? 16 : 8;
   n3 = (size_t)g.nsite * 3;
-  nslot = full ? (int)(sizeof(kFullSlots) / sizeof(int)) : (int)(sizeof(kLightSlots) / sizeof(int));
+  nslot = full ? (pre ? (int)(sizeof(kPreSlots) / sizeof(int)) : (int)(sizeof(kFullSlots) / sizeof(int)))
+               : (int)(sizeof(kLightSlots) / sizeof(int));
   pc = make_pass_cfg(g, dtype == DDA_C128);
   RB = grid_for((long long)n3, nb, c.num_sms);
   t1n = (size_t)g.nx * g.ny * g.Lz * 3;
   t2n = (size_t)g.nx * g.Ly * g.Lz * 3;
+  if (pre) {
+    // the preconditioner passes share the transform scratch
+    gp = *gp_;
+    pcp = make_pass_cfg(gp, dtype == DDA_C128);
+    t1n = std::max(t1n, (size_t)gp.nx * gp.ny * gp.Lz * 3);
+    t2n = std::max(t2n, (size_t)gp.nx * gp.Ly * gp.Lz * 3);
+  }
   if (cudaMalloc(&vecs, (size_t)nb * nslot * n3 * esz) != cudaSuccess ||
       cudaMalloc(&scratch, (size_t)nb * (t1n + t2n) * esz) != cudaSuccess ||
       cudaMalloc((void**)&d_st, nb * sizeof(InstState)) != cudaSuccess ||
@@ -108,9 +127,9 @@ void BatchWs::base_state(int j, InstState& S, bool sites) const {
   std::memset(&S, 0, sizeof(S));
   S.nv = (long long)n3;
   S.cidx = (sites && cidx) ? cidx + (size_t)j * g.nsite : nullptr;
-  const int* slots = full ? kFullSlots : kLightSlots;
+  const int* sl = slots();
   char* v0 = (char*)vecs + (size_t)j * nslot * n3 * esz;
-  for (int q = 0; q < nslot; ++q) S.vec[slots[q]] = v0 + (size_t)q * n3 * esz;
+  for (int q = 0; q < nslot; ++q) S.vec[sl[q]] = v0 + (size_t)q * n3 * esz;
   if (full) S.vec[V_X] = S.vec[V_XA];
   char* sc = (char*)scratch + (size_t)j * (t1n + t2n) * esz;
   S.t1 = sc;
@@ -118,15 +137,15 @@ void BatchWs::base_state(int j, InstState& S, bool sites) const {
   S.best_x = -1;
 }
 
-BatchWs* Ctx::workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag) {
-  char key[160];
-  snprintf(key, sizeof(key), "%d:%d,%d,%d:%d,%d,%d:%d:%d:%d", dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, nb,
-           full ? 1 : 0, tag);
+BatchWs* Ctx::workspace(int dtype, const Geo& g, int nb, bool full, int* err, int tag, const Geo* gp) {
+  char key[200];
+  snprintf(key, sizeof(key), "%d:%d,%d,%d:%d,%d,%d:%d:%d:%d:p%d,%d,%d", dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz,
+           nb, full ? 1 : 0, tag, gp ? gp->Lx : 0, gp ? gp->Ly : 0, gp ? gp->Lz : 0);
   std::lock_guard<std::mutex> lk(mu);
   auto it = ws.find(key);
   if (it != ws.end()) return it->second;
   BatchWs* w = new BatchWs();
-  const int e = w->alloc(*this, dtype, g, nb, full);
+  const int e = w->alloc(*this, dtype, g, nb, full, gp);
   if (e != DDA_OK) { delete w; *err = e; return nullptr; }
   ws[key] = w;
   return w;
@@ -151,10 +170,25 @@ static bool fuse_krylov() {
   return e && *e == '1';
 }
 
+// out = A in, or A M in for a preconditioned workspace (M in goes to V_MH):
+// Gpbicgstab.py:1008-1015, :1026-1033 and the residuals :1061-1064, :1143-1144
+template <typename R>
+static cudaError_t amul(Ctx& c, BatchWs& w, int in, int out, int mode, int cond, double gscale, cudaStream_t s) {
+  if (w.pre) {
+    MvFuse f;
+    f.tensor = 1;
+    cudaError_t e = launch_matvec<R>(c, w.gp, w.pcp, w.d_st, nullptr, w.nb, in, V_MH, MV_CONV_MASKED, cond, w.pscale,
+                                     s, f);
+    if (e != cudaSuccess) return e;
+    in = V_MH;
+  }
+  return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, in, out, mode, cond, gscale, s);
+}
+
 template <typename R>
 static cudaError_t enqueue_front(Ctx& c, BatchWs& w, double gscale, cudaStream_t s, const KrylovLaunch& k) {
   cudaError_t e;
-  if (fuse_krylov()) {
+  if (fuse_krylov() && !w.pre) {
     MvFuse f1, f2;
     f1.post = MV_POST_ALPHA; f1.red = w.red; f1.cnt = w.cnt;
     f2.pre = MV_PRE_SY; f2.post = MV_POST_ZETA; f2.red = w.red; f2.cnt = w.cnt;
@@ -163,10 +197,10 @@ static cudaError_t enqueue_front(Ctx& c, BatchWs& w, double gscale, cudaStream_t
     if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s, f2)))
       return e;
   } else {
-    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
+    if ((e = amul<R>(c, w, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
     launch_alpha<R>(k, s);
     launch_sy<R>(k, s);
-    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return e;
+    if ((e = amul<R>(c, w, V_S, V_T, MV_AX, C_ACTIVE, gscale, s))) return e;
     launch_zeta<R>(k, s);
   }
   launch_uzrx<R>(k, s);
@@ -178,11 +212,9 @@ cudaError_t enqueue_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s)
   KrylovLaunch k{w.d_st, nullptr, w.nb, w.red, w.cnt, (long long)w.n3, w.RB};
   cudaError_t e;
   if ((e = enqueue_front<R>(c, w, gscale, s, k))) return e;
-  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s)))
-    return e;
+  if ((e = amul<R>(c, w, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s))) return e;
   launch_norm<R>(k, s);
-  if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s)))
-    return e;
+  if ((e = amul<R>(c, w, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s))) return e;
   launch_fin<R>(k, s);
   return cudaGetLastError();
 }
@@ -243,29 +275,37 @@ cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s,
     k.cond_reset = hR;
     std::vector<cudaGraphNode_t> none, d1, d2, d3;
     cudaGraphNode_t n1 = nullptr, n2 = nullptr;
+    // kernels every launch of the graph runs: the three unconditional
+    // segments (the bodies of the IF nodes are not counted)
+    long long nk = 0, c0 = 0;
+    c0 = g_captured;
     e = capture_segment(s, G, none, d1, [&]() -> cudaError_t { return enqueue_front<R>(c, w, gscale, s, k); });
+    nk += g_captured - c0;
     if (e == cudaSuccess)
       e = add_if(s, G, hT, d1, &n1, [&]() -> cudaError_t {
-        return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s);
+        return amul<R>(c, w, V_X, V_R, MV_RESIDUAL, C_TRUE_RES, gscale, s);
       });
+    c0 = g_captured;
     if (e == cudaSuccess)
       e = capture_segment(s, G, std::vector<cudaGraphNode_t>{n1}, d2, [&]() -> cudaError_t {
         launch_norm<R>(k, s);
         return cudaGetLastError();
       });
+    nk += g_captured - c0;
     if (e == cudaSuccess)
       e = add_if(s, G, hR, d2, &n2, [&]() -> cudaError_t {
-        return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s);
+        return amul<R>(c, w, V_X, V_R, MV_RESIDUAL, C_RESET_RES, gscale, s);
       });
+    c0 = g_captured;
     if (e == cudaSuccess)
       e = capture_segment(s, G, std::vector<cudaGraphNode_t>{n2}, d3, [&]() -> cudaError_t {
         launch_fin<R>(k, s);
         return cudaGetLastError();
       });
+    nk += g_captured - c0;
     if (e == cudaSuccess) {
       *out = G;
-      // kernels every launch runs (conditional bodies excluded)
-      *kernels = fuse_krylov() ? 5 + 5 + 3 : 5 + 5 + 6;
+      *kernels = nk;
       return cudaSuccess;
     }
     cudaGetLastError();
@@ -275,15 +315,15 @@ cudaError_t capture_iteration(Ctx& c, BatchWs& w, double gscale, cudaStream_t s,
   cudaGraphDestroy(G);
   G = nullptr;
   if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+  const long long c1 = g_captured;
   cudaError_t e1 = enqueue_iteration<R>(c, w, gscale, s);
+  const long long nk = g_captured - c1;
   e = cudaStreamEndCapture(s, &G);
   if (e1 != cudaSuccess || e != cudaSuccess) {
     if (G) cudaGraphDestroy(G);
     return e1 != cudaSuccess ? e1 : e;
   }
-  size_t nn = 0;
-  cudaGraphGetNodes(G, nullptr, &nn);
-  *kernels = (long long)nn;
+  *kernels = nk;
   *out = G;
   return cudaSuccess;
 }
@@ -293,10 +333,13 @@ template cudaError_t capture_iteration<double>(Ctx&, BatchWs&, double, cudaStrea
 
 template <typename R>
 static int build_graph(Ctx& c, BatchWs& w, double gscale) {
-  if (w.gexec && w.graph_gscale == gscale) return DDA_OK;
+  if (w.gexec && w.graph_gscale == gscale && w.graph_pscale == w.pscale) return DDA_OK;
   if (w.gexec) { cudaGraphExecDestroy(w.gexec); w.gexec = nullptr; }
   // make sure lazily created resources exist before capture
   c.twiddles(w.g.Lx, sizeof(R) == 8); c.twiddles(w.g.Ly, sizeof(R) == 8); c.twiddles(w.g.Lz, sizeof(R) == 8);
+  if (w.pre) {
+    c.twiddles(w.gp.Lx, sizeof(R) == 8); c.twiddles(w.gp.Ly, sizeof(R) == 8); c.twiddles(w.gp.Lz, sizeof(R) == 8);
+  }
   cudaGraph_t graph = nullptr;
   long long nk = 0;
   cudaError_t e = capture_iteration<R>(c, w, gscale, c.stream, &graph, &nk);
@@ -309,7 +352,20 @@ static int build_graph(Ctx& c, BatchWs& w, double gscale) {
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) { set_error(std::string("graph instantiate: ") + cudaGetErrorString(e)); return DDA_ERR_CUDA; }
   w.graph_gscale = gscale;
+  w.graph_pscale = w.pscale;
   return DDA_OK;
+}
+
+// Preconditioned solves iterate on y with x = M y (Gpbicgstab.py:1171-1199):
+// M is applied in place to the iterate the store / accumulate step reads.
+template <typename R>
+static cudaError_t finish_pre(Ctx& c, BatchWs& w, cudaStream_t s) {
+  if (!w.pre) return cudaSuccess;
+  launch_pick_solution(w.d_st, w.nb, s, nullptr);
+  MvFuse f;
+  f.tensor = 1;
+  return launch_matvec<R>(c, w.gp, w.pcp, w.d_st, nullptr, w.nb, V_TMP, V_TMP, MV_CONV_MASKED, C_LIVE, w.pscale, s,
+                          f);
 }
 
 // Run iterations until every active instance is done.  Status is polled
@@ -359,16 +415,18 @@ static void fill_result(const InstState& S, dda_result& r) {
 
 template <typename R>
 int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, int nb, double target, int max_iter,
-                double ratio, dda_result* res, cudaStream_t user) {
+                double ratio, dda_result* res, cudaStream_t user, const PreSpec* pre) {
   int err = DDA_OK;
   const int dtype = sizeof(R) == 8 ? DDA_C128 : DDA_C64;
-  BatchWs* w = c.workspace(dtype, g, nb, true, &err);
+  BatchWs* w = c.workspace(dtype, g, nb, true, &err, 0, pre ? &pre->g : nullptr);
   if (!w) return err;
+  if (pre) w->pscale = pre->scale;
   InstState* H = w->h_st[0];
   const bool sites = compress_sites();
   for (int j = 0; j < nb; ++j) {
     w->base_state(j, H[j], sites);
     H[j].ghat = inst[j].ghat;
+    H[j].pghat = pre ? pre->phat[j] : nullptr;
     H[j].inva = inst[j].inv_alpha;
     H[j].vec[V_TMP] = (void*)inst[j].e_inc;
     H[j].out = inst[j].p_out;
@@ -388,6 +446,7 @@ int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, i
   DDA_CUDA_OK(cudaGetLastError());
   int rc = run_iterations<R>(c, *w, gscale, 4);
   if (rc) return rc;
+  DDA_CUDA_OK(finish_pre<R>(c, *w, s));
   launch_store_solution<R>(w->d_st, nb, (long long)w->n3, c.num_sms, s, nullptr);
   DDA_CUDA_OK(cudaGetLastError());
   for (int j = 0; j < nb; ++j)
@@ -397,19 +456,20 @@ int solve_batch(Ctx& c, const Geo& g, double gscale, const dda_instance* inst, i
   return DDA_OK;
 }
 template int solve_batch<float>(Ctx&, const Geo&, double, const dda_instance*, int, double, int, double, dda_result*,
-                                cudaStream_t);
+                                cudaStream_t, const PreSpec*);
 template int solve_batch<double>(Ctx&, const Geo&, double, const dda_instance*, int, double, int, double,
-                                 dda_result*, cudaStream_t);
+                                 dda_result*, cudaStream_t, const PreSpec*);
 
 // ---------------------------------------------------------------------------
 // mixed precision: complex64 sweeps inside FP64 iterative refinement
 // ---------------------------------------------------------------------------
 int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, const dda_instance* i128, int nb,
                 double tol, double inner_tol, int max_iter, int max_outer, double ratio, dda_result* res,
-                cudaStream_t user) {
+                cudaStream_t user, const PreSpec* pre) {
   int err = DDA_OK;
-  BatchWs* w64 = c.workspace(DDA_C64, g, nb, true, &err);
+  BatchWs* w64 = c.workspace(DDA_C64, g, nb, true, &err, 0, pre ? &pre->g : nullptr);
   if (!w64) return err;
+  if (pre) w64->pscale = pre->scale;
   BatchWs* w128 = c.workspace(DDA_C128, g, nb, false, &err);
   if (!w128) return err;
   cudaStream_t s = c.stream;
@@ -452,6 +512,7 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
     for (int j = 0; j < nb; ++j) {
       w64->base_state(j, H64[j], sites);
       H64[j].ghat = i64[j].ghat;
+      H64[j].pghat = pre ? pre->phat[j] : nullptr;
       H64[j].inva = i64[j].inv_alpha;
       // inner target: inner_tol, relaxed on later sweeps to what the FP64
       // target still needs (with a safety factor), never above 0.5
@@ -471,6 +532,7 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
     launch_init<float>(k, s);
     int rc = run_iterations<float>(c, *w64, gscale, 4);
     if (rc) return rc;
+    DDA_CUDA_OK(finish_pre<float>(c, *w64, s));
     for (int j = 0; j < nb; ++j) {
       if (!active[j]) continue;
       const InstState& S = w64->h_st[0][j];

@@ -60,6 +60,24 @@ __device__ __forceinline__ const float2* sol64(const InstState& S) {
   return nullptr;
 }
 
+// S.vec[V_TMP] := the iterate sol64 / k_store_solution read (the current one
+// when no solution exists: it is never stored then), so a preconditioned
+// solve can apply M to it in place before the store.
+__global__ void k_pick_solution(InstState* st, const int* act, int nb) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nb) return;
+  InstState& S = st[act ? act[j] : j];
+  if (!S.active) return;
+  void* e = S.vec[V_X];
+  if (S.status != ST_CONVERGED && S.best_x >= 0) e = S.vec[V_XA + S.best_x];
+  S.vec[V_TMP] = e;
+}
+
+void launch_pick_solution(InstState* st, int nb, cudaStream_t s, const int* act) {
+  k_pick_solution<<<(nb + 127) / 128, 128, 0, s>>>(st, act, nb);
+  note_launch(s, 1);
+}
+
 // x128 += solution(c64)
 __global__ void __launch_bounds__(KNT) k_accum(InstState* st128, int xid, const InstState* st64, const int* act,
                                                long long n3) {

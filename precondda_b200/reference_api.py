@@ -11,8 +11,8 @@ from __future__ import annotations
 import numpy as np
 import torch
 
-from .engine import (DDAOperator, as_device, _device, fft_lengths, green_octant, solve_many, cross_sections,
-                     SolveInfo)
+from .engine import (DDAOperator, Preconditioner, as_device, _device, fft_lengths, green_octant, solve_many,
+                     cross_sections, SolveInfo)
 
 _C64, _C128 = torch.complex64, torch.complex128
 
@@ -56,9 +56,15 @@ def expand_octant(oct_, Ls):
 def prepare_interaction_matrices(grid_size, k, refract_mult, x_expansion, y_expansion, z_expansion, alpha_array,
                                  lattice_spacing, reduced=True, is_2d=False, cutoff=False, double_precision=False):
     """(inv_alpha, mask, interaction_matrix, preconditioner) as in
-    ddaforgit.py:1085-1159.  The reference's preconditioner builders are not
-    part of it (they are imported from missing modules), so preconditioner is
-    None and solves run with precon=False."""
+    ddaforgit.py:1085-1159.  The reference's preconditioner builders
+    (pre_preconditioner / circulant_approximation, :1118-1136) are not part
+    of it; the preconditioner returned here is the engine's
+    (``engine.Preconditioner``: the inverse of the occupancy-weighted
+    circulant approximation of A) as a (L/2+1, L/2+1, L/2+1, 6) octant in the
+    reference's layout on the interaction grid L (2n where compiled, else the
+    next compiled length), the shape of the interaction octant.
+    ``refract_mult`` and the expansions size the reference's missing builder
+    and are accepted and ignored; is_2d returns None."""
     dt = _C128 if double_precision else _C64
     dev = _device()
     a = as_device(alpha_array, dt, dev)
@@ -69,7 +75,11 @@ def prepare_interaction_matrices(grid_size, k, refract_mult, x_expansion, y_expa
     mask = nz_
     nx, ny, nz = grid_size
     G = generate_interaction_row(nx, ny, nz, k, lattice_spacing, reduced=reduced, double_precision=double_precision)
-    return inv_alpha, mask, G, None
+    pre = None
+    if not is_2d and bool(mask.any()):
+        pre = Preconditioner(inv_alpha=inv_alpha.to(_C128), k=k, d=lattice_spacing,
+                             device=dev).reference_octant(dt)
+    return inv_alpha, mask, G, pre
 
 
 def _inv_alpha_box(alpha_inv, nx, ny, nz, dt, dev):
@@ -118,6 +128,27 @@ def fft_matvec(in_array, out_array, matrix, mask, chunk_params, nx, ny, nz, dtyp
     return op.conv_masked(in_array).reshape(-1)
 
 
+def _pre_from_reference(preconditioner, ia):
+    if isinstance(preconditioner, Preconditioner):
+        return preconditioner
+    if preconditioner is None:
+        raise ValueError("precon=True needs a preconditioner (prepare_interaction_matrices returns one)")
+    return Preconditioner(inv_alpha=ia, octant=preconditioner, device=ia.device)
+
+
+def fft_matvec3(in_array, out_array, preconditioner, mask, chunk_params, nx, ny, nz, precon, dtype=_C64):
+    """Preconditioner application M x = mask * IFFT[P FFT(pad x)] on the
+    octant's grid 2 (extent - 1), cropped (Gpbicgstab.py:633-668); the input
+    unchanged (flattened) when precon is False.  out_array and chunk_params
+    are accepted and ignored."""
+    if not precon:
+        return in_array.reshape(-1) if hasattr(in_array, "reshape") else np.ravel(in_array)
+    dev = _device()
+    m = as_device(mask, torch.bool, dev).reshape(nx, ny, nz)
+    ia = torch.where(m, torch.ones((), dtype=_C128, device=dev), torch.zeros((), dtype=_C128, device=dev))
+    return _pre_from_reference(preconditioner, ia).apply(in_array, dtype).reshape(-1)
+
+
 def E_field_solver(polarization, interaction_matrix, grid_size, dtype=_C64):
     """Excited field IFFT[FFT(-A) FFT(P)] on the lattice, (nx,ny,nz,3), no
     mask and no alpha term (ExcitedField.py:129-195).  Raises ValueError on a
@@ -141,17 +172,18 @@ def solve_gpbicgstab(grid_size, inv_alpha, interaction_matrix, preconditioner, E
     with the reference's codes: i+1 when converged, max_iter when not,
     -(i+1) on NaN or stagnation.  The reference computes in complex64; pass
     dtype=torch.complex128 for the FP64 solve it imports from a missing
-    module.  precon=True needs the reference's preconditioner builder, which
-    it does not ship; it raises NotImplementedError, as does is_2d."""
+    module.  precon=True runs the reference's right-preconditioned
+    recurrence with ``preconditioner`` (an octant in the reference's
+    (hx,hy,hz,6) layout read on the grid 2 (extent - 1), as fft_matvec3
+    reads it, or an ``engine.Preconditioner``); is_2d raises
+    NotImplementedError."""
     if is_2d:
         raise NotImplementedError("the 2D preconditioned path is not part of the engine")
-    if precon:
-        raise NotImplementedError("preconditioned solves need the reference's missing preconditioner builder; "
-                                  "call with precon=False")
     nx, ny, nz = grid_size
     op = _op_from_reference(interaction_matrix, inv_alpha, nx, ny, nz, dtype)
     _check_mask(mask, op.inv_alpha)
-    P, info = op.solve(E_inc, tol=target, max_iter=max_iter, ratio=ratio)
+    pre = _pre_from_reference(preconditioner, op.inv_alpha.to(_C128)) if precon else None
+    P, info = op.solve(E_inc, tol=target, max_iter=max_iter, ratio=ratio, preconditioner=pre)
     return info.iters, P, info.lowest_rel, info.first_rel
 
 

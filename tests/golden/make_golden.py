@@ -8,7 +8,8 @@ Run from the repository root in a checkout that has the reference:
 The reference (Toastlovesjam/preconDDA) is executed unchanged through
 ``oracle/ref_loader.py``: ``Gpbicgstab.solve_gpbicgstab``,
 ``Gpbicgstab.interaction_mult`` / ``inner_product`` /
-``calculate_zeta_eta_twostep``, ``ExcitedField.E_field_solver`` and, from
+``calculate_zeta_eta_twostep`` / ``fft_matvec3`` (with precon=True, given a
+preconditioner octant), ``ExcitedField.E_field_solver`` and, from
 ``ddaforgit.py``, ``calculate_alpha``, ``build_problem_from_shapes`` and
 ``generate_interaction_row``.  Its device kernels run as CPU builds of their
 CUDA-C source; everything else is its own Python.  The outputs are written to
@@ -117,6 +118,36 @@ def main(ref):
         put(f"{name}_lowfirst", np.array([float(low), float(first)]), "lowest/initial, first/initial")
         put(f"{name}_P", np.asarray(P), "solution P (nx,ny,nz,3) complex64")
         put(f"{name}_Efield", np.asarray(Ef), "E_field_solver(P)")
+
+    # ---- preconditioned path (precon=True): the reference's fft_matvec3 and
+    # solve_gpbicgstab given the engine's preconditioner octant (restated by
+    # the oracle's circulant_preconditioner; the reference's own builders are
+    # missing), on a grid just above the box (L = 12 >= n = 10; the engine
+    # compiles L = 12, not 10) and on the doubled grid (L = 2n)
+    from oracle import dda_oracle as O
+    k, d, alpha, E = probs["s10"]
+    n = alpha.shape[0]
+    ia_o = np.where(alpha != 0, 1.0 / np.where(alpha != 0, alpha, 1), 0)
+    for Lp in (12, 2 * n):
+        pre = O.circulant_preconditioner(ia_o, k, d, L=(Lp,) * 3).astype(np.complex64)
+        rng = np.random.default_rng(9)
+        x = (rng.standard_normal((n, n, n, 3)) + 1j * rng.standard_normal((n, n, n, 3))).astype(np.complex64)
+        with ref_loader.quiet():
+            a = cp.asarray(alpha, dtype=np.complex64)
+            inv_alpha = cp.where(a != 0, 1.0 / a, 0)
+            mask = a != 0
+            maskf = cp.asarray(mask, dtype=np.float32)[..., None]
+            chunks = G.setup_chunked_values(Lp // 2, Lp // 2, Lp // 2)
+            y = G.fft_matvec3(cp.asarray(x).ravel(), None, cp.asarray(pre), maskf, chunks, n, n, n, True)
+            it, P, low, first = G.solve_gpbicgstab((n, n, n), inv_alpha, fx["s10_G"], pre, E, mask, 100, 500,
+                                                   target=1e-5, precon=True)
+        tag = f"pre{Lp}"
+        put(f"{tag}_octant", pre, f"s10 preconditioner octant on the {Lp}^3 grid, complex64 (hx,hy,hz,6)")
+        put(f"{tag}_x", x, "seeded input of fft_matvec3")
+        put(f"{tag}_Mx", np.asarray(y).reshape(n, n, n, 3), "fft_matvec3(x, octant, precon=True)")
+        put(f"{tag}_iters", np.array(int(it)), "solve_gpbicgstab(s10, precon=True) iterations (ratio 100, 1e-5)")
+        put(f"{tag}_lowfirst", np.array([float(low), float(first)]), "lowest/initial, first/initial")
+        put(f"{tag}_P", np.asarray(P), "solution P = M p_current (nx,ny,nz,3) complex64")
 
     # ---- matvec and reductions on seeded vectors
     k, d, alpha, E = probs["s8"]

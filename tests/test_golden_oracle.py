@@ -80,3 +80,70 @@ def test_solver_matches_reference(fx, name):
     assert abs(low - lo) / lo < 5e-2          # complex64 recursion near the target
     Ef = O.E_field_solver(Pr.astype(np.complex128), G, alpha.shape)
     assert _rel(Ef, fx[f"{name}_Efield"]) < 1e-5
+
+
+@pytest.mark.parametrize("Lp", [12, 20])
+def test_preconditioned_path_matches_reference(fx, Lp):
+    """precon=True: the oracle's preconditioner application and
+    right-preconditioned GPBiCGSTAB against the reference's own fft_matvec3
+    and solve_gpbicgstab(precon=True), given the same preconditioner octant
+    (which the oracle's builder restates to complex64 rounding)."""
+    k, d = fx["s10_kd"]
+    alpha = fx["s10_alpha"]
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    pre = fx[f"pre{Lp}_octant"]
+    assert pre.shape == (Lp // 2 + 1,) * 3 + (6,)
+    built = O.circulant_preconditioner(ia, k, d, L=(Lp,) * 3)
+    assert _rel(built, pre) < 1e-6
+    Mx = O.precondition_apply(fx[f"pre{Lp}_x"], pre.astype(np.complex128), mask)
+    assert _rel(Mx, fx[f"pre{Lp}_Mx"]) < 1e-5
+    it, P, low, first = O.solve_gpbicgstab(alpha.shape, ia, G, fx["s10_E"], mask, 100, 500, target=1e-5,
+                                           preconditioner=pre.astype(np.complex128))
+    assert it == int(fx[f"pre{Lp}_iters"]) and it < int(fx["s10_iters"])
+    Pr = fx[f"pre{Lp}_P"]
+    assert np.linalg.norm(P - Pr) / np.linalg.norm(Pr) < 1e-4
+    assert abs(first - fx[f"pre{Lp}_lowfirst"][1]) / fx[f"pre{Lp}_lowfirst"][1] < 1e-4
+
+
+def test_occupancy_weights_of_a_full_box_are_chan_weights():
+    """For a filled box the weights are T. Chan's per-axis factors
+    prod (1 - |j_i|/n_i) of the optimal circulant of a Toeplitz matrix."""
+    shape = (4, 6, 5)
+    W = O.occupancy_weights(np.ones(shape, bool))
+    for j in [(0, 0, 0), (1, 2, 3), (-3, 5, -4), (2, -1, 0)]:
+        idx = tuple(jj % (2 * n) for jj, n in zip(j, shape))
+        want = np.prod([1 - abs(jj) / n for jj, n in zip(j, shape)])
+        assert abs(W[idx] - want) < 1e-12
+
+
+def test_precondition_apply_is_the_dense_circulant_inverse():
+    """M x with the engine's octant equals mask * inv(C) x for the dense
+    circulant C = abar I + sum_j w(j) G(j) shift_j on the L-periodic grid
+    (folded), the matrix the builder inverts."""
+    shape, L = (3, 4, 3), (4, 4, 4)
+    rng = np.random.default_rng(4)
+    k, d = 2 * np.pi / 0.5, 0.03
+    ia = np.where(rng.random(shape) < 0.7, 20.0 + 3.0j + rng.random(shape), 0)
+    pre = O.circulant_preconditioner(ia, k, d, L=L)
+    occ = ia != 0
+    abar = ia[occ].mean()
+    La = tuple(2 * n for n in shape)
+    Gw = O.green_embedded(*shape, k, d, La) * O.occupancy_weights(occ)[..., None]
+    npt = int(np.prod(L))
+    Cm = np.zeros((npt, 3, npt, 3), complex)
+    pts = [np.unravel_index(p, L) for p in range(npt)]
+    for p, P_ in enumerate(pts):
+        Cm[p, :, p, :] += abar * np.eye(3)
+        for q, Q_ in enumerate(pts):
+            t = tuple((a - b) % Ln for a, b, Ln in zip(P_, Q_, L))
+            for i_ in np.ndindex(*La):
+                off = [ii if ii < n else ii - Lan for ii, n, Lan in zip(i_, shape, La)]
+                if all(o % Ln == tt for o, Ln, tt in zip(off, L, t)) and any(o != 0 for o in off):
+                    g = Gw[i_]
+                    Cm[p, :, q, :] += np.array([[g[0], g[1], g[2]], [g[1], g[3], g[4]], [g[2], g[4], g[5]]])
+    Ci = np.linalg.inv(Cm.reshape(3 * npt, 3 * npt))
+    x = rng.standard_normal(shape + (3,)) + 1j * rng.standard_normal(shape + (3,))
+    xp = np.zeros(L + (3,), complex)
+    xp[:shape[0], :shape[1], :shape[2]] = x
+    y = (Ci @ xp.reshape(-1)).reshape(L + (3,))[:shape[0], :shape[1], :shape[2]] * occ[..., None]
+    assert _rel(O.precondition_apply(x, pre, occ), y) < 1e-10

@@ -190,7 +190,7 @@ def test_reference_api_solve_and_near_field():
     assert _rel(Ef, O.E_field_solver(P_ref, G_o, (n, n, n))) < 1e-8
     with pytest.raises(ValueError):
         P.E_field_solver(Pg.reshape(-1)[:-3], G, (n, n, n))
-    with pytest.raises(NotImplementedError):
+    with pytest.raises(ValueError):          # precon=True needs a preconditioner
         P.solve_gpbicgstab((n, n, n), ia, G, None, E, mask, 100, 10, precon=True)
 
 
