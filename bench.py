@@ -29,7 +29,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "DDA solves/s, p99 latency, matvec GB/s; mixed vs FP64 at C_ext err≤1e-4"
 WORKLOAD = "sphere64_precision: 64^3 box, 137376 dipoles, m=1.7+0.1i, |m|kd=0.5, lambda=0.5um, RR alpha, " \
-           "x+y polarisations along +z, c64 GPBiCGSTAB (tol 1e-4) in FP64 refinement to 1e-6"
+           "x+y polarisations along +z, c64 GPBiCGSTAB (tol 1e-4, right-preconditioned: precon=True) in FP64 " \
+           "refinement to 1e-6"
 N_BOX, M_REF, KD_M, WAVELENGTH = 64, 1.7 + 0.1j, 0.5, 0.5
 TOL, INNER_TOL, MAX_ITER, RATIO = 1e-6, 1e-4, 2000, 100.0
 # Iterations the reference's complex128 GPBiCGSTAB (ratio 100, tol 1e-6) takes
@@ -272,17 +273,32 @@ def run_ours(args, ws, rank, local):
     k, d, ia, Es, ndip = problem()
     op = P.DDAOperator(ia, k, d, dtype=torch.complex128, device=dev, with_twin=True)
     op64 = op.twin(torch.complex64)
+    # the reference's precon=True solve with the engine's circulant
+    # preconditioner on the operator's grid, built once per geometry like the
+    # Green octant (inside the e2e step below)
+    pre = op.preconditioner()
 
-    def step():
-        return P.solve_many([op, op], Es_dev, tol=TOL, max_iter=MAX_ITER, ratio=RATIO, precision="mixed",
-                            inner_tol=INNER_TOL)
+    def step(precision="mixed", preconditioner=pre, tol=TOL):
+        return P.solve_many([op, op], Es_dev, tol=tol, max_iter=MAX_ITER, ratio=RATIO, precision=precision,
+                            inner_tol=INNER_TOL, preconditioner=preconditioner)
+
+    def time_steps(n, **kw):
+        """(solves/s, infos) of n steps timed on the stream."""
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True); a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(n):
+            _, inf = step(**kw)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        return 2 * n / (a0.elapsed_time(a1) / 1e3), inf
 
     Es_dev = [torch.as_tensor(E, device=dev) for E in Es]
+    stream = torch.cuda.current_stream(dev)
     for _ in range(max(args.warmup, 1)):
         Ps, infos = step()
     torch.cuda.synchronize()
     # --- timed region: device-resident inputs -------------------------------
-    stream = torch.cuda.current_stream(dev)
     lc0 = L.lib().dda_kernel_launches()
     with ClockSampler(dev.index) as clk:
         barrier(ws)
@@ -320,8 +336,9 @@ def run_ours(args, ws, rank, local):
         ia_d = ia_h.to(dev, non_blocking=True)
         Ed = [E.to(dev, non_blocking=True) for E in Es_h]
         op_e = P.DDAOperator(ia_d, k, d, dtype=torch.complex128, L_=op.L, device=dev, with_twin=True)
+        pre_e = op_e.preconditioner()
         Pe, inf_e = P.solve_many([op_e, op_e], Ed, tol=TOL, max_iter=MAX_ITER, ratio=RATIO, precision="mixed",
-                                 inner_tol=INNER_TOL)
+                                 inner_tol=INNER_TOL, preconditioner=pre_e)
         xs = [op_e.cross_sections(Pe[j], Ed[j]) for j in range(2)]
         for j in range(2):
             P_h[j].copy_(Pe[j], non_blocking=True)
@@ -345,16 +362,15 @@ def run_ours(args, ws, rank, local):
                          "P_rel_err": float(torch.linalg.vector_norm(Ps[j] - Pf[j]) /
                                             torch.linalg.vector_norm(Pf[j])),
                          "C_ext": cm[0], "C_abs": cm[1], "C_sca": cm[2]})
-        # --- plain complex128 solve (denominator of the 3x target) ------------
-        torch.cuda.synchronize()
-        g0 = torch.cuda.Event(enable_timing=True); g1 = torch.cuda.Event(enable_timing=True)
-        g0.record(stream)
+        # --- plain complex128 solves (denominator of the 3x target) and the
+        # unpreconditioned solves (the reference's precon=False), same problem
         nplain = max(1, min(args.steps, 3))
-        for _ in range(nplain):
-            Pp, inf_p = P.solve_many([op, op], Es_dev, tol=TOL, max_iter=MAX_ITER, ratio=RATIO, precision="c128")
-        g1.record(stream)
-        torch.cuda.synchronize()
-        plain = 2 * nplain / (g0.elapsed_time(g1) / 1e3)
+        step(precision="c128")
+        plain, inf_p = time_steps(nplain, precision="c128")
+        step(preconditioner=None)
+        mixed_np, inf_mnp = time_steps(nplain, preconditioner=None)
+        step(precision="c128", preconditioner=None)
+        plain_np, inf_pnp = time_steps(nplain, precision="c128", preconditioner=None)
         # --- roofline of the matvec (complex64, the inner solve's) -----------
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)   # 256 MB > L2
         # the dominant kernel as the timed solve launches it: one complex64
@@ -383,6 +399,11 @@ def run_ours(args, ws, rank, local):
         del flush
         out = {"roofline": roof, "matvec_128": big, "plain_c128_solves_per_s": plain,
                "mixed_over_plain": value / ws / plain,
+               "unpreconditioned": {"mixed_solves_per_s": mixed_np, "plain_c128_solves_per_s": plain_np,
+                                    "mixed_over_plain": mixed_np / plain_np,
+                                    "mixed_inner_total": [i.iters for i in inf_mnp],
+                                    "plain_c128": [i.iters for i in inf_pnp],
+                                    "preconditioned_over_unpreconditioned": value / ws / mixed_np},
                "accuracy_vs_fp64": cerr,
                "iterations": {"mixed_inner_total": [i.iters for i in infos], "outer": [i.outer for i in infos],
                               "true_relres": [i.true_relres for i in infos],
@@ -395,11 +416,13 @@ def run_ours(args, ws, rank, local):
                 "data": "synthetic (seeded sphere lattice; no dataset)",
                 "config": {"workload": WORKLOAD, "global_batch": 2 * ws, "dipoles": ndip, "box": [N_BOX] * 3,
                            "fft": list(op.L), "parallelism": "replicas" if ws > 1 else "single",
+                           "preconditioner": f"precon=True: occupancy-weighted circulant on the {pre.L[0]}^3 grid "
+                                             "(complex64 sweeps; FP64 refinement residual unpreconditioned)",
                            "l2": "working set > L2 (c64 + c128 workspaces ~0.4 GB); roofline launches flush L2"},
                 "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "step_ms_p50": 1e3 * statistics.median(e2e_steps), "step_ms_max": 1e3 * max(e2e_steps),
-                        "includes": "H2D of inv_alpha and E_inc, Green build, mixed solve, cross sections, "
-                                    "D2H of P"},
+                        "includes": "H2D of inv_alpha and E_inc, Green build, preconditioner build, mixed solve, "
+                                    "cross sections, D2H of P"},
                 "gpu_launches": int(launches)}
         line.update(out)
         if ws == 1 and not args.no_cpu:
@@ -466,9 +489,21 @@ def run_large128(args, ws, rank, local):
     ia, k, d, Es = build_geometry(spec, dev)
     op = P.DDAOperator(ia, k, d, dtype=torch.complex128, device=dev, with_twin=True)
     E = Es[0]
+    pre = op.preconditioner()
 
-    def solve(prec, tol=TOL):
-        return P.solve_many([op], [E], tol=tol, max_iter=4000, ratio=RATIO, precision=prec, inner_tol=INNER_TOL)
+    def solve(prec, tol=TOL, preconditioner=pre):
+        return P.solve_many([op], [E], tol=tol, max_iter=4000, ratio=RATIO, precision=prec, inner_tol=INNER_TOL,
+                            preconditioner=preconditioner)
+
+    def timed(prec, preconditioner):
+        solve(prec, preconditioner=preconditioner)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True); a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        Px, ix = solve(prec, preconditioner=preconditioner)
+        a1.record(stream)
+        torch.cuda.synchronize()
+        return 1.0 / (a0.elapsed_time(a1) / 1e3), Px, ix
 
     for _ in range(max(args.warmup, 1)):
         solve("mixed")
@@ -488,13 +523,10 @@ def run_large128(args, ws, rank, local):
     value = args.steps * ws / t
     if rank != 0:
         return
-    g0 = torch.cuda.Event(enable_timing=True); g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    Pp, ip = solve("c128")
-    g1.record(stream)
-    torch.cuda.synchronize()
-    plain = 1.0 / (g0.elapsed_time(g1) / 1e3)
-    Pf, iff = solve("c128", tol=1e-10)
+    plain, Pp, ip = timed("c128", pre)
+    mixed_np, _, imn = timed("mixed", None)
+    plain_np, _, ipn = timed("c128", None)
+    Pf, iff = solve("c128", tol=1e-10, preconditioner=None)
     cm, cp, cf = (op.cross_sections(Pm[0], E), op.cross_sections(Pp[0], E), op.cross_sections(Pf[0], E))
     err = lambda a, b: abs(a - b) / abs(b)
     nocc = int((ia != 0).sum().item())
@@ -505,9 +537,14 @@ def run_large128(args, ws, rank, local):
     line = _line(METRIC, value, "solves/s", args, ws, t,
                  {"workload": f"large128: 128^3 box ({nocc} dipoles), ellipsoid semi-axes (64,48,40)d, seeded Euler "
                               f"angles, m={spec['m']:.4f}, |m|kd=0.6, mixed c64 (1e-4) + FP64 refinement to 1e-6",
-                  "box": [128] * 3, "fft": list(op.L), "parallelism": "replicas" if ws > 1 else "single"},
+                  "box": [128] * 3, "fft": list(op.L), "parallelism": "replicas" if ws > 1 else "single",
+                  "preconditioner": f"precon=True: occupancy-weighted circulant on the {pre.L[0]}^3 grid"},
                  gpu_launches=int(launches),
                  plain_c128_solves_per_s=plain, mixed_over_plain=value / ws / plain,
+                 unpreconditioned={"mixed_solves_per_s": mixed_np, "plain_c128_solves_per_s": plain_np,
+                                   "mixed_over_plain": mixed_np / plain_np, "mixed_inner": imn[0].iters,
+                                   "plain_c128": ipn[0].iters,
+                                   "preconditioned_over_unpreconditioned": value / ws / mixed_np},
                  iterations={"mixed_inner": im[0].iters, "outer": im[0].outer, "plain_c128": ip[0].iters,
                              "true_relres_mixed": im[0].true_relres},
                  accuracy_vs_fp64={"mixed": {"C_ext_rel_err": err(cm[0], cf[0]), "C_abs_rel_err": err(cm[1], cf[1])},
