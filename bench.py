@@ -591,7 +591,7 @@ def run_batch64(args, ws, rank, local):
             xs[(g, j)] = cross_sections(Pv.contiguous(), G.E_incs[j], G.inv_alpha, G.k)
 
         res = solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, tuner=tuner, device=dev,
-                               keep_results=False, on_result=on_result)
+                               keep_results=False, on_result=on_result, precondition=not args.no_precondition)
         torch.cuda.synchronize()
         t_all = time.perf_counter() - t_all
     launches = L.lib().dda_kernel_launches() - lc0
@@ -611,6 +611,8 @@ def run_batch64(args, ws, rank, local):
                               f"edge, m Re U[1.3,2], Im U[0,0.3], lambda U[0.4,0.8] um, |m|kd=0.5, 2 pols x 8 "
                               f"directions ({n} RHS), mixed c64 (1e-4) + FP64 refinement to 1e-5",
                   "global_batch": n * ws, "parallelism": "replicas" if ws > 1 else "single",
+                  "preconditioner": "none (precon=False)" if args.no_precondition else
+                                    "precon=True: occupancy-weighted circulant per geometry on its bucket's grid",
                   "buckets": buckets},
                  e2e={"value": n * ws / te, "unit": "solves/s", "h2d_bytes_per_step": 0,
                       "d2h_bytes_per_step": 3 * 8 * n,
@@ -635,7 +637,8 @@ def run_serve(args, ws, rank, local):
     from precondda_b200.workloads import serving_stream, build_geometry
     dev = torch.device("cuda", local)
     stream = serving_stream(50 + rank, rate=args.rate, duration=args.duration)
-    srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=8, device=dev)
+    srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=8, device=dev,
+                    precondition=not args.no_precondition)
     # warm the kernels of every bucket outside the timed region
     warm = sorted({srv.bucket_for(sp["box"]) for _, sp in stream})
     for b in warm:
@@ -681,7 +684,7 @@ def run_serve(args, ws, rank, local):
                 n_rhs = len(sp["dirs"]) * (len(sp["fixed_pols"]) if "fixed_pols" in sp else sp.get("pols", 2))
                 for j in range(n_rhs):
                     r = srv.submit(Request(inv_alpha=None, E_inc=None, k=k, d=d, tol=1e-5, shape=tuple(sp["box"]),
-                                           build=make(j)))
+                                           build=make(j), pre_key=("group", q)))
                     r.t_submit = t0 + arr
                     reqs.append(r)
                 groups[q] = (t0 + arr, reqs)
@@ -706,6 +709,8 @@ def run_serve(args, ws, rank, local):
                               f"boxes 16^3-128^3, m Re U[1.3,2] Im U[0,0.5], lambda U[0.4,0.8] um, 1-16 incidences, "
                               f"mixed precision to 1e-5, continuous batching",
                   "parallelism": "replicas" if ws > 1 else "single", "slots_per_bucket": args.slots,
+                  "preconditioner": "none (precon=False)" if args.no_precondition else
+                                    "precon=True: occupancy-weighted circulant per request group on its bucket's grid",
                   "pools": {str(k): v for k, v in st.get("pools", {}).items()}},
                  latency_ms={"request_p50": float(np.percentile(lat_req, 50) * 1e3),
                              "request_p99": float(np.percentile(lat_req, 99) * 1e3),
@@ -737,6 +742,8 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=16, help="serve: slots per size bucket")
+    ap.add_argument("--no-precondition", action="store_true",
+                    help="batch64 / serve: the reference's precon=False solve instead of the preconditioned one")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     if args.profile_matvec:

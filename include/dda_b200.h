@@ -252,6 +252,15 @@ int dda_slots_free_slot(const dda_slots* pool);
  * matter for mixed pools.  The result lands in p_out when the slot finishes. */
 int dda_slots_admit(dda_slots* pool, int slot, const dda_instance* lo, const dda_instance* hi, double tol,
                     double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
+/* Preconditioned pools (the precon=True solve of dda_solve_batch_pre for
+ * every slot): the preconditioner grid Px,Py,Pz and scale are the pool's;
+ * each admitted request brings its own octant `phat` (engine layout,
+ * complex64 for DDA_PREC_C64 / DDA_PREC_MIXED, complex128 for DDA_PREC_C128)
+ * through dda_slots_admit_pre. */
+int dda_slots_create_pre(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                         int Px, int Py, int Pz, double pscale, int nslots, dda_slots** out);
+int dda_slots_admit_pre(dda_slots* pool, int slot, const dda_instance* lo, const dda_instance* hi, const void* phat,
+                        double tol, double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
 /* Enqueue `niter` GPBiCGSTAB iterations of every occupied slot. */
 int dda_slots_run(dda_slots* pool, int niter);
 /* Wait for the pool's stream, then report the slots that finished since the

@@ -44,7 +44,7 @@ EXPORTS = (
     "dda_voxelize", "dda_incident_field", "dda_slots_create", "dda_slots_destroy", "dda_slots_capacity",
     "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
     "dda_far_field", "dda_matvec_batch", "dda_precond_build", "dda_precond_op_create", "dda_gpbicgstab_pre",
-    "dda_solve_batch_pre", "dda_solve_mixed_batch_pre",
+    "dda_solve_batch_pre", "dda_solve_mixed_batch_pre", "dda_slots_create_pre", "dda_slots_admit_pre",
 )
 
 
@@ -112,6 +112,9 @@ def _declare(lib):
     lib.dda_slots_run.argtypes = [vp, i]
     lib.dda_slots_poll.argtypes = [vp, C.POINTER(i), C.POINTER(dda_result), C.POINTER(i), C.POINTER(i)]
     lib.dda_slots_release.argtypes = [vp, i]
+    lib.dda_slots_create_pre.argtypes = [vp, i, i, i, i, i, i, i, d, i, i, i, d, i, C.POINTER(vp)]
+    lib.dda_slots_admit_pre.argtypes = [vp, i, C.POINTER(dda_instance), C.POINTER(dda_instance), vp, d, d, i, i,
+                                        d, vp]
     lib.dda_far_field.argtypes = [vp, i, i, i, i, d, d, vp, i, C.POINTER(d), C.POINTER(d), vp]
     lib.dda_matvec_batch.argtypes = [C.POINTER(vp), i, i, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp), vp]
     lib.dda_precond_build.argtypes = [vp, i, i, i, i, i, i, d, d, vp, i, vp, vp, vp]

@@ -30,7 +30,8 @@ import torch
 
 from . import _lib as L
 from .engine import _C64, _C128, _device, fft_lengths, green_octant_pair, compiled_fft_lengths
-from .serve import SlotPool, request_bytes, slot_bytes
+from .engine import Preconditioner
+from .serve import SlotPool, precond_bytes, request_bytes, slot_bytes
 
 DEFAULT_EDGES = (8, 12, 16, 20, 24, 32, 40, 48, 64, 72, 80, 96, 128, 144, 160, 192, 256)
 
@@ -159,24 +160,27 @@ def green_bytes(L_):
     return 6 * (L_[0] // 2 + 1) * (L_[1] // 2 + 1) * (L_[2] // 2 + 1) * (16 + 8)
 
 
-def item_bytes(box, L_, precision, nrhs, ngeom):
+def item_bytes(box, L_, precision, nrhs, ngeom, precondition=False):
     """Device bytes a bucket item holds while it runs: its slot pool, the
-    per-request tensors and padded copies, and one octant per geometry."""
+    per-request tensors and padded copies, and one octant per geometry (two
+    with a preconditioner)."""
     n = box[0] * box[1] * box[2]
-    per_rhs = slot_bytes(box, L_, precision) + request_bytes(box, precision) + 3 * n * 16 + n * 8
-    return nrhs * per_rhs + ngeom * (green_bytes(L_) + n * 16)
+    per_rhs = slot_bytes(box, L_, precision, precondition) + request_bytes(box, precision) + 3 * n * 16 + n * 8
+    return nrhs * per_rhs + ngeom * (green_bytes(L_) + n * 16 + (precond_bytes(L_, precision) if precondition else 0))
 
 
 def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_iter=2000, max_outer=12,
                      ratio=100.0, chunk=8, tuner=None, hbm_budget=None, device=None, keep_results=True,
-                     on_result=None):
+                     on_result=None, precondition=False):
     """Solve every right-hand side of every geometry.
 
     Buckets (geometries sharing a padded box and FFT lengths) become slot
     pools; pools are started while the HBM budget (default 75% of the free
     memory) allows, advanced round-robin on their own streams, and a new
-    bucket starts as soon as a running one finishes.  ``on_result(g, j, P,
-    info)`` is called for each finished right-hand side (P cropped to the
+    bucket starts as soon as a running one finishes.  ``precondition`` runs
+    the reference's precon=True solve with one engine preconditioner per
+    geometry (its padded lattice, the bucket's FFT grid).  ``on_result(g, j,
+    P, info)`` is called for each finished right-hand side (P cropped to the
     geometry's box); P is also kept in the result unless ``keep_results`` is
     False."""
     from collections import deque
@@ -199,7 +203,7 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
         for g in groups[key]:
             trial = acc + [g]
             if acc and item_bytes(box, L_, precision, sum(len(geoms[x].E_incs) for x in trial),
-                                  len(trial)) > hbm_budget:
+                                  len(trial), precondition) > hbm_budget:
                 items.append((key, acc))
                 acc = [g]
             else:
@@ -213,26 +217,29 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
     def start(key, gl):
         box, L_ = key
         nrhs = sum(len(geoms[g].E_incs) for g in gl)
-        pool = SlotPool(box, L_, nrhs, precision, 1.0, dev)
+        pool = SlotPool(box, L_, nrhs, precision, 1.0, dev, precond_L=L_ if precondition else None)
         where, slot = {}, 0
         try:
             for g in gl:
                 G = geoms[g]
                 g128, g64 = green_octant_pair(box, G.k, G.d, L_, 1.0 / (L_[0] * L_[1] * L_[2]), dev)
                 ia = _pad(G.inv_alpha.to(_C128), box)
+                pre = (Preconditioner(inv_alpha=ia, k=G.k, d=G.d, L_=L_, device=dev,
+                                      dtypes=(_C128,) if precision == "c128" else (_C64,))
+                       if precondition else None)
                 if precision == "c64":
                     ia = ia.to(_C64)
                 gh = (g64, g128) if precision == "mixed" else (g64 if precision == "c64" else g128)
                 for j, E in enumerate(G.E_incs):
                     Ep = _pad(E.to(_C64 if precision == "c64" else _C128), box, (3,))
                     pool.admit(slot, gh, ia, Ep, tol=tol, inner_tol=inner_tol, max_iter=max_iter,
-                               max_outer=max_outer, ratio=ratio)
+                               max_outer=max_outer, ratio=ratio, preconditioner=pre)
                     where[slot] = (g, j)
                     slot += 1
         except BaseException:
             pool.close()
             raise
-        return pool, where, item_bytes(box, L_, precision, nrhs, len(gl))
+        return pool, where, item_bytes(box, L_, precision, nrhs, len(gl), precondition)
 
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -240,7 +247,8 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
     while items or active:
         while items:
             key, gl = items[0]
-            est = item_bytes(key[0], key[1], precision, sum(len(geoms[g].E_incs) for g in gl), len(gl))
+            est = item_bytes(key[0], key[1], precision, sum(len(geoms[g].E_incs) for g in gl), len(gl),
+                             precondition)
             if active and used + est > hbm_budget:
                 break
             try:

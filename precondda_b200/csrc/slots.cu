@@ -43,6 +43,7 @@ struct dda_slots {
   int prec = DDA_PREC_C64;
   Geo g{};
   double gscale = 1.0;
+  bool pre = false;   // preconditioned slots (precon=True): octant per slot, grid p->w.gp
   int n = 0;
   BatchWs w;      // solver workspace (complex64 for C64 / MIXED, complex128 for C128)
   BatchWs w128;   // MIXED: FP64 right-hand side and residual per slot
@@ -69,12 +70,13 @@ static int put_state(dda_slots* p, BatchWs& w, int j, const InstState& S) {
 
 // (Re)initialise the complex64 / complex128 Krylov state of slot j from its
 // right-hand side (already in V_B for mixed pools, in V_TMP otherwise).
-static int arm_solver(dda_slots* p, int j, const void* ghat, const void* inva, const void* e_inc, double target,
-                      int max_iter, double ratio, bool from_tmp, void* out) {
+static int arm_solver(dda_slots* p, int j, const void* ghat, const void* pghat, const void* inva, const void* e_inc,
+                      double target, int max_iter, double ratio, bool from_tmp, void* out) {
   InstState S;
   p->w.base_state(j, S, compress_sites());
   S.out = out;
   S.ghat = ghat;
+  S.pghat = pghat;
   S.inva = inva;
   if (from_tmp) S.vec[V_TMP] = (void*)e_inc;
   S.target = target;
@@ -86,8 +88,31 @@ static int arm_solver(dda_slots* p, int j, const void* ghat, const void* inva, c
 
 extern "C" {
 
+static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                        const Geo* gp, double pscale, int nslots, dda_slots** out);
+
 int dda_slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
                      int nslots, dda_slots** out) {
+  return slots_create(ctx, precision, nx, ny, nz, Lx, Ly, Lz, gscale, nullptr, 1.0, nslots, out);
+}
+
+int dda_slots_create_pre(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                         int Px, int Py, int Pz, double pscale, int nslots, dda_slots** out) {
+  const int dt = precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64;
+  if (Px < nx || Py < ny || Pz < nz || !dda_fft_length_ok(Px, dt) || !dda_fft_length_ok(Py, dt) ||
+      !dda_fft_length_ok(Pz, dt)) {
+    set_error("slot pool: bad preconditioner grid");
+    return DDA_ERR_BAD_SHAPE;
+  }
+  Geo gp;
+  gp.nx = nx; gp.ny = ny; gp.nz = nz; gp.Lx = Px; gp.Ly = Py; gp.Lz = Pz;
+  gp.hx = Px / 2 + 1; gp.hy = Py / 2 + 1; gp.hz = Pz / 2 + 1;
+  gp.nsite = (long long)nx * ny * nz;
+  return slots_create(ctx, precision, nx, ny, nz, Lx, Ly, Lz, gscale, &gp, pscale, nslots, out);
+}
+
+static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx, int Ly, int Lz, double gscale,
+                        const Geo* gp, double pscale, int nslots, dda_slots** out) {
   if (!ctx || !out || nslots < 1) { set_error("bad slot-pool arguments"); return DDA_ERR_ARG; }
   if (precision < DDA_PREC_C64 || precision > DDA_PREC_MIXED) { set_error("bad precision"); return DDA_ERR_ARG; }
   *out = nullptr;
@@ -110,7 +135,9 @@ int dda_slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx
   p->gscale = gscale;
   p->n = nslots;
   p->info.resize(nslots);
-  int rc = p->w.alloc(ctx->c, precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64, g, nslots, true);
+  p->pre = gp != nullptr;
+  int rc = p->w.alloc(ctx->c, precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64, g, nslots, true, gp);
+  p->w.pscale = pscale;
   if (!rc && precision == DDA_PREC_MIXED) rc = p->w128.alloc(ctx->c, DDA_C128, g, nslots, false);
   if (!rc) {
     if (cudaMalloc((void**)&p->d_bnorm, nslots * sizeof(double)) != cudaSuccess ||
@@ -135,6 +162,7 @@ int dda_slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int Lx
   if (!rc) {
     const bool dbl = precision == DDA_PREC_C128;
     ctx->c.twiddles(Lx, dbl); ctx->c.twiddles(Ly, dbl); ctx->c.twiddles(Lz, dbl);
+    if (gp) { ctx->c.twiddles(gp->Lx, dbl); ctx->c.twiddles(gp->Ly, dbl); ctx->c.twiddles(gp->Lz, dbl); }
     if (precision == DDA_PREC_MIXED) { ctx->c.twiddles(Lx, true); ctx->c.twiddles(Ly, true); ctx->c.twiddles(Lz, true); }
     cudaGraph_t graph = nullptr;
     long long nk = 0;
@@ -181,8 +209,24 @@ int dda_slots_free_slot(const dda_slots* p) {
   return -1;
 }
 
+static int slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_instance* hi, const void* phat,
+                       double tol, double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
+
 int dda_slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_instance* hi, double tol,
                     double inner_tol, int max_iter, int max_outer, double ratio, void* stream) {
+  if (p && p->pre) { set_error("a preconditioned pool admits with dda_slots_admit_pre"); return DDA_ERR_ARG; }
+  return slots_admit(p, slot, lo, hi, nullptr, tol, inner_tol, max_iter, max_outer, ratio, stream);
+}
+
+int dda_slots_admit_pre(dda_slots* p, int slot, const dda_instance* lo, const dda_instance* hi, const void* phat,
+                        double tol, double inner_tol, int max_iter, int max_outer, double ratio, void* stream) {
+  if (!p || !p->pre) { set_error("dda_slots_admit_pre needs a pool made by dda_slots_create_pre"); return DDA_ERR_ARG; }
+  if (!phat) { set_error("null preconditioner octant"); return DDA_ERR_ARG; }
+  return slots_admit(p, slot, lo, hi, phat, tol, inner_tol, max_iter, max_outer, ratio, stream);
+}
+
+static int slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_instance* hi, const void* phat,
+                       double tol, double inner_tol, int max_iter, int max_outer, double ratio, void* stream) {
   if (!p || slot < 0 || slot >= p->n) { set_error("bad slot"); return DDA_ERR_ARG; }
   if (p->info[slot].state != 0) { set_error("slot is occupied"); return DDA_ERR_ARG; }
   const dda_instance* in = p->prec == DDA_PREC_C128 ? hi : lo;
@@ -206,7 +250,7 @@ int dda_slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_in
   Ctx& c = p->ctx->c;
   if (p->prec != DDA_PREC_MIXED) {
     I.p_out = in->p_out;
-    if ((rc = arm_solver(p, slot, in->ghat, in->inv_alpha, in->e_inc, tol, max_iter, ratio, true, in->p_out)))
+    if ((rc = arm_solver(p, slot, in->ghat, phat, in->inv_alpha, in->e_inc, tol, max_iter, ratio, true, in->p_out)))
       return rc;
     KrylovLaunch k{p->w.d_st, act, 1, p->w.red, p->w.cnt, (long long)p->w.n3, p->w.RB};
     const bool sites = compress_sites();
@@ -234,7 +278,8 @@ int dda_slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda_in
     launch_norm2<double>(p->w128.d_st, V_B, 1, (long long)p->w128.n3, p->w128.red, p->w128.cnt, p->w128.RB,
                          p->d_bnorm, p->s, act);
     cudaMemcpyAsync(H.vec[V_R], H.vec[V_B], bytes, cudaMemcpyDeviceToDevice, p->s);
-    if ((rc = arm_solver(p, slot, lo->ghat, lo->inv_alpha, nullptr, inner_tol, max_iter, ratio, false, nullptr)))
+    if ((rc = arm_solver(p, slot, lo->ghat, phat, lo->inv_alpha, nullptr, inner_tol, max_iter, ratio, false,
+                         nullptr)))
       return rc;
     if (compress_sites()) launch_site_map<float>(p->w.d_st, 1, p->g.nsite, p->w.bcount, p->s, act);
     launch_down(p->w.d_st, V_B, p->w128.d_st, V_R, 1, (long long)p->w.n3, c.num_sms, p->s, act);
@@ -284,10 +329,27 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
     ++*nfinished;
     I.state = 0;
   };
+  // preconditioned slots iterate on y with x = M y: M goes in place onto the
+  // iterate the store / accumulate below reads (Gpbicgstab.py:1171-1199)
+  auto apply_pre = [&](int m, const int* act) -> cudaError_t {
+    if (!p->pre) return cudaSuccess;
+    launch_pick_solution(p->w.d_st, m, p->s, act);
+    MvFuse f;
+    f.tensor = 1;
+    if (p->prec == DDA_PREC_C128)
+      return launch_matvec<double>(c, p->w.gp, p->w.pcp, p->w.d_st, act, m, V_TMP, V_TMP, MV_CONV_MASKED, C_LIVE,
+                                   p->w.pscale, p->s, f);
+    return launch_matvec<float>(c, p->w.gp, p->w.pcp, p->w.d_st, act, m, V_TMP, V_TMP, MV_CONV_MASKED, C_LIVE,
+                                p->w.pscale, p->s, f);
+  };
   if (p->prec != DDA_PREC_MIXED) {
     if (!done.empty()) {
       int rc = set_act(p, 0, done);
       if (rc) return rc;
+      if ((e = apply_pre((int)done.size(), p->d_act)) != cudaSuccess) {
+        set_error(cudaGetErrorString(e));
+        return DDA_ERR_CUDA;
+      }
       if (p->prec == DDA_PREC_C128)
         launch_store_solution<double>(p->w.d_st, (int)done.size(), (long long)p->w.n3, c.num_sms, p->s, p->d_act);
       else
@@ -308,6 +370,7 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
     int rc = set_act(p, 0, done);
     if (rc) return rc;
     const int* act = p->d_act;
+    if ((e = apply_pre(m, act)) != cudaSuccess) { set_error(cudaGetErrorString(e)); return DDA_ERR_CUDA; }
     launch_accum(p->w128.d_st, V_X, p->w.d_st, m, (long long)p->w.n3, c.num_sms, p->s, act);
     e = launch_matvec<double>(c, p->g, p->w128.pc, p->w128.d_st, act, m, V_X, V_R, MV_RESIDUAL, C_ACTIVE,
                               p->gscale, p->s);
@@ -339,7 +402,8 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
         SlotInfo& I = p->info[j];
         const InstState& S = p->w.h_st[1][j];
         const double tj = std::max(I.inner_tol, std::min(0.5, 0.3 * I.tol / I.relres));
-        if ((rc = arm_solver(p, j, S.ghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false, nullptr))) return rc;
+        if ((rc = arm_solver(p, j, S.ghat, S.pghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false, nullptr)))
+          return rc;
       }
       if ((rc = set_act(p, 1, rearm))) return rc;
       const int* act2 = p->d_act + p->n;

@@ -164,7 +164,8 @@ class Preconditioner:
     2 (extent - 1) per axis, as fft_matvec3 reads it).
     """
 
-    def __init__(self, op=None, L_=None, *, inv_alpha=None, k=None, d=None, octant=None, device=None):
+    def __init__(self, op=None, L_=None, *, inv_alpha=None, k=None, d=None, octant=None, device=None,
+                 dtypes=(_C128, _C64)):
         if op is not None:
             dev = op.device
             ia = op.twin(_C128).inv_alpha if op.dtype != _C128 else op.inv_alpha
@@ -194,19 +195,25 @@ class Preconditioner:
             if L_ is None:
                 L_ = op.L if op is not None else fft_lengths(self.shape, _C128)
             self.L = tuple(int(v) for v in L_)
+            # the octant in the precisions asked for (both from one FP64 build)
             h = tuple(v // 2 + 1 for v in self.L)
-            e128 = torch.empty((6,) + h, dtype=_C128, device=dev)
-            e64 = torch.empty((6,) + h, dtype=_C64, device=dev)
+            e128 = torch.empty((6,) + h, dtype=_C128, device=dev) if _C128 in dtypes else None
+            e64 = torch.empty((6,) + h, dtype=_C64, device=dev) if _C64 in dtypes else None
+            if e128 is None and e64 is None:
+                raise ValueError("dtypes must contain complex64 and/or complex128")
             with torch.cuda.device(dev):
                 L.check(L.lib().dda_precond_build(self._ctx.handle, *self.shape, *self.L, float(k), float(d),
-                                                  ia.data_ptr(), L.GHAT_ENGINE, e128.data_ptr(), e64.data_ptr(),
+                                                  ia.data_ptr(), L.GHAT_ENGINE,
+                                                  e128.data_ptr() if e128 is not None else None,
+                                                  e64.data_ptr() if e64 is not None else None,
                                                   stream_handle(dev)))
-            self._eng = {_C128: e128, _C64: e64}
+            self._eng = {t: e for t, e in ((_C128, e128), (_C64, e64)) if e is not None}
         self.scale = 1.0 / (self.L[0] * self.L[1] * self.L[2])
         self._ops = {}
 
     def octant(self, dtype=_C128) -> torch.Tensor:
-        """Engine-layout (6,hx,hy,hz) octant in ``dtype``."""
+        """Engine-layout (6,hx,hy,hz) octant in ``dtype`` (converted from the
+        other precision when only that one was built)."""
         if dtype not in self._eng:
             src = self._eng[_C128] if _C128 in self._eng else next(iter(self._eng.values()))
             self._eng[dtype] = src.to(dtype)

@@ -35,34 +35,44 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .engine import (SolveInfo, _device, _info, as_device, fft_lengths, green_octant_pair, stream_handle,
-                     _C64, _C128)
+from .engine import (SolveInfo, Preconditioner, _device, _info, as_device, fft_lengths, green_octant_pair,
+                     stream_handle, _C64, _C128)
 
 PRECISIONS = {"c64": L.DDA_PREC_C64, "c128": L.DDA_PREC_C128, "mixed": L.DDA_PREC_MIXED}
 DEFAULT_BUCKETS = (8, 12, 16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256)
 
 
-def slot_bytes(box, L_, precision) -> int:
-    """Device bytes one pool slot holds: 16 Krylov vectors and the two FFT
-    scratch volumes in the solver dtype, plus the FP64 right-hand side and
-    residual of a mixed slot."""
+def slot_bytes(box, L_, precision, precondition=False) -> int:
+    """Device bytes one pool slot holds: 16 Krylov vectors (17 with the
+    preconditioned vector) and the two FFT scratch volumes in the solver
+    dtype, plus the FP64 right-hand side and residual of a mixed slot.  A
+    preconditioner on the pool's FFT grid shares the scratch."""
     nx, ny, nz = box
     Lx, Ly, Lz = L_
     n3 = nx * ny * nz * 3
     esz = 16 if precision == "c128" else 8
-    b = (16 * n3 + nx * ny * Lz * 3 + nx * Ly * Lz * 3) * esz
+    b = ((17 if precondition else 16) * n3 + nx * ny * Lz * 3 + nx * Ly * Lz * 3) * esz
     if precision == "mixed":
         b += 2 * n3 * 16
     return b
 
 
-def request_bytes(box, precision) -> int:
-    """Per-request tensors: inv_alpha and E_inc / P in the solve precisions."""
+def precond_bytes(L_, precision="mixed") -> int:
+    """One preconditioner octant in the precision a pool of ``precision``
+    reads (complex64 for mixed and c64 pools)."""
+    return 6 * (L_[0] // 2 + 1) * (L_[1] // 2 + 1) * (L_[2] // 2 + 1) * (16 if precision == "c128" else 8)
+
+
+def request_bytes(box, precision, L_=None) -> int:
+    """Per-request tensors: inv_alpha and E_inc / P in the solve precisions,
+    plus the request's preconditioner octant (the solve precision) when L_
+    (its grid) is given."""
     n = box[0] * box[1] * box[2]
+    extra = precond_bytes(L_, precision) if L_ is not None else 0
     if precision == "mixed":
-        return n * (8 + 16) + n * 3 * 16 * 2
+        return n * (8 + 16) + n * 3 * 16 * 2 + extra
     esz = 16 if precision == "c128" else 8
-    return n * esz + n * 3 * esz * 2
+    return n * esz + n * 3 * esz * 2 + extra
 
 
 def choose_bucket(shape, buckets=DEFAULT_BUCKETS) -> int:
@@ -74,26 +84,36 @@ def choose_bucket(shape, buckets=DEFAULT_BUCKETS) -> int:
     raise ValueError(f"lattice {tuple(shape)} exceeds the largest bucket {max(buckets)}")
 
 
-def pool_slots(box, L_, precision, budget_bytes, cap) -> int:
+def pool_slots(box, L_, precision, budget_bytes, cap, precondition=False) -> int:
     """Slots a pool may have under ``budget_bytes`` (HBM admission)."""
-    per = slot_bytes(box, L_, precision) + request_bytes(box, precision)
+    per = slot_bytes(box, L_, precision, precondition) + request_bytes(box, precision,
+                                                                       L_ if precondition else None)
     return int(max(0, min(int(cap), int(budget_bytes) // per)))
 
 
 class SlotPool:
-    """``dda_slots_*`` pool: ``nslots`` solver instances of one box / FFT size."""
+    """``dda_slots_*`` pool: ``nslots`` solver instances of one box / FFT size.
+    ``precond_L``: make a preconditioned pool (the precon=True solve) whose
+    requests bring a ``Preconditioner`` on that grid."""
 
-    def __init__(self, box, L_, nslots, precision="mixed", gscale=1.0, device=None):
+    def __init__(self, box, L_, nslots, precision="mixed", gscale=1.0, device=None, precond_L=None):
         self.device = _device(device)
         self.box = tuple(int(v) for v in box)
         self.L = tuple(int(v) for v in L_)
         self.precision = precision
         self.nslots = int(nslots)
+        self.precond_L = tuple(int(v) for v in precond_L) if precond_L is not None else None
         self._ctx = L.context(self.device.index)
         h = C.c_void_p()
         with torch.cuda.device(self.device):
-            L.check(L.lib().dda_slots_create(self._ctx.handle, PRECISIONS[precision], *self.box, *self.L,
-                                             float(gscale), self.nslots, C.byref(h)))
+            if self.precond_L is None:
+                L.check(L.lib().dda_slots_create(self._ctx.handle, PRECISIONS[precision], *self.box, *self.L,
+                                                 float(gscale), self.nslots, C.byref(h)))
+            else:
+                P_ = self.precond_L
+                L.check(L.lib().dda_slots_create_pre(self._ctx.handle, PRECISIONS[precision], *self.box, *self.L,
+                                                     float(gscale), *P_, 1.0 / (P_[0] * P_[1] * P_[2]),
+                                                     self.nslots, C.byref(h)))
         self._h = h
         self._fin = (C.c_int * self.nslots)()
         self._res = (L.dda_result * self.nslots)()
@@ -115,11 +135,17 @@ class SlotPool:
         return L.lib().dda_slots_free_slot(self._h)
 
     def admit(self, slot, ghat, inv_alpha, E_inc, tol=1e-5, inner_tol=1e-4, max_iter=2000, max_outer=12,
-              ratio=100.0):
+              ratio=100.0, preconditioner=None):
         """Start a solve in ``slot``.  ``ghat``: engine-layout octant, a
         (complex64, complex128) pair for mixed pools; inv_alpha / E_inc on the
-        device in the pool's precision (complex128 for mixed pools).  Returns
-        the output tensor, valid once the slot is reported finished."""
+        device in the pool's precision (complex128 for mixed pools);
+        ``preconditioner`` (a ``Preconditioner`` on the pool's grid) for
+        preconditioned pools.  Returns the output tensor, valid once the slot
+        is reported finished."""
+        if (self.precond_L is None) != (preconditioner is None):
+            raise ValueError("a preconditioned pool needs a preconditioner per request, a plain one none")
+        if preconditioner is not None and (preconditioner.L != self.precond_L or preconditioner.shape != self.box):
+            raise ValueError("preconditioner grid / box differs from the pool's")
         lo, hi = L.dda_instance(), L.dda_instance()
         dev = self.device
         if self.precision == "mixed":
@@ -141,9 +167,16 @@ class SlotPool:
             inst.ghat, inst.inv_alpha, inst.e_inc, inst.p_out = g.data_ptr(), ia.data_ptr(), E.data_ptr(), P.data_ptr()
             keep = (g, ia, E, P)
         with torch.cuda.device(dev):
-            L.check(L.lib().dda_slots_admit(self._h, int(slot), C.byref(lo), C.byref(hi), float(tol),
-                                            float(inner_tol), int(max_iter), int(max_outer), float(ratio),
-                                            stream_handle(dev)))
+            if preconditioner is None:
+                L.check(L.lib().dda_slots_admit(self._h, int(slot), C.byref(lo), C.byref(hi), float(tol),
+                                                float(inner_tol), int(max_iter), int(max_outer), float(ratio),
+                                                stream_handle(dev)))
+            else:
+                ph = preconditioner.octant(_C128 if self.precision == "c128" else _C64)
+                keep = (preconditioner, ph) + keep
+                L.check(L.lib().dda_slots_admit_pre(self._h, int(slot), C.byref(lo), C.byref(hi), ph.data_ptr(),
+                                                    float(tol), float(inner_tol), int(max_iter), int(max_outer),
+                                                    float(ratio), stream_handle(dev)))
         self._keep[int(slot)] = keep
         return P
 
@@ -228,6 +261,7 @@ class Request:
     bucket: int = 0
     shape: tuple = ()
     build: object = None
+    pre_key: object = None     # requests with one key share one preconditioner (same lattice, k, d)
 
 
 @dataclass
@@ -243,16 +277,21 @@ class DDAServer:
     """Continuous-batching server (one GPU, one pool per cubic size bucket).
 
     precision: 'mixed' (complex64 sweeps + FP64 refinement, the default),
-    'c64' or 'c128'.  hbm_budget: bytes the pools may hold (default: 60% of
-    the free device memory at construction; the rest is left to Green builds,
+    'c64' or 'c128'.  precondition: run every request as the reference's
+    precon=True solve, with the engine's circulant preconditioner of its
+    padded lattice on the bucket's FFT grid (built when the request is
+    admitted).  hbm_budget: bytes the pools may hold (default: 60% of the
+    free device memory at construction; the rest is left to Green builds,
     the Green cache and the requests' arrays)."""
 
     def __init__(self, precision="mixed", buckets=DEFAULT_BUCKETS, slots_per_bucket=16, chunk_iters=8,
-                 hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None):
+                 hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None,
+                 precondition=False):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.device = _device(device)
         self.precision = precision
+        self.precondition = bool(precondition)
         self.buckets = tuple(sorted(int(b) for b in buckets))
         self.slots_per_bucket = int(slots_per_bucket)
         self.chunk = int(chunk_iters)
@@ -266,6 +305,7 @@ class DDAServer:
         self._b: dict[int, _Bucket] = {}
         self._next = 0
         self.done: list[Request] = []
+        self._pre: dict = {}       # pre_key -> [Preconditioner or None, requests not yet finished]
 
     # -- buckets ------------------------------------------------------------
     def bucket_for(self, shape) -> int:
@@ -276,13 +316,14 @@ class DDAServer:
             return self._b[n]
         box = (n, n, n)
         L_ = fft_lengths(box, _C64 if self.precision == "c64" else _C128)
-        per = slot_bytes(box, L_, self.precision) + request_bytes(box, self.precision)
+        pre = self.precondition
+        per = slot_bytes(box, L_, self.precision, pre) + request_bytes(box, self.precision, L_ if pre else None)
         room = self.hbm_budget - self.hbm_used
-        ns = pool_slots(box, L_, self.precision, room, self.slots_per_bucket)
+        ns = pool_slots(box, L_, self.precision, room, self.slots_per_bucket, pre)
         if ns < 1:
             raise MemoryError(f"bucket {n}^3 needs {per / 2**20:.0f} MiB per slot; "
                               f"{room / 2**20:.0f} MiB of the HBM budget is left")
-        pool = SlotPool(box, L_, ns, self.precision, 1.0, self.device)
+        pool = SlotPool(box, L_, ns, self.precision, 1.0, self.device, precond_L=L_ if pre else None)
         self.hbm_used += ns * per
         b = _Bucket(n, L_, pool)
         self._b[n] = b
@@ -305,8 +346,28 @@ class DDAServer:
         req.rid = self._next
         self._next += 1
         req.t_submit = time.perf_counter()
+        if self.precondition and req.pre_key is not None:
+            self._pre.setdefault(req.pre_key, [None, 0])[1] += 1
         self._bucket(req.bucket).queue.append(req)
         return req
+
+    def _preconditioner(self, req, ia, L_):
+        """The request's preconditioner (shared by requests with one pre_key)."""
+        dts = (_C128,) if self.precision == "c128" else (_C64,)
+        if req.pre_key is None:
+            return Preconditioner(inv_alpha=ia, k=req.k, d=req.d, L_=L_, device=self.device, dtypes=dts)
+        ent = self._pre[req.pre_key]
+        if ent[0] is None:
+            ent[0] = Preconditioner(inv_alpha=ia, k=req.k, d=req.d, L_=L_, device=self.device, dtypes=dts)
+        return ent[0]
+
+    def _release_pre(self, req):
+        if self.precondition and req.pre_key is not None:
+            ent = self._pre.get(req.pre_key)
+            if ent is not None:
+                ent[1] -= 1
+                if ent[1] <= 0:
+                    del self._pre[req.pre_key]
 
     def _pad(self, req, n):
         dt = _C64 if self.precision == "c64" else _C128
@@ -332,8 +393,9 @@ class DDAServer:
             g64, g128 = self.green.get((b.n,) * 3, b.L, req.k, req.d)
             ghat = (g64, g128) if self.precision == "mixed" else (g64 if self.precision == "c64" else g128)
             ia, E = self._pad(req, b.n)
+            pre = self._preconditioner(req, ia, b.L) if self.precondition else None
             b.pool.admit(s, ghat, ia, E, tol=req.tol, inner_tol=self.inner_tol, max_iter=req.max_iter,
-                         max_outer=self.max_outer, ratio=self.ratio)
+                         max_outer=self.max_outer, ratio=self.ratio, preconditioner=pre)
             b.active[s] = req
 
     def pending(self) -> int:
@@ -355,6 +417,7 @@ class DDAServer:
                 nx, ny, nz = req.shape
                 req.P = P[:nx, :ny, :nz] if P.shape[:3] != req.shape else P
                 req.info = info
+                self._release_pre(req)
                 out.append(req)
         self.done.extend(out)
         return out

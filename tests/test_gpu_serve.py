@@ -201,3 +201,62 @@ def test_slot_pool_argument_errors():
     pool.close()
     with pytest.raises(Exception):
         SlotPool((n, n, n), (14, 16, 16), 1, "c128")       # FFT length < 2n
+
+
+def test_preconditioned_pool_matches_batched_solve():
+    """A preconditioned slot runs the same precon=True solve as the batched
+    solver: same iterations and solution."""
+    import precondda_b200 as P
+    from precondda_b200.serve import SlotPool
+    n, m = 12, 2.2 + 0.1j
+    k, d, alpha, E = _sphere(n, m)
+    ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    pre = op.preconditioner()
+    Pb, ib = op.solve(E, tol=1e-7, max_iter=500, preconditioner=pre)
+    pool = SlotPool((n, n, n), op.L, 2, "c128", precond_L=op.L)
+    with pytest.raises(ValueError):
+        pool.admit(0, op.ghat, op.inv_alpha, torch.tensor(E, device="cuda"), tol=1e-7)       # no preconditioner
+    Pd = pool.admit(0, op.ghat, op.inv_alpha, torch.tensor(E, device="cuda"), tol=1e-7, max_iter=500,
+                    preconditioner=pre)
+    res = _run_pool(pool)
+    info, Pout = res[0]
+    assert Pout.data_ptr() == Pd.data_ptr()
+    assert info.status == "converged" and info.iters == ib.iters
+    assert np.abs((Pout - Pb).cpu().numpy()).max() / np.abs(Pb.cpu().numpy()).max() < 1e-10
+    pool.close()
+    plain = SlotPool((n, n, n), op.L, 1, "c128")
+    with pytest.raises(ValueError):
+        plain.admit(0, op.ghat, op.inv_alpha, torch.tensor(E, device="cuda"), preconditioner=pre)
+    plain.close()
+
+
+@pytest.mark.parametrize("precision", ["mixed", "c64"])
+def test_preconditioned_server_same_alone_and_in_the_mix(precision):
+    import precondda_b200 as P
+    from precondda_b200.serve import DDAServer
+    cfg = dict(precision=precision, buckets=(16,), slots_per_bucket=3, chunk_iters=3, precondition=True)
+    srv = DDAServer(**cfg)
+    alone = srv.submit(_requests(P, SPECS[:1])[0])
+    srv.drain()
+    P_alone, info_alone = alone.P.cpu().numpy().copy(), alone.info
+    srv.close()
+    srv = DDAServer(**cfg)
+    reqs = _requests(P, SPECS)
+    for r in reqs[1:3]:
+        srv.submit(r)
+    srv.step()
+    tgt = srv.submit(reqs[0])
+    for r in reqs[3:]:
+        srv.submit(r)
+    srv.drain()
+    assert tgt.info.iters == info_alone.iters and np.array_equal(tgt.P.cpu().numpy(), P_alone)
+    if precision == "mixed":
+        assert all(r.info.status == "converged" and r.info.true_relres <= r.tol for r in reqs)
+    srv.close()
+    # fewer iterations than the unpreconditioned server on the same request
+    srv = DDAServer(**dict(cfg, precondition=False))
+    r0 = srv.submit(_requests(P, SPECS[:1])[0])
+    srv.drain()
+    assert info_alone.iters < r0.info.iters
+    srv.close()
