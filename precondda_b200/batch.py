@@ -243,26 +243,27 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
 
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    active, used = [], 0
-    while items or active:
+    active, fresh, used = [], [], 0
+    while items or active or fresh:
         while items:
             key, gl = items[0]
             est = item_bytes(key[0], key[1], precision, sum(len(geoms[g].E_incs) for g in gl), len(gl),
                              precondition)
-            if active and used + est > hbm_budget:
+            if (active or fresh) and used + est > hbm_budget:
                 break
             try:
                 entry = start(key, gl)
             except (MemoryError, torch.cuda.OutOfMemoryError):
-                if not active:
+                if not (active or fresh):
                     raise
                 torch.cuda.empty_cache()
                 break
             items.popleft()
-            active.append(entry)
+            entry[0].run(chunk)             # a new pool starts iterating at once
+            fresh.append(entry)
             used += entry[2]
-        for pool, _, _ in active:
-            pool.run(chunk)
+        # each pool is polled (waiting for its own last chunk only) and given
+        # its next chunk right away, so no pool waits for the slowest one
         still = []
         for pool, where, est in active:
             for s, info, P in pool.poll():
@@ -275,13 +276,13 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
                 if keep_results:
                     Ps[g][j] = Pc
             if pool.running:
+                pool.run(chunk)
                 still.append((pool, where, est))
             else:
                 pool.close()
                 used -= est
-        if len(still) < len(active):
-            torch.cuda.empty_cache()
-        active = still
+        active = still + fresh
+        fresh = []
     torch.cuda.synchronize(dev)
     secs = time.perf_counter() - t0
     n = sum(len(g.E_incs) for g in geoms)

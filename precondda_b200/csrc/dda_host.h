@@ -84,6 +84,10 @@ struct Ctx {
   ~Ctx();
 };
 
+// Recycled pinned host blocks (cudaFreeHost would synchronise the device).
+void* pinned_get(size_t bytes);
+void pinned_put(void* p, size_t bytes);
+
 // Launch geometry of the five matvec passes for one (Geo, dtype).
 struct PassCfg {
   int nl = 1, th1 = 0;           // z passes: lines per CTA, threads
@@ -133,7 +137,13 @@ struct BatchWs {
   cudaGraphExec_t gexec = nullptr;
   double graph_gscale = 0.0;
   long long graph_kernels = 0;
+  // set before alloc: device buffers come from the stream-ordered pool on
+  // this stream and are freed on it (no device-wide synchronisation)
+  cudaStream_t astream = nullptr;
+  size_t pin_bytes = 0, pin_out = 0;
   int alloc(Ctx& c, int dtype, const Geo& g, int nb, bool full, const Geo* gp = nullptr);
+  // frees everything (idempotent; the destructor calls it)
+  void release();
   // vector slots the workspace allocates, in storage order
   const int* slots() const;
   // state of instance j: vector slots and scratch; with `sites` the

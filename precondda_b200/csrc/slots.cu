@@ -136,15 +136,24 @@ static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int
   p->n = nslots;
   p->info.resize(nslots);
   p->pre = gp != nullptr;
-  int rc = p->w.alloc(ctx->c, precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64, g, nslots, true, gp);
+  // the pool's memory is ordered on its own stream: creating and destroying
+  // pools does not synchronise the device (other pools keep running)
+  int rc = DDA_OK;
+  if (cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("slot pool: stream creation failed");
+    rc = DDA_ERR_CUDA;
+  }
+  p->w.astream = p->s;
+  p->w128.astream = p->s;
+  if (!rc) rc = p->w.alloc(ctx->c, precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64, g, nslots, true, gp);
   p->w.pscale = pscale;
   if (!rc && precision == DDA_PREC_MIXED) rc = p->w128.alloc(ctx->c, DDA_C128, g, nslots, false);
   if (!rc) {
-    if (cudaMalloc((void**)&p->d_bnorm, nslots * sizeof(double)) != cudaSuccess ||
-        cudaMalloc((void**)&p->d_act, 2 * nslots * sizeof(int)) != cudaSuccess ||
-        cudaMallocHost((void**)&p->h_norm, 2 * nslots * sizeof(double)) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&p->s, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&p->ev, cudaEventDisableTiming) != cudaSuccess) {
+    p->h_norm = (double*)pinned_get(2 * nslots * sizeof(double));
+    if (cudaMallocAsync((void**)&p->d_bnorm, nslots * sizeof(double), p->s) != cudaSuccess ||
+        cudaMallocAsync((void**)&p->d_act, 2 * nslots * sizeof(int), p->s) != cudaSuccess || !p->h_norm) {
       cudaGetLastError();
       set_error("slot pool: out of device memory");
       rc = DDA_ERR_OOM;
@@ -154,7 +163,9 @@ static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int
     // inactive slots: all kernels of the graph skip them
     std::vector<InstState> H(nslots);
     for (int j = 0; j < nslots; ++j) p->w.base_state(j, H[j]);
-    if (cudaMemcpy(p->w.d_st, H.data(), nslots * sizeof(InstState), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (cudaMemcpyAsync(p->w.d_st, H.data(), nslots * sizeof(InstState), cudaMemcpyHostToDevice, p->s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(p->s) != cudaSuccess) {
       set_error("slot pool: state upload failed");
       rc = DDA_ERR_CUDA;
     }
@@ -191,13 +202,20 @@ static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int
 void dda_slots_destroy(dda_slots* p) {
   if (!p) return;
   cudaSetDevice(p->ctx->c.device);
+  // the pool's own work completes first (its pinned blocks are then free to
+  // reuse); device memory returns to the stream-ordered pool on its stream
   if (p->s) cudaStreamSynchronize(p->s);
-  cudaFree(p->d_bnorm);
-  cudaFree(p->d_act);
-  cudaFreeHost(p->h_norm);
+  p->w.release();
+  p->w128.release();
+  if (p->s) {
+    if (p->d_bnorm) cudaFreeAsync(p->d_bnorm, p->s);
+    if (p->d_act) cudaFreeAsync(p->d_act, p->s);
+  }
+  pinned_put(p->h_norm, 2 * p->n * sizeof(double));
   if (p->ev) cudaEventDestroy(p->ev);
   if (p->s) cudaStreamDestroy(p->s);
-  delete p;    // BatchWs members free their device memory
+  cudaGetLastError();
+  delete p;
 }
 
 int dda_slots_capacity(const dda_slots* p) { return p ? p->n : 0; }

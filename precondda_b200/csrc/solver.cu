@@ -2,6 +2,8 @@
 // batched GPBiCGSTAB driver (graph-captured iterations, pipelined status
 // polling) and the mixed-precision iterative-refinement driver.
 #include <algorithm>
+#include <map>
+#include <mutex>
 #include <atomic>
 #include <cmath>
 #include <vector>
@@ -72,12 +74,62 @@ static const int kLightSlots[] = {V_R, V_B};
 
 const int* BatchWs::slots() const { return full ? (pre ? kPreSlots : kFullSlots) : kLightSlots; }
 
-BatchWs::~BatchWs() {
-  if (gexec) cudaGraphExecDestroy(gexec);
-  cudaFree(vecs); cudaFree(scratch); cudaFree(d_st); cudaFreeHost(h_st[0]); cudaFreeHost(h_st[1]);
-  cudaFree(red); cudaFree(cnt); cudaFree(d_out); cudaFreeHost(h_out);
-  cudaFree(cidx); cudaFree(bcount);
+// Pinned host blocks are recycled by size instead of returned to the
+// driver: cudaFreeHost synchronises the whole device, which would stall every
+// other stream each time a short-lived workspace (a slot pool) goes away.
+namespace {
+std::mutex g_pin_mu;
+std::multimap<size_t, void*> g_pin_free;
+}  // namespace
+
+void* pinned_get(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    auto it = g_pin_free.find(bytes);
+    if (it != g_pin_free.end()) {
+      void* p = it->second;
+      g_pin_free.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
 }
+
+void pinned_put(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pin_free.emplace(bytes, p);
+}
+
+// Device buffers come from the stream-ordered pool when the workspace has a
+// stream of its own (slot pools): freeing them then orders after that
+// stream's work instead of synchronising the device.
+static cudaError_t ws_malloc(void** p, size_t bytes, cudaStream_t as) {
+  return as ? cudaMallocAsync(p, bytes, as) : cudaMalloc(p, bytes);
+}
+static void ws_free(void* p, cudaStream_t as) {
+  if (!p) return;
+  if (as) cudaFreeAsync(p, as);
+  else cudaFree(p);
+}
+
+void BatchWs::release() {
+  if (gexec) { cudaGraphExecDestroy(gexec); gexec = nullptr; }
+  ws_free(vecs, astream); ws_free(scratch, astream); ws_free(d_st, astream);
+  ws_free(red, astream); ws_free(cnt, astream); ws_free(d_out, astream);
+  ws_free(cidx, astream); ws_free(bcount, astream);
+  vecs = scratch = nullptr; d_st = nullptr; red = nullptr; cnt = nullptr; d_out = nullptr;
+  cidx = nullptr; bcount = nullptr;
+  pinned_put(h_st[0], pin_bytes); pinned_put(h_st[1], pin_bytes); pinned_put(h_out, pin_out);
+  h_st[0] = h_st[1] = nullptr; h_out = nullptr;
+}
+
+BatchWs::~BatchWs() { release(); }
 
 int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_, const Geo* gp_) {
   dtype = dtype_; g = g_; nb = nb_; full = full_;
@@ -97,22 +149,27 @@ int BatchWs::alloc(Ctx& c, int dtype_, const Geo& g_, int nb_, bool full_, const
     t1n = std::max(t1n, (size_t)gp.nx * gp.ny * gp.Lz * 3);
     t2n = std::max(t2n, (size_t)gp.nx * gp.Ly * gp.Lz * 3);
   }
-  if (cudaMalloc(&vecs, (size_t)nb * nslot * n3 * esz) != cudaSuccess ||
-      cudaMalloc(&scratch, (size_t)nb * (t1n + t2n) * esz) != cudaSuccess ||
-      cudaMalloc((void**)&d_st, nb * sizeof(InstState)) != cudaSuccess ||
-      cudaMallocHost((void**)&h_st[0], nb * sizeof(InstState)) != cudaSuccess ||
-      cudaMallocHost((void**)&h_st[1], nb * sizeof(InstState)) != cudaSuccess ||
-      cudaMalloc((void**)&red, (size_t)nb * std::max<long long>(RB, pc.grid1) * KRED * sizeof(double)) != cudaSuccess ||
-      cudaMalloc((void**)&cnt, nb * sizeof(unsigned)) != cudaSuccess ||
-      cudaMalloc((void**)&d_out, nb * sizeof(double)) != cudaSuccess ||
-      cudaMallocHost((void**)&h_out, nb * sizeof(double)) != cudaSuccess ||
-      (full && (cudaMalloc((void**)&cidx, (size_t)nb * g.nsite * sizeof(int)) != cudaSuccess ||
-                cudaMalloc((void**)&bcount, (size_t)nb * site_blocks(g.nsite) * sizeof(int)) != cudaSuccess))) {
+  pin_bytes = (size_t)nb * sizeof(InstState);
+  pin_out = (size_t)nb * sizeof(double);
+  cudaStream_t as = astream;
+  h_st[0] = (InstState*)pinned_get(pin_bytes);
+  h_st[1] = (InstState*)pinned_get(pin_bytes);
+  h_out = (double*)pinned_get(pin_out);
+  if (ws_malloc(&vecs, (size_t)nb * nslot * n3 * esz, as) != cudaSuccess ||
+      ws_malloc(&scratch, (size_t)nb * (t1n + t2n) * esz, as) != cudaSuccess ||
+      ws_malloc((void**)&d_st, nb * sizeof(InstState), as) != cudaSuccess || !h_st[0] || !h_st[1] || !h_out ||
+      ws_malloc((void**)&red, (size_t)nb * std::max<long long>(RB, pc.grid1) * KRED * sizeof(double), as) !=
+          cudaSuccess ||
+      ws_malloc((void**)&cnt, nb * sizeof(unsigned), as) != cudaSuccess ||
+      ws_malloc((void**)&d_out, nb * sizeof(double), as) != cudaSuccess ||
+      (full && (ws_malloc((void**)&cidx, (size_t)nb * g.nsite * sizeof(int), as) != cudaSuccess ||
+                ws_malloc((void**)&bcount, (size_t)nb * site_blocks(g.nsite) * sizeof(int), as) != cudaSuccess))) {
     cudaGetLastError();
     set_error("solver workspace: out of device memory");
     return DDA_ERR_OOM;
   }
-  cudaMemset(cnt, 0, nb * sizeof(unsigned));
+  if (as) cudaMemsetAsync(cnt, 0, nb * sizeof(unsigned), as);
+  else cudaMemset(cnt, 0, nb * sizeof(unsigned));
   std::memset(h_st[0], 0, nb * sizeof(InstState));
   return DDA_OK;
 }

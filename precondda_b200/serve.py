@@ -271,6 +271,7 @@ class _Bucket:
     pool: SlotPool
     queue: deque = field(default_factory=deque)
     active: dict = field(default_factory=dict)    # slot -> Request
+    outstanding: bool = False                     # a chunk of iterations is enqueued and not yet polled
 
 
 class DDAServer:
@@ -402,23 +403,26 @@ class DDAServer:
         return sum(len(b.queue) + len(b.active) for b in self._b.values())
 
     def step(self) -> list:
-        """Admit waiting requests, advance every busy pool by ``chunk_iters``
-        iterations, collect finished requests.  Returns those requests."""
-        for b in self._b.values():
-            self._fill(b)
-        busy = [b for b in self._b.values() if b.active]
-        for b in busy:
-            b.pool.run(self.chunk)
+        """For every bucket: collect the requests its last chunk finished
+        (waiting for that pool only), admit waiting requests into the freed
+        slots and enqueue the next ``chunk_iters`` iterations at once, so a
+        pool never waits for the others.  Returns the finished requests."""
         out = []
-        for b in busy:
-            for s, info, P in b.pool.poll():
-                req = b.active.pop(s)
-                req.t_done = time.perf_counter()
-                nx, ny, nz = req.shape
-                req.P = P[:nx, :ny, :nz] if P.shape[:3] != req.shape else P
-                req.info = info
-                self._release_pre(req)
-                out.append(req)
+        for b in self._b.values():
+            if b.outstanding:
+                for s, info, P in b.pool.poll():
+                    req = b.active.pop(s)
+                    req.t_done = time.perf_counter()
+                    nx, ny, nz = req.shape
+                    req.P = P[:nx, :ny, :nz] if P.shape[:3] != req.shape else P
+                    req.info = info
+                    self._release_pre(req)
+                    out.append(req)
+                b.outstanding = False
+            self._fill(b)
+            if b.active:
+                b.pool.run(self.chunk)
+                b.outstanding = True
         self.done.extend(out)
         return out
 
