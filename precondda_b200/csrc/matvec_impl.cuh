@@ -68,12 +68,31 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 // is pruned), and only the kept half of each inverse output is formed.
 // NC = 0 reads the sizes from Geo.
 
+// Occupancy floors (CTAs per SM) of the cubic complex64 z and y passes.
+// Passes 1 and 5 of power-of-two lengths >= 128 at three CTAs of 384 threads
+// (<= 56 registers, a few bytes of spill; pass 5 otherwise takes 76 and fits
+// two): B200, 128^3 matvec 0.570 -> 0.538 ms, 64^3 unchanged.  Mixed-radix
+// lengths (E up to 24 per thread) would spill a kilobyte and keep the
+// compiler's choice.  DDA_Z_MINB / DDA_Y_MINB override (DDA_Y_MINB unset: the
+// compiler picks the y passes' registers; 4 measured slower).
+#ifndef DDA_Z_MINB
+#define DDA_Z_MINB 3
+#endif
+#define DDA_ZLB(R, NC)                                                                                           \
+  __launch_bounds__(kMvMaxThreads,                                                                              \
+                    ((NC) >= 64 && sizeof(R) == 4 && ((2 * (NC)) & (2 * (NC) - 1)) == 0) ? DDA_Z_MINB : 1)
+#ifdef DDA_Y_MINB
+#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads, ((NC) > 0 && sizeof(R) == 4) ? DDA_Y_MINB : 1)
+#else
+#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads)
+#endif
+
 // ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
 // thread = (c fastest, t, line)
 // ---------------------------------------------------------------------------
 template <typename R, int LZ, int NC>
-__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void DDA_ZLB(R, NC) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int cond,
                                                             int nl_, int pre) {
   grid_dep_begin();
@@ -146,7 +165,7 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass1(Geo g, const typenam
 // INV=true: T2 -> T1 keeping rows y < ny.
 // ---------------------------------------------------------------------------
 template <typename R, bool INV, int LY, int NC>
-__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void DDA_YLB(R, NC) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                              InstState* st, const int* act, int cond, int tz_,
                                                              int ntz_) {
   grid_dep_begin();
@@ -315,14 +334,18 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
 
 // variant with one component per thread and the tensor product through
 // shared memory: thread = (w fastest, t)
-// Cubic complex64 kernels of power-of-two length (E <= 16 per thread) fit
-// three CTAs of 384 threads per SM without spills worth the occupancy.
-#ifndef DDA_P3_MINB
-#define DDA_P3_MINB 3
-#endif
+// Cubic complex64 kernels of power-of-two length (E <= 16 per thread): three
+// CTAs of 384 threads per SM (56 registers), except L = 128 (64^3 boxes),
+// where two CTAs without spills measured faster (B200, two-RHS 64^3 matvec
+// 0.1362 -> 0.1321 ms; at L = 256 two CTAs were slower).  DDA_P3_MINB
+// overrides all lengths.
 template <typename R, int LX, int NC>
 constexpr int p3_min_blocks() {
+#ifdef DDA_P3_MINB
   return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? DDA_P3_MINB : 1;
+#else
+  return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? (LX == 128 ? 2 : 3) : 1;
+#endif
 }
 template <typename R, int LX, int V, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_mv_pass3s(Geo g, const typename CT<R>::T* __restrict__ tw,
@@ -440,7 +463,7 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
 // ---------------------------------------------------------------------------
 template <typename R, int LZ, int NC>
-__global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void DDA_ZLB(R, NC) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int out_id,
                                                             int mode, int cond, int nl_, int post, double* red,
                                                             unsigned* cnt) {
