@@ -78,9 +78,17 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 #ifndef DDA_Z_MINB
 #define DDA_Z_MINB 3
 #endif
-#define DDA_ZLB(R, NC)                                                                                           \
-  __launch_bounds__(kMvMaxThreads,                                                                              \
-                    ((NC) >= 64 && sizeof(R) == 4 && ((2 * (NC)) & (2 * (NC) - 1)) == 0) ? DDA_Z_MINB : 1)
+#ifndef DDA_Z1_MINB
+#define DDA_Z1_MINB DDA_Z_MINB
+#endif
+#define DDA_ZLB_N(R, NC, N)                                                                                      \
+  __launch_bounds__(kMvMaxThreads, ((NC) >= 64 && sizeof(R) == 4 && ((2 * (NC)) & (2 * (NC) - 1)) == 0) ? (N) : 1)
+#define DDA_ZLB(R, NC) DDA_ZLB_N(R, NC, DDA_Z_MINB)
+#if DDA_Z1_MINB == 0
+#define DDA_ZLB1(R, NC) __launch_bounds__(kMvMaxThreads)
+#else
+#define DDA_ZLB1(R, NC) DDA_ZLB_N(R, NC, DDA_Z1_MINB)
+#endif
 #ifdef DDA_Y_MINB
 #define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads, ((NC) > 0 && sizeof(R) == 4) ? DDA_Y_MINB : 1)
 #else
@@ -92,7 +100,7 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 // thread = (c fastest, t, line)
 // ---------------------------------------------------------------------------
 template <typename R, int LZ, int NC>
-__global__ void DDA_ZLB(R, NC) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void DDA_ZLB1(R, NC) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                             InstState* st, const int* act, int in_id, int cond,
                                                             int nl_, int pre) {
   grid_dep_begin();
