@@ -215,7 +215,9 @@ def run_reference(args, ws, rank):
             "config": {"workload": WORKLOAD, "global_batch": 2, "parallelism": "replicas"},
             "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
                              "sample": f"oracle complex128 GPBiCGSTAB iterations at 64^3 (FFT 128^3), one iteration "
-                                       f"per step, scaled by {iters} iterations per solve plus one Green build"},
+                                       f"per step, scaled by {iters} iterations per solve plus one Green build; the "
+                                       f"reference's runnable path, precon=False (its preconditioner builder is "
+                                       f"missing)"},
             "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -431,7 +433,8 @@ def run_ours(args, ws, rank, local):
             v = 1.0 / (t_green + t_it * iters)
             line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"one oracle complex128 GPBiCGSTAB iteration + one Green build at "
-                                              f"64^3, scaled to {iters} iterations per solve"}
+                                              f"64^3, scaled to {iters} iterations per solve (the reference's "
+                                              f"runnable path, precon=False)"}
         line["clocks"] = clk.summary()
         print(json.dumps(line), flush=True)
 
