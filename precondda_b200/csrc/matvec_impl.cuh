@@ -226,27 +226,6 @@ __global__ void DDA_YLB(R, NC) k_mv_pass_y(Geo g, const typename CT<R>::T* __res
 // Ghat is stored structure-of-arrays inside the engine: component c of octant
 // point (mx,my,mz) at gh[c*H + (mx*hy + my)*hz + mz], H = hx*hy*hz, so the
 // lanes of a warp (consecutive kz) read consecutive addresses.
-template <class C, typename R>
-__device__ __forceinline__ void tensor3(const C* __restrict__ gh, const Geo& g, int LX, int kx, int my, bool fy,
-                                        int kz, R gscale, C& a, C& b, C& c) {
-  const bool fx = kx > LX / 2, fz = kz > g.Lz / 2;
-  const int mx = fx ? LX - kx : kx;
-  const int mz = fz ? g.Lz - kz : kz;
-  const long long H = (long long)g.hx * g.hy * g.hz;
-  const C* q = gh + ((long long)mx * g.hy + my) * g.hz + mz;
-  C gxx = __ldg(q), gxy = __ldg(q + H), gxz = __ldg(q + 2 * H), gyy = __ldg(q + 3 * H), gyz = __ldg(q + 4 * H),
-    gzz = __ldg(q + 5 * H);
-  const R sxy = (fx != fy) ? -gscale : gscale;
-  const R sxz = (fx != fz) ? -gscale : gscale;
-  const R syz = (fy != fz) ? -gscale : gscale;
-  gxx = cscale(gxx, gscale); gyy = cscale(gyy, gscale); gzz = cscale(gzz, gscale);
-  gxy = cscale(gxy, sxy); gxz = cscale(gxz, sxz); gyz = cscale(gyz, syz);
-  const C a0 = a, b0 = b, c0 = c;
-  a = cadd(cadd(cmul(gxx, a0), cmul(gxy, b0)), cmul(gxz, c0));
-  b = cadd(cadd(cmul(gxy, a0), cmul(gyy, b0)), cmul(gyz, c0));
-  c = cadd(cadd(cmul(gxz, a0), cmul(gyz, b0)), cmul(gzz, c0));
-}
-
 __device__ __forceinline__ int pencil_ky(int p, int Ly) {
   if (p == 0) return 0;
   const int pr = (p + 1) >> 1;

@@ -136,6 +136,17 @@ def test_serve_buckets_and_hbm_admission():
     assert pool_slots(box, L, "mixed", 10 * per + per // 2, 64) == 10
     assert pool_slots(box, L, "mixed", 10 * per, 4) == 4
     assert pool_slots(box, L, "mixed", per - 1, 4) == 0
+    # preconditioned pools: one more vector per slot, the request's octant in
+    # the precision the pool reads
+    from precondda_b200.serve import precond_bytes
+    assert slot_bytes(box, L, "mixed", True) == slot_bytes(box, L, "mixed") + n3 * 8
+    assert slot_bytes(box, L, "c128", True) == slot_bytes(box, L, "c128") + n3 * 16
+    assert precond_bytes(L, "mixed") == 6 * 65 ** 3 * 8 and precond_bytes(L, "c128") == 6 * 65 ** 3 * 16
+    assert request_bytes(box, "mixed", L) == request_bytes(box, "mixed") + precond_bytes(L, "mixed")
+    perp = slot_bytes(box, L, "mixed", True) + request_bytes(box, "mixed", L)
+    assert pool_slots(box, L, "mixed", 3 * perp, 64, precondition=True) == 3
+    from precondda_b200.batch import item_bytes
+    assert item_bytes(box, L, "mixed", 4, 1, True) > item_bytes(box, L, "mixed", 4, 1)
 
 
 def test_workload_generators_are_seeded_and_valid():

@@ -166,3 +166,41 @@ def test_run_solver_default_precon_and_errors():
         P.solve_gpbicgstab((n, n, n), ia, G, None, E, mask, 100, 10, precon=True)
     with pytest.raises(NotImplementedError):
         P.solve_gpbicgstab((n, n, n), ia, G, pre, E, mask, 100, 10, precon=True, is_2d=True)
+
+
+def test_precond_edge_cases_and_errors():
+    """Zero right-hand side, an empty lattice and bad C-ABI arguments."""
+    import ctypes as C
+    import precondda_b200 as P
+    from precondda_b200 import _lib as L
+    n, m = 8, 2.0 + 0.1j
+    k, d, ia, E = _sphere(n, m)
+    op = P.DDAOperator(ia, k, d, dtype=C128)
+    pre = op.preconditioner()
+    Pz, iz = op.solve(np.zeros_like(E), tol=1e-6, max_iter=50, preconditioner=pre)
+    assert float(Pz.abs().max()) == 0.0
+    # a batch where one instance has no right-hand side: the other is unaffected
+    Pb, ib = P.solve_many([op, op], [E, np.zeros_like(E)], tol=1e-6, max_iter=200, preconditioner=pre)
+    Ps, is_ = op.solve(E, tol=1e-6, max_iter=200, preconditioner=pre)
+    assert ib[0].iters == is_.iters and float(Pb[1].abs().max()) == 0.0
+    # an empty lattice: prepare_interaction_matrices returns no preconditioner
+    alpha0 = np.zeros((n, n, n), np.complex128)
+    _, _, _, pre0 = P.prepare_interaction_matrices((n, n, n), k, None, 0, 0, 0, alpha0, d)
+    assert pre0 is None
+    # C ABI argument checks
+    ctx = L.context(0)
+    lib = L.lib()
+    out = torch.empty((6, 9, 9, 9), dtype=C128, device="cuda")
+    iac = torch.as_tensor(ia, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    assert lib.dda_precond_build(ctx.handle, n, n, n, 6, 16, 16, k, d, iac.data_ptr(), L.GHAT_ENGINE,
+                                 out.data_ptr(), None, s) == L.DDA_ERR_BAD_SHAPE          # grid < box
+    assert lib.dda_precond_build(ctx.handle, n, n, n, 16, 16, 16, k, d, None, L.GHAT_ENGINE,
+                                 out.data_ptr(), None, s) == L.DDA_ERR_ARG                # no inv_alpha
+    assert lib.dda_precond_build(ctx.handle, n, n, n, 16, 16, 16, k, d, iac.data_ptr(), 7,
+                                 out.data_ptr(), None, s) == L.DDA_ERR_ARG                # bad layout
+    h = C.c_void_p()
+    assert lib.dda_precond_op_create(ctx.handle, L.DDA_C128, n, n, n, 14, 16, 16, out.data_ptr(), 1.0,
+                                      iac.data_ptr(), C.byref(h)) == L.DDA_ERR_BAD_SHAPE  # 14: not compiled
+    with pytest.raises(ValueError):
+        P.Preconditioner(inv_alpha=ia, k=k, d=d, L_=(4, 16, 16))                          # grid < box
