@@ -219,40 +219,45 @@ void Ctx::trim() {
 // ---------------------------------------------------------------------------
 // DDA_FUSE_KRYLOV=1 lets the Krylov steps alpha (<rhat, v>), s / y and
 // zeta / eta ride on the two matvecs (dot products in the last pass, s and y
-// formed in the first) instead of three separate kernels.  Measured on B200
-// it is no faster (64^3 x 16 RHS: equal; 128^3: 7 % slower), so the separate
-// kernels are the default.
+// formed in the first -- M's first pass in a preconditioned solve) instead of
+// three separate kernels.  Measured on B200 it is no faster (64^3 x 16 RHS:
+// equal; 128^3: 7 % slower; preconditioned 64^3 x 2 RHS: mixed equal, c128
+// 2 % slower), so the separate kernels are the default.
 static bool fuse_krylov() {
   const char* e = getenv("DDA_FUSE_KRYLOV");
   return e && *e == '1';
 }
 
 // out = A in, or A M in for a preconditioned workspace (M in goes to V_MH):
-// Gpbicgstab.py:1008-1015, :1026-1033 and the residuals :1061-1064, :1143-1144
+// Gpbicgstab.py:1008-1015, :1026-1033 and the residuals :1061-1064, :1143-1144.
+// fz carries the fused Krylov steps: `pre` goes to the first product (M when
+// preconditioned, so s and y are formed by M's first pass), `post` to A.
 template <typename R>
-static cudaError_t amul(Ctx& c, BatchWs& w, int in, int out, int mode, int cond, double gscale, cudaStream_t s) {
+static cudaError_t amul(Ctx& c, BatchWs& w, int in, int out, int mode, int cond, double gscale, cudaStream_t s,
+                        const MvFuse& fz = MvFuse()) {
+  MvFuse fa = fz;
   if (w.pre) {
-    MvFuse f;
-    f.tensor = 1;
+    MvFuse fm;
+    fm.tensor = 1;
+    fm.pre = fz.pre;
     cudaError_t e = launch_matvec<R>(c, w.gp, w.pcp, w.d_st, nullptr, w.nb, in, V_MH, MV_CONV_MASKED, cond, w.pscale,
-                                     s, f);
+                                     s, fm);
     if (e != cudaSuccess) return e;
     in = V_MH;
+    fa.pre = MV_PRE_NONE;
   }
-  return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, in, out, mode, cond, gscale, s);
+  return launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, in, out, mode, cond, gscale, s, fa);
 }
 
 template <typename R>
 static cudaError_t enqueue_front(Ctx& c, BatchWs& w, double gscale, cudaStream_t s, const KrylovLaunch& k) {
   cudaError_t e;
-  if (fuse_krylov() && !w.pre) {
+  if (fuse_krylov()) {
     MvFuse f1, f2;
     f1.post = MV_POST_ALPHA; f1.red = w.red; f1.cnt = w.cnt;
     f2.pre = MV_PRE_SY; f2.post = MV_POST_ZETA; f2.red = w.red; f2.cnt = w.cnt;
-    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_P, V_V, MV_AX, C_ACTIVE, gscale, s, f1)))
-      return e;
-    if ((e = launch_matvec<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, V_S, V_T, MV_AX, C_ACTIVE, gscale, s, f2)))
-      return e;
+    if ((e = amul<R>(c, w, V_P, V_V, MV_AX, C_ACTIVE, gscale, s, f1))) return e;
+    if ((e = amul<R>(c, w, V_S, V_T, MV_AX, C_ACTIVE, gscale, s, f2))) return e;
   } else {
     if ((e = amul<R>(c, w, V_P, V_V, MV_AX, C_ACTIVE, gscale, s))) return e;
     launch_alpha<R>(k, s);
