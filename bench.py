@@ -333,12 +333,20 @@ def run_ours(args, ws, rank, local):
     f0.record(stream)
     xs = None
     e2e_steps = []
+    copy_stream = torch.cuda.Stream(dev)
     for _ in range(args.steps):
         ts0 = time.perf_counter()
         ia_d = ia_h.to(dev, non_blocking=True)
-        Ed = [E.to(dev, non_blocking=True) for E in Es_h]
+        # the incident fields cross on a second stream while the Green and
+        # preconditioner builds (which need only inv_alpha) run
+        copy_stream.wait_stream(stream)
+        with torch.cuda.stream(copy_stream):
+            Ed = [E.to(dev, non_blocking=True) for E in Es_h]
         op_e = P.DDAOperator(ia_d, k, d, dtype=torch.complex128, L_=op.L, device=dev, with_twin=True)
         pre_e = op_e.preconditioner()
+        stream.wait_stream(copy_stream)
+        for e_ in Ed:
+            e_.record_stream(stream)
         Pe, inf_e = P.solve_many([op_e, op_e], Ed, tol=TOL, max_iter=MAX_ITER, ratio=RATIO, precision="mixed",
                                  inner_tol=INNER_TOL, preconditioner=pre_e)
         xs = [op_e.cross_sections(Pe[j], Ed[j]) for j in range(2)]

@@ -239,6 +239,13 @@ def test_fused_krylov_steps_match_oracle(n, monkeypatch):
     assert _rel(Pg.cpu().numpy(), P_ref) < 1e-8
     Pm, im = op.solve(E, tol=1e-6, max_iter=500, ratio=100, precision="mixed")
     assert im.status == "converged" and im.true_relres <= 1e-6
+    # preconditioned: s and y formed by M's first pass
+    op._ctx.trim()
+    pre = op.preconditioner()
+    it_p, P_p, _, _ = O.solve_gpbicgstab((n, n, n), ia, G, E, mask, 100, 500, target=1e-6,
+                                         preconditioner=pre.reference_octant(C128).cpu().numpy())
+    Pq, iq = op.solve(E, tol=1e-6, max_iter=500, ratio=100, preconditioner=pre)
+    assert iq.iters == it_p and _rel(Pq.cpu().numpy(), P_p) < 1e-8
 
 
 @pytest.mark.parametrize("dtype,tol", [(C128, 1e-11), (C64, 2e-5)])
