@@ -187,9 +187,12 @@ def solve_gpbicgstab(grid_size, inv_alpha, interaction_matrix, preconditioner, E
     return info.iters, P, info.lowest_rel, info.first_rel
 
 
-def Gpbicgstab(A, E_inc, tol=1e-5, maxiter=2000, ratio=100.0, precision=None):
-    """Short form: solve A.P = E_inc for a DDAOperator A; returns (P, iters)."""
-    P, info = A.solve(E_inc, tol=tol, max_iter=maxiter, ratio=ratio, precision=precision)
+def Gpbicgstab(A, E_inc, tol=1e-5, maxiter=2000, ratio=100.0, precision=None, preconditioner=None):
+    """Short form: solve A.P = E_inc for a DDAOperator A; returns (P, iters).
+    ``preconditioner`` (None, True or an ``engine.Preconditioner``) selects
+    the precon=True recurrence."""
+    P, info = A.solve(E_inc, tol=tol, max_iter=maxiter, ratio=ratio, precision=precision,
+                      preconditioner=preconditioner)
     return P, info.iters
 
 
