@@ -68,32 +68,26 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 // is pruned), and only the kept half of each inverse output is formed.
 // NC = 0 reads the sizes from Geo.
 
-// Occupancy floors (CTAs per SM) of the cubic complex64 z and y passes.
-// Passes 1 and 5 of power-of-two lengths >= 128 at three CTAs of 384 threads
-// (<= 56 registers, a few bytes of spill; pass 5 otherwise takes 76 and fits
-// two): B200, 128^3 matvec 0.570 -> 0.538 ms, 64^3 unchanged.  Mixed-radix
-// lengths (E up to 24 per thread) would spill a kilobyte and keep the
-// compiler's choice.  DDA_Z_MINB / DDA_Y_MINB override (DDA_Y_MINB unset: the
-// compiler picks the y passes' registers; 4 measured slower).
-#ifndef DDA_Z_MINB
-#define DDA_Z_MINB 3
+// Register caps of the cubic complex64 z passes (1 and 5) of power-of-two
+// lengths >= 128: 56 registers, i.e. three CTAs of 384 threads per SM (a few
+// bytes of spill; pass 5 otherwise takes 76 and fits two).  B200, 128^3
+// matvec 0.570 -> 0.538 ms, 64^3 unchanged.  Mixed-radix lengths (E up to 24
+// per thread) would spill a kilobyte, and every other instantiation keeps the
+// compiler's own allocation (__maxnreg__ 255 is no cap).  DDA_Z_REGS /
+// DDA_Z1_REGS override the cap of both passes / of pass 1.
+#ifndef DDA_Z_REGS
+#define DDA_Z_REGS 56
 #endif
-#ifndef DDA_Z1_MINB
-#define DDA_Z1_MINB DDA_Z_MINB
+#ifndef DDA_Z1_REGS
+#define DDA_Z1_REGS DDA_Z_REGS
 #endif
-#define DDA_ZLB_N(R, NC, N)                                                                                      \
-  __launch_bounds__(kMvMaxThreads, ((NC) >= 64 && sizeof(R) == 4 && ((2 * (NC)) & (2 * (NC) - 1)) == 0) ? (N) : 1)
-#define DDA_ZLB(R, NC) DDA_ZLB_N(R, NC, DDA_Z_MINB)
-#if DDA_Z1_MINB == 0
-#define DDA_ZLB1(R, NC) __launch_bounds__(kMvMaxThreads)
-#else
-#define DDA_ZLB1(R, NC) DDA_ZLB_N(R, NC, DDA_Z1_MINB)
-#endif
-#ifdef DDA_Y_MINB
-#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads, ((NC) > 0 && sizeof(R) == 4) ? DDA_Y_MINB : 1)
-#else
+template <typename R, int NC, int CAP>
+constexpr int z_regs() {
+  return (NC >= 64 && sizeof(R) == 4 && ((2 * NC) & (2 * NC - 1)) == 0) ? CAP : 255;
+}
+#define DDA_ZLB(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z_REGS>()))
+#define DDA_ZLB1(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z1_REGS>()))
 #define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads)
-#endif
 
 // ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
@@ -326,8 +320,17 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
 // where two CTAs without spills measured faster (B200, two-RHS 64^3 matvec
 // 0.1362 -> 0.1321 ms; at L = 256 two CTAs were slower).  DDA_P3_MINB
 // overrides all lengths.
+// Complex128 cubic x passes of power-of-two length: at most 85 registers (two
+// 384-thread CTAs; the 192-thread launches then fit four per SM).  ptxas
+// settles at 80 without spills, against 100-108 uncapped: 64^3 two-RHS
+// matvec 0.347 -> 0.323 ms, 128^3 1.636 -> 1.54 ms, preconditioned c128
+// solve of the 64^3 sphere 39.2 -> 35.7 ms.  DDA_P3D_MINB overrides.
+#ifndef DDA_P3D_MINB
+#define DDA_P3D_MINB 2
+#endif
 template <typename R, int LX, int NC>
 constexpr int p3_min_blocks() {
+  if (NC > 0 && sizeof(R) == 8 && LX >= 64 && (LX & (LX - 1)) == 0) return DDA_P3D_MINB;
 #ifdef DDA_P3_MINB
   return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? DDA_P3_MINB : 1;
 #else
