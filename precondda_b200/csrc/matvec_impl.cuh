@@ -92,15 +92,28 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 #define DDA_P3MR_MINB 2
 #endif
 template <int NC> constexpr bool mixed_radix_mid() { return NC >= 20 && NC <= 96 && ((2 * NC) & (2 * NC - 1)) != 0; }
+// General (runtime-size, NC = 0) complex64 kernels: z and y passes at <= 85
+// registers and the x pass at two CTAs per SM (uncapped, many lengths take
+// 87-178 registers and run one CTA per SM).  Measured on 16-RHS matvecs of
+// non-cubic boxes: 64x80x20 -10 %, 80x40x72 -10 %, 96x64x96 -2 %, 48x32x64
+// equal.  DDA_GEN_REGS / DDA_GEN_P3_MINB override.
+#ifndef DDA_GEN_REGS
+#define DDA_GEN_REGS 85
+#endif
+#ifndef DDA_GEN_P3_MINB
+#define DDA_GEN_P3_MINB 2
+#endif
 template <typename R, int NC, int CAP>
 constexpr int z_regs() {
   return (NC >= 64 && sizeof(R) == 4 && ((2 * NC) & (2 * NC - 1)) == 0)
              ? CAP
-             : ((sizeof(R) == 4 && mixed_radix_mid<NC>()) ? DDA_ZMR_REGS : 255);
+             : ((sizeof(R) == 4 && mixed_radix_mid<NC>()) ? DDA_ZMR_REGS
+                                                           : ((sizeof(R) == 4 && NC == 0) ? DDA_GEN_REGS : 255));
 }
+template <typename R, int NC> constexpr int y_regs() { return (sizeof(R) == 4 && NC == 0) ? DDA_GEN_REGS : 255; }
 #define DDA_ZLB(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z_REGS>()))
 #define DDA_ZLB1(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z1_REGS>()))
-#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads)
+#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((y_regs<R, NC>()))
 
 // ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
@@ -345,6 +358,7 @@ template <typename R, int LX, int NC>
 constexpr int p3_min_blocks() {
   if (NC > 0 && sizeof(R) == 8 && LX >= 64 && (LX & (LX - 1)) == 0) return DDA_P3D_MINB;
   if (sizeof(R) == 4 && mixed_radix_mid<NC>()) return DDA_P3MR_MINB;
+  if (sizeof(R) == 4 && NC == 0) return DDA_GEN_P3_MINB;
 #ifdef DDA_P3_MINB
   return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? DDA_P3_MINB : 1;
 #else
