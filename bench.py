@@ -613,7 +613,8 @@ def run_batch64(args, ws, rank, local):
             xs[(g, j)] = cross_sections(Pv.contiguous(), G.E_incs[j], G.inv_alpha, G.k)
 
         res = solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, tuner=tuner, device=dev,
-                               keep_results=False, on_result=on_result, precondition=not args.no_precondition)
+                               keep_results=False, on_result=on_result, precondition=not args.no_precondition,
+                               chunk=args.chunk)
         torch.cuda.synchronize()
         t_all = time.perf_counter() - t_all
     launches = L.lib().dda_kernel_launches() - lc0
@@ -659,7 +660,7 @@ def run_serve(args, ws, rank, local):
     from precondda_b200.workloads import serving_stream, build_geometry
     dev = torch.device("cuda", local)
     stream = serving_stream(50 + rank, rate=args.rate, duration=args.duration)
-    srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=8, device=dev,
+    srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=args.chunk, device=dev,
                     precondition=not args.no_precondition)
     # warm the kernels of every bucket outside the timed region
     warm = sorted({srv.bucket_for(sp["box"]) for _, sp in stream})
@@ -764,6 +765,7 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
     ap.add_argument("--slots", type=int, default=16, help="serve: slots per size bucket")
+    ap.add_argument("--chunk", type=int, default=8, help="batch64 / serve: iterations per pool chunk between polls")
     ap.add_argument("--no-precondition", action="store_true",
                     help="batch64 / serve: the reference's precon=False solve instead of the preconditioned one")
     args = ap.parse_args()
