@@ -34,7 +34,7 @@ def _nvcc() -> str:
 
 
 def _headers_mtime() -> float:
-    hs = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) + \
+    hs = [h for pat in ("*.cuh", "*.inc", "*.h") for h in glob.glob(os.path.join(CSRC, pat))] + \
         glob.glob(os.path.join(INCLUDE, "*.h"))
     return max((os.path.getmtime(h) for h in hs), default=0.0)
 

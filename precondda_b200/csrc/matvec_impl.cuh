@@ -68,13 +68,19 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 // is pruned), and only the kept half of each inverse output is formed.
 // NC = 0 reads the sizes from Geo.
 
-// Register caps of the cubic complex64 z passes (1 and 5) of power-of-two
-// lengths >= 128: 56 registers, i.e. three CTAs of 384 threads per SM (a few
-// bytes of spill; pass 5 otherwise takes 76 and fits two).  B200, 128^3
-// matvec 0.570 -> 0.538 ms, 64^3 unchanged.  Mixed-radix lengths (E up to 24
-// per thread) would spill a kilobyte, and every other instantiation keeps the
-// compiler's own allocation (__maxnreg__ 255 is no cap).  DDA_Z_REGS /
-// DDA_Z1_REGS override the cap of both passes / of pass 1.
+// Register caps.  Each z / y pass exists twice: the plain kernel under
+// __launch_bounds__(384) alone, and a `_cap` twin with __maxnreg__ (the same
+// body, included from mv_pass*.inc); the dispatch takes the twin only for the
+// instantiations a cap was measured to help.  __maxnreg__ 255 is not "no
+// cap": ptxas then allocates more freely than under the launch bound alone
+// (cubic L = 128 y pass 56 -> 87 registers, 128^3 complex64 matvec 7 %
+// slower), and above 170 registers a 384-thread CTA cannot launch at all.
+//
+// Cubic complex64 z passes (1 and 5) of power-of-two lengths >= 128: 56
+// registers, i.e. three CTAs of 384 threads per SM (a few bytes of spill;
+// pass 5 otherwise takes 76 and fits two).  B200, 128^3 matvec 0.570 ->
+// 0.538 ms, 64^3 unchanged.  DDA_Z_REGS / DDA_Z1_REGS override the cap of
+// both passes / of pass 1.
 #ifndef DDA_Z_REGS
 #define DDA_Z_REGS 56
 #endif
@@ -92,100 +98,45 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 #define DDA_P3MR_MINB 2
 #endif
 template <int NC> constexpr bool mixed_radix_mid() { return NC >= 20 && NC <= 96 && ((2 * NC) & (2 * NC - 1)) != 0; }
-// General (runtime-size, NC = 0) complex64 kernels: z and y passes at <= 85
-// registers and the x pass at two CTAs per SM (uncapped, many lengths take
-// 87-178 registers and run one CTA per SM).  Measured on 16-RHS matvecs of
-// non-cubic boxes: 64x80x20 -10 %, 80x40x72 -10 %, 96x64x96 -2 %, 48x32x64
-// equal.  DDA_GEN_REGS / DDA_GEN_P3_MINB override.
+// General (runtime-size, NC = 0) complex64 kernels: the x pass at two CTAs
+// per SM (one CTA: 16-RHS matvecs of non-cubic boxes 1-17 % slower); z and y
+// passes plain (capped at 85 registers they were 5-16 % slower).
+// DDA_GEN_REGS (z), DDA_GEN_Y_REGS (y) and DDA_GEN_P3_MINB override; a
+// register cap of 0 selects the plain kernel.
 #ifndef DDA_GEN_REGS
-#define DDA_GEN_REGS 85
+#define DDA_GEN_REGS 0
+#endif
+#ifndef DDA_GEN_Y_REGS
+#define DDA_GEN_Y_REGS DDA_GEN_REGS
 #endif
 #ifndef DDA_GEN_P3_MINB
 #define DDA_GEN_P3_MINB 2
 #endif
+// Register cap of a z pass (0 = the plain kernel).
 template <typename R, int NC, int CAP>
 constexpr int z_regs() {
-  return (NC >= 64 && sizeof(R) == 4 && ((2 * NC) & (2 * NC - 1)) == 0)
-             ? CAP
-             : ((sizeof(R) == 4 && mixed_radix_mid<NC>()) ? DDA_ZMR_REGS
-                                                           : ((sizeof(R) == 4 && NC == 0) ? DDA_GEN_REGS : 255));
+  if (sizeof(R) != 4) return 0;
+  if (NC >= 64 && ((2 * NC) & (2 * NC - 1)) == 0) return CAP;
+  if (mixed_radix_mid<NC>()) return DDA_ZMR_REGS;
+  return NC == 0 ? DDA_GEN_REGS : 0;
 }
-template <typename R, int NC> constexpr int y_regs() { return (sizeof(R) == 4 && NC == 0) ? DDA_GEN_REGS : 255; }
-#define DDA_ZLB(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z_REGS>()))
-#define DDA_ZLB1(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z1_REGS>()))
-#define DDA_YLB(R, NC) __launch_bounds__(kMvMaxThreads) __maxnreg__((y_regs<R, NC>()))
+// Register cap of a y pass (0 = the plain kernel).
+template <typename R, int NC> constexpr int y_regs() { return (sizeof(R) == 4 && NC == 0) ? DDA_GEN_Y_REGS : 0; }
 
 // ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
 // thread = (c fastest, t, line)
 // ---------------------------------------------------------------------------
 template <typename R, int LZ, int NC>
-__global__ void DDA_ZLB1(R, NC) k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                            InstState* st, const int* act, int in_id, int cond,
-                                                            int nl_, int pre) {
-  grid_dep_begin();
-  typedef typename CT<R>::T C;
-  typedef MvShape<R, LZ> SH;
-  typedef typename SH::P P;
-  constexpr bool CUBE = NC > 0;
-  static_assert(!CUBE || LZ == 2 * NC, "cubic kernels need L = 2n");
-  constexpr int NLC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), NC * NC) : 1;
-  constexpr bool ZH = CUBE && P::r[0] % 2 == 0;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  InstState& S = st[inst_of(act)];
-  if (!cond_ok(S, cond)) return;
-  const C* __restrict__ x = (const C*)S.vec[in_id];
-  C* __restrict__ t1 = (C*)S.t1;
-  const int nl = CUBE ? NLC : nl_;
-  const int nz = CUBE ? NC : g.nz;
-  const long long nlines = CUBE ? (long long)NC * NC : (long long)g.nx * g.ny;
-  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
-  const int t = rest % SH::T, l = rest / SH::T;
-  const long long line = (long long)blockIdx.x * nl + l;
-  const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
-  const long long base = line * nz * 3 + c;
-  // occupied-site vectors: element (site, c) lives at 3 cidx[site] + c
-  const int* __restrict__ cid = S.cidx ? S.cidx + line * nz : nullptr;
-  auto eidx = [&](int pos) -> long long {
-    if (!cid) return base + (long long)pos * 3;
-    const int k = cid[pos];
-    return k < 0 ? -1 : 3LL * k + c;
-  };
-  C* tl = t1 + line * (long long)LZ * 3 + c;
-  C* sl = s + l * 3 * SH::LP + c;
-  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
-  auto stf = [&](int, int pos, C v) { if (ok) __stcg(tl + pos * 3, v); };
-  C a[P::E];
-  if (pre == MV_PRE_SY) {
-    // the input is s = r - alpha v, formed here together with
-    // y = s_prev - s - alpha w (Gpbicgstab.py:1020-1021); both are stored
-    const C* __restrict__ r = (const C*)S.vec[V_R];
-    const C* __restrict__ v = (const C*)S.vec[V_V];
-    const C* __restrict__ sp = (const C*)S.vec[V_SPREV];
-    const C* __restrict__ w = (const C*)S.vec[V_W];
-    C* __restrict__ so = (C*)S.vec[V_S];
-    C* __restrict__ yo = (C*)S.vec[V_Y];
-    const C al = mk<C>(S.alpha.x, S.alpha.y);
-    auto ld = [&](int, int pos) -> C {
-      if (!(ok && (ZH || pos < nz))) return czero<C>();
-      const long long i = eidx(pos);
-      if (i < 0) return czero<C>();
-      const C sv = csub(__ldcg(r + i), cmul(al, __ldcg(v + i)));
-      __stcg(so + i, sv);
-      __stcg(yo + i, csub(csub(__ldcg(sp + i), sv), cmul(al, __ldcg(w + i))));
-      return sv;
-    };
-    rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
-  } else {
-    auto ld = [&](int, int pos) -> C {
-      if (!(ok && (ZH || pos < nz))) return czero<C>();
-      const long long i = eidx(pos);
-      return i < 0 ? czero<C>() : __ldcg(x + i);
-    };
-    rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
-  }
-}
+__global__ void __launch_bounds__(kMvMaxThreads)
+    k_mv_pass1(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int in_id,
+               int cond, int nl_, int pre)
+#include "mv_pass1.inc"
+template <typename R, int LZ, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z1_REGS>()))
+    k_mv_pass1_cap(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int in_id,
+                   int cond, int nl_, int pre)
+#include "mv_pass1.inc"
 
 // ---------------------------------------------------------------------------
 // pass 2 / 4: y transforms on a (ix, kz-tile) slab, W = 3 tz transforms;
@@ -193,46 +144,15 @@ __global__ void DDA_ZLB1(R, NC) k_mv_pass1(Geo g, const typename CT<R>::T* __res
 // INV=true: T2 -> T1 keeping rows y < ny.
 // ---------------------------------------------------------------------------
 template <typename R, bool INV, int LY, int NC>
-__global__ void DDA_YLB(R, NC) k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                             InstState* st, const int* act, int cond, int tz_,
-                                                             int ntz_) {
-  grid_dep_begin();
-  typedef typename CT<R>::T C;
-  typedef MvShape<R, LY> SH;
-  typedef typename SH::P P;
-  constexpr bool CUBE = NC > 0;
-  static_assert(!CUBE || LY == 2 * NC, "cubic kernels need L = 2n");
-  constexpr int TZC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), LY) : 1;
-  constexpr int NTZC = (LY + TZC - 1) / TZC;
-  constexpr bool ZH = CUBE && !INV && P::r[0] % 2 == 0;
-  constexpr bool DH = CUBE && INV && half_store_ok<P>();
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  InstState& S = st[inst_of(act)];
-  if (!cond_ok(S, cond)) return;
-  C* __restrict__ t1 = (C*)S.t1;
-  C* __restrict__ t2 = (C*)S.t2;
-  const int tz = CUBE ? TZC : tz_;
-  const int ntz = CUBE ? NTZC : ntz_;
-  const int Lz = CUBE ? LY : g.Lz;
-  const int ny = CUBE ? NC : g.ny;
-  const int W = 3 * tz;
-  const int w = threadIdx.x % W, t = threadIdx.x / W;
-  const int ix = blockIdx.x / ntz, kzt = blockIdx.x - ix * ntz;
-  const int kz0 = kzt * tz;
-  const bool ok = (CUBE && LY % TZC == 0) || w < 3 * min(tz, Lz - kz0);
-  const long long rs = (long long)Lz * 3;                 // row stride of T1/T2
-  const C* src = (INV ? t2 + (long long)ix * LY * rs : t1 + (long long)ix * ny * rs) + kz0 * 3 + w;
-  C* dst = (INV ? t1 + (long long)ix * ny * rs : t2 + (long long)ix * LY * rs) + kz0 * 3 + w;
-  C* sw = s + w;
-  auto ld = [&](int, int pos) -> C {
-    return (ok && (INV || ZH || pos < ny)) ? __ldcg(src + pos * rs) : czero<C>();
-  };
-  auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
-  auto stf = [&](int, int pos, C v) { if (ok && (!INV || DH || pos < ny)) __stcg(dst + pos * rs, v); };
-  C a[P::E];
-  rfft<P, 1, INV, ZH, DH>(a, t, ld, sm, stf, tw);
-}
+__global__ void __launch_bounds__(kMvMaxThreads)
+    k_mv_pass_y(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int cond,
+                int tz_, int ntz_)
+#include "mv_pass_y.inc"
+template <typename R, bool INV, int LY, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((y_regs<R, NC>()))
+    k_mv_pass_y_cap(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int cond,
+                    int tz_, int ntz_)
+#include "mv_pass_y.inc"
 
 // ---------------------------------------------------------------------------
 // pass 3: x-pencils: forward x-FFT, symmetric 3x3 tensor product with the
@@ -481,101 +401,15 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
 // ---------------------------------------------------------------------------
 template <typename R, int LZ, int NC>
-__global__ void DDA_ZLB(R, NC) k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw,
-                                                            InstState* st, const int* act, int in_id, int out_id,
-                                                            int mode, int cond, int nl_, int post, double* red,
-                                                            unsigned* cnt) {
-  grid_dep_begin();
-  typedef typename CT<R>::T C;
-  typedef MvShape<R, LZ> SH;
-  typedef typename SH::P P;
-  constexpr bool CUBE = NC > 0;
-  static_assert(!CUBE || LZ == 2 * NC, "cubic kernels need L = 2n");
-  constexpr int NLC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), NC * NC) : 1;
-  constexpr bool DH = CUBE && half_store_ok<P>();
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* s = reinterpret_cast<C*>(smem_raw);
-  const int inst = inst_of(act);
-  InstState& S = st[inst];
-  if (!cond_ok(S, cond)) return;
-  const C* __restrict__ t1 = (const C*)S.t1;
-  const int nl = CUBE ? NLC : nl_;
-  const int nz = CUBE ? NC : g.nz;
-  const long long nlines = CUBE ? (long long)NC * NC : (long long)g.nx * g.ny;
-  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
-  const int t = rest % SH::T, l = rest / SH::T;
-  const long long line = (long long)blockIdx.x * nl + l;
-  const bool ok = (CUBE && (NC * NC) % NLC == 0) || line < nlines;
-  const C* tl = t1 + line * (long long)LZ * 3 + c;
-  C* sl = s + l * 3 * SH::LP + c;
-  // the combine runs on the last stage's registers: for a fixed leg the
-  // lanes (component fastest, then t) hold consecutive sites of a line, so
-  // the stores below are contiguous
-  const long long site0 = line * nz;
-  const C* __restrict__ xg = (const C*)S.vec[in_id];
-  C* __restrict__ yg = (C*)S.vec[out_id];
-  const C* __restrict__ iag = (const C*)S.inva + site0;
-  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] : nullptr;
-  // occupied-site vectors: element (site, c) lives at 3 cidx[site] + c
-  const int* __restrict__ cid = S.cidx ? S.cidx + site0 : nullptr;
-  // fused dot products of the output (post): <rhat, v> for alpha, or the
-  // zeta / eta dots of t with s and y
-  const bool first = (S.iter == 0) || S.was_reset;
-  const C* __restrict__ d0 = post == MV_POST_ALPHA ? (const C*)S.vec[V_RHAT]
-                           : (post == MV_POST_ZETA ? (const C*)S.vec[V_S] : nullptr);
-  const C* __restrict__ d1 = post == MV_POST_ZETA ? (const C*)S.vec[V_Y] : nullptr;
-  double acc[8];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) acc[k] = 0.0;
-  auto ld = [&](int, int pos) -> C { return ok ? __ldcg(tl + pos * 3) : czero<C>(); };
-  auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
-  auto stf = [&](int, int pos, C v) {
-    if (!(ok && (DH || pos < nz))) return;
-    long long e = (site0 + pos) * 3 + c;
-    if (cid) {
-      const int k = cid[pos];
-      if (k < 0) return;               // empty site: not stored
-      e = 3LL * k + c;
-    }
-    C r;
-    if (mode == MV_CONV) {
-      r = v;
-    } else {
-      const C a_ = __ldg(iag + pos);        // shared by the 3 component lanes
-      const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
-      if (!msk) v = czero<C>();
-      if (mode == MV_CONV_MASKED) {
-        r = v;
-      } else {
-        r = csub(cmul(a_, __ldcg(xg + e)), v);
-        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + e), r);
-      }
-    }
-    __stcg(yg + e, r);
-    if (post == MV_POST_ALPHA) {
-      const C h = __ldcg(d0 + e);
-      acc[0] += (double)h.x * r.x + (double)h.y * r.y;
-      acc[1] += (double)h.x * r.y - (double)h.y * r.x;
-    } else if (post == MV_POST_ZETA) {
-      const C sv = __ldcg(d0 + e);
-      if (first) {
-        acc[0] += (double)r.x * r.x + (double)r.y * r.y;
-        acc[1] += (double)r.x * sv.x + (double)r.y * sv.y;
-        acc[2] += (double)r.x * sv.y - (double)r.y * sv.x;
-      } else {
-        zeta_dots_acc(acc, r, sv, __ldcg(d1 + e));
-      }
-    }
-  };
-  C a[P::E];
-  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
-  if (post == MV_POST_NONE) return;
-  double tot[8];
-  if (reduce_last_n<8>(acc, tot, red, cnt, inst, (int)gridDim.x, blockDim.x) && threadIdx.x == 0) {
-    if (post == MV_POST_ALPHA) alpha_from_dot(S, tot);
-    else zeta_eta_from_dots(S, tot, first);
-  }
-}
+__global__ void __launch_bounds__(kMvMaxThreads)
+    k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int in_id,
+               int out_id, int mode, int cond, int nl_, int post, double* red, unsigned* cnt)
+#include "mv_pass5.inc"
+template <typename R, int LZ, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z_REGS>()))
+    k_mv_pass5_cap(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int in_id,
+                   int out_id, int mode, int cond, int nl_, int post, double* red, unsigned* cnt)
+#include "mv_pass5.inc"
 
 // ---------------------------------------------------------------------------
 // Passes 1+2 and 4+5 fused over a thread-block cluster (cubic boxes; the
@@ -795,17 +629,39 @@ template <> bool mv_general_set<double>(int, int, int, int, MvSet<double>&);
 template <> bool mv_cube_set<float>(int, int, MvSet<float>&);
 template <> bool mv_cube_set<double>(int, int, MvSet<double>&);
 
+// The z / y pass kernels of an instantiation: the `_cap` twin where a
+// register cap applies, else the plain kernel.
+template <typename R, int L, int NC>
+auto pick_pass1() {
+  if constexpr (z_regs<R, NC, DDA_Z1_REGS>() > 0) return k_mv_pass1_cap<R, L, NC>;
+  else return k_mv_pass1<R, L, NC>;
+}
+template <typename R, int L, int NC>
+auto pick_pass5() {
+  if constexpr (z_regs<R, NC, DDA_Z_REGS>() > 0) return k_mv_pass5_cap<R, L, NC>;
+  else return k_mv_pass5<R, L, NC>;
+}
+template <typename R, bool INV, int L, int NC>
+auto pick_pass_y() {
+  if constexpr (y_regs<R, NC>() > 0) return k_mv_pass_y_cap<R, INV, L, NC>;
+  else return k_mv_pass_y<R, INV, L, NC>;
+}
+
 template <typename R>
 bool mv_general_set_impl(int Lx, int Ly, int Lz, int p3var, MvSet<R>& o) {
   typedef MvSet<R> M;
   switch (Lz) {
-#define DDA_K(n) case n: o.k1 = k_mv_pass1<R, n, 0>; o.k5 = k_mv_pass5<R, n, 0>; break;
+#define DDA_K(n) case n: o.k1 = pick_pass1<R, n, 0>(); o.k5 = pick_pass5<R, n, 0>(); break;
     DDA_FFT_SIZES(DDA_K)
 #undef DDA_K
     default: return false;
   }
   switch (Ly) {
-#define DDA_K(n) case n: o.k2 = (typename M::PY)k_mv_pass_y<R, false, n, 0>; o.k4 = (typename M::PY)k_mv_pass_y<R, true, n, 0>; break;
+#define DDA_K(n)                                                                                   \
+  case n:                                                                                          \
+    o.k2 = (typename M::PY)pick_pass_y<R, false, n, 0>();                                          \
+    o.k4 = (typename M::PY)pick_pass_y<R, true, n, 0>();                                           \
+    break;
     DDA_FFT_SIZES(DDA_K)
 #undef DDA_K
     default: return false;
@@ -828,12 +684,12 @@ template <typename R, int L, int V>
 void mv_cube_fill(MvSet<R>& o) {
   typedef MvSet<R> M;
   constexpr int NC = L / 2;
-  o.k1 = k_mv_pass1<R, L, NC>;
-  o.k2 = (typename M::PY)k_mv_pass_y<R, false, L, NC>;
+  o.k1 = pick_pass1<R, L, NC>();
+  o.k2 = (typename M::PY)pick_pass_y<R, false, L, NC>();
   if constexpr (V == 1) o.k3 = (typename M::P3)k_mv_pass3r<R, L, V, NC>;
   else o.k3 = (typename M::P3)k_mv_pass3s<R, L, V, NC>;
-  o.k4 = (typename M::PY)k_mv_pass_y<R, true, L, NC>;
-  o.k5 = k_mv_pass5<R, L, NC>;
+  o.k4 = (typename M::PY)pick_pass_y<R, true, L, NC>();
+  o.k5 = pick_pass5<R, L, NC>();
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
   o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
   o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);

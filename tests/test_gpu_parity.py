@@ -79,6 +79,26 @@ def test_matvec_pass3_variants(variant, shape, dtype, tol, monkeypatch):
     assert _rel(op.matvec(x).cpu().numpy(), ref) < tol
 
 
+@pytest.mark.parametrize("n", [4, 6, 10, 12, 16, 20, 24, 32, 36, 40, 48, 64, 72, 80, 96, 128, 144, 160])
+@pytest.mark.parametrize("dtype,tol", [(C128, 1e-12), (C64, 2e-5)])
+def test_cubic_kernels_launch_and_match_general(n, dtype, tol, monkeypatch):
+    """Every compiled cubic FFT length up to 320 (box n^3 on (2n)^3) launches
+    and equals the runtime-size kernels on the same operator.  Above 170
+    registers per thread a 384-thread CTA cannot launch, so this catches
+    launch-bound mistakes at lengths no other test reaches."""
+    P = _pkg()
+    k, d, alpha, x = _rand_problem((n,) * 3, seed=n)
+    ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+    op = P.DDAOperator(ia, k, d, dtype=dtype)
+    assert tuple(op.L) == (2 * n,) * 3
+    monkeypatch.delenv("DDA_NO_CUBE", raising=False)
+    cube = op.matvec(x).cpu().numpy()
+    monkeypatch.setenv("DDA_NO_CUBE", "1")
+    general = op.matvec(x).cpu().numpy()
+    assert np.isfinite(cube).all()
+    assert _rel(cube, general) < tol
+
+
 def test_matvec_dense_tiny():
     P = _pkg()
     k, d, alpha, x = _rand_problem((4, 4, 4), seed=3)
