@@ -87,12 +87,12 @@ template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T
 #ifndef DDA_Z1_REGS
 #define DDA_Z1_REGS DDA_Z_REGS
 #endif
-// Mixed-radix lengths 40-192 (boxes 20^3-96^3): z passes at <= 85 registers
-// and the x pass at two CTAs per SM (instead of one at 118-158 registers);
-// measured together on batched complex64 matvecs: 80^3 -7.7 %, 40^3 -5 %,
-// 96^3 -1.5 %, 48^3 equal.  DDA_ZMR_REGS / DDA_P3MR_MINB override.
+// Mixed-radix lengths 40-192 (boxes 20^3-96^3): the x pass at two CTAs per
+// SM (one CTA at 118-158 registers: 16-RHS matvecs 2-15 % slower); z passes
+// plain (capped at 85 registers they were 5-9 % slower).  DDA_ZMR_REGS /
+// DDA_P3MR_MINB override.
 #ifndef DDA_ZMR_REGS
-#define DDA_ZMR_REGS 85
+#define DDA_ZMR_REGS 0
 #endif
 #ifndef DDA_P3MR_MINB
 #define DDA_P3MR_MINB 2
