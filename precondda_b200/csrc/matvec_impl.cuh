@@ -112,10 +112,17 @@ template <int NC> constexpr bool mixed_radix_mid() { return NC >= 20 && NC <= 96
 #ifndef DDA_GEN_P3_MINB
 #define DDA_GEN_P3_MINB 2
 #endif
+// Complex128 z passes of power-of-two cubic lengths >= 128: plain.  At 56
+// registers (three CTAs per SM) the 128^3 matvec took 1.403 against 1.428 ms
+// and the one-RHS 64^3 one 0.1556 against 0.1536 ms, within noise; the x
+// pass dominates.  DDA_ZD_REGS sets a cap.
+#ifndef DDA_ZD_REGS
+#define DDA_ZD_REGS 0
+#endif
 // Register cap of a z pass (0 = the plain kernel).
 template <typename R, int NC, int CAP>
 constexpr int z_regs() {
-  if (sizeof(R) != 4) return 0;
+  if (sizeof(R) != 4) return (NC >= 64 && ((2 * NC) & (2 * NC - 1)) == 0) ? DDA_ZD_REGS : 0;
   if (NC >= 64 && ((2 * NC) & (2 * NC - 1)) == 0) return CAP;
   if (mixed_radix_mid<NC>()) return DDA_ZMR_REGS;
   return NC == 0 ? DDA_GEN_REGS : 0;
