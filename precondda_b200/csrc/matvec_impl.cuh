@@ -281,9 +281,17 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
 #ifndef DDA_P3D_MINB
 #define DDA_P3D_MINB 2
 #endif
+// Complex128 x passes of every other length (general and mixed-radix
+// cubic kernels): one CTA per SM.  At two, 4-RHS matvecs took 80^3 1.92
+// against 1.38 ms, 48^3 0.42 against 0.27 ms, 96x64x96 2.55 against 1.42 ms
+// (100x60x30 0.59 against 0.65 ms).  DDA_P3D_GEN_MINB overrides.
+#ifndef DDA_P3D_GEN_MINB
+#define DDA_P3D_GEN_MINB 1
+#endif
 template <typename R, int LX, int NC>
 constexpr int p3_min_blocks() {
   if (NC > 0 && sizeof(R) == 8 && LX >= 64 && (LX & (LX - 1)) == 0) return DDA_P3D_MINB;
+  if (sizeof(R) == 8) return DDA_P3D_GEN_MINB;
   if (sizeof(R) == 4 && mixed_radix_mid<NC>()) return DDA_P3MR_MINB;
   if (sizeof(R) == 4 && NC == 0) return DDA_GEN_P3_MINB;
 #ifdef DDA_P3_MINB
