@@ -130,19 +130,22 @@ int dda_matvec(dda_op* op, int mode, const void* x, void* y, const void* b, void
 int dda_matvec_batch(dda_op* const* ops, int nb, int mode, const void* const* x, void* const* y,
                      const void* const* b, void* stream);
 
-/* Allocation-free A.x.  No counterpart in the reference: it exists for
- * callers that cannot allocate device memory where they need the product --
- * code recording into a CUDA graph (cudaMalloc cannot be captured), serving
- * loops that forbid allocator latency, and hosts whose device memory is owned
- * by another framework's pool.  Same product and modes as dda_matvec, with
+/* Allocation-free A.x.  No counterpart in the reference.  It serves callers
+ * that cannot allocate device memory where they need the product: serving or
+ * real-time loops whose latency budget rules out allocator calls (cudaMalloc
+ * may synchronise the device and takes unbounded time), and host applications
+ * whose device memory belongs to another framework's caching pool, which raw
+ * cudaMalloc calls would bypass.  Same product and modes as dda_matvec, with
  * ghat in the engine layout and every array caller-owned; the transform
- * scratch, state and twiddles live in one static __device__ buffer of
- * DDA_NOALLOC_SCRATCH_BYTES that each GPU loading the library keeps until
- * exit.  Problems whose scratch (nx*ny*Lz*3 + nx*Ly*Lz*3 complex) does not fit
- * are rejected with DDA_ERR_BAD_SHAPE (e.g. a 64^3 box with FFT 128^3 fits in
- * complex64, not in complex128).  The first call on a device looks up the
- * buffer's address and should come before any stream capture.  Calls share
- * the buffer: calls that overlap on the GPU race and must not be issued. */
+ * scratch, state block and twiddle tables live in one static __device__
+ * array of DDA_NOALLOC_SCRATCH_BYTES that each GPU loading the library keeps
+ * until exit.  Problems whose scratch (nx*ny*Lz*3 + nx*Ly*Lz*3 complex) does
+ * not fit are rejected with DDA_ERR_BAD_SHAPE (e.g. a 64^3 box with FFT 128^3
+ * fits in complex64, not in complex128).  The first call on a device looks up
+ * the array's address and writes the twiddle tables with a synchronous copy;
+ * it should come before any stream capture.  Later calls only enqueue
+ * kernels.  Calls share the array: calls that overlap on the GPU race and
+ * must not be issued. */
 #define DDA_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, const void* ghat,
                        double gscale, const void* inv_alpha, int mode, const void* x, void* y, const void* b,

@@ -13,7 +13,10 @@ shared library and the manifest stay (``oracle/_ref`` is not committed).
 Kernels that are not on the DDA path (the preconditioner's template kernels and
 the cuComplex gather/scatter helpers) are skipped.
 
-Usage:  python oracle/build_ref.py [--ref /root/reference]
+Usage:  python oracle/build_ref.py [--ref <reference checkout>]
+
+The checkout is found by ``reference_dir()``: ``$DDA_REFERENCE_DIR`` if set,
+else the checkout path of the build container.
 """
 from __future__ import annotations
 
@@ -30,6 +33,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 SHIM = os.path.join(HERE, "refshim")
 DEFAULT_REF = "/root/reference"
+
+
+def reference_dir():
+    """Where this recipe reads the reference checkout: $DDA_REFERENCE_DIR, else
+    the build container's checkout path.  It is the one place that names it."""
+    return os.environ.get("DDA_REFERENCE_DIR", DEFAULT_REF)
 FILES = ("Gpbicgstab.py", "ExcitedField.py", "ddaforgit.py")
 
 _EW_TYPES = {"int32": "int", "int64": "long long", "float32": "float", "float64": "double",
@@ -118,7 +127,8 @@ def _ew_kernel(mod, var, in_params, out_params, body, name):
     return code, man
 
 
-def build(ref=DEFAULT_REF, verbose=False):
+def build(ref=None, verbose=False):
+    ref = ref or reference_dir()
     os.makedirs(OUT, exist_ok=True)
     units, manifest = [], []
     for fn in FILES:
@@ -158,7 +168,7 @@ def build(ref=DEFAULT_REF, verbose=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default=DEFAULT_REF)
+    ap.add_argument("--ref", default=None)
     a = ap.parse_args()
     lib, man = build(a.ref, verbose=True)
     print(lib)

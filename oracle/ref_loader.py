@@ -83,7 +83,7 @@ def _import_file(path, name, torch_proxy):
     return mod
 
 
-def load(ref_dir="/root/reference"):
+def load(ref_dir):
     torch_proxy = _TorchCPU()
     srcs = {}
     for fn in ("Gpbicgstab.py", "ExcitedField.py", "ddaforgit.py"):

@@ -3,7 +3,7 @@
 Run from the repository root in a checkout that has the reference:
 
     python oracle/build_ref.py                 # compile its kernel strings
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref <reference checkout>]
 
 The reference (Toastlovesjam/preconDDA) is executed unchanged through
 ``oracle/ref_loader.py``: ``Gpbicgstab.solve_gpbicgstab``,
@@ -28,7 +28,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from oracle import ref_loader  # noqa: E402
+from oracle import build_ref, ref_loader  # noqa: E402
 
 OUT = os.path.join(ROOT, "tests", "golden", "ref_fixtures.npz")
 
@@ -177,5 +177,5 @@ def main(ref):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
-    main(ap.parse_args().ref)
+    ap.add_argument("--ref", default=None, help="reference checkout (default: oracle.build_ref.reference_dir())")
+    main(ap.parse_args().ref or build_ref.reference_dir())
