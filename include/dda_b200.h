@@ -282,21 +282,37 @@ int dda_slots_release(dda_slots* pool, int slot);
 #define DDA_SHAPE_CYLINDER 3
 #define DDA_SHAPE_PRISM 4
 
+/* Flags of a dda_shape.
+ * DDA_SHAPE_WINDOW: the shape marks only sites with win[2a] <= i_a < win[2a+1]
+ *   on each axis a -- the per-shape index window of the reference's
+ *   mark_shapes (ddaforgit.py:626-649), which bounds its x- and y-axis
+ *   cylinders (see below).
+ * DDA_SHAPE_GEOMETRIC_AXES: x- and y-axis cylinders take the radial distance
+ *   perpendicular to their axis and the absolute axial offset.  Without it a
+ *   cylinder follows the reference's Numba cylinder (ddaforgit.py:477-509):
+ *   the radial distance is always taken in the (x, y) plane, and for the x
+ *   and y axes the height test compares the signed z offset with height/2. */
+#define DDA_SHAPE_WINDOW 1
+#define DDA_SHAPE_GEOMETRIC_AXES 2
+
 /* One shape of a voxelisation, in the length unit of d.  p[]: sphere r;
  * ellipsoid semi-axes (a,b,c); rectangle edge lengths (x,y,z); cylinder
  * (radius, height); prism (circumradius, height).  axis (0,1,2 = x,y,z) for
  * cylinder / prism, sides for prism.  rot: ellipsoid body->lab rotation,
  * row-major (identity for the reference's axis-aligned ellipsoid).
- * inv_alpha: value written at member sites. */
+ * inv_alpha: value written at member sites.  flags / win: see above (win in
+ * the voxelised box's site indices). */
 typedef struct dda_shape {
   int type;
   int axis;
   int sides;
-  int reserved;
+  int flags;
   double center[3];
   double p[4];
   double rot[9];
   double inv_alpha[2];
+  int win[6];
+  int reserved[2];
 } dda_shape;
 
 /* Replaces mark_shapes / create_alpha_and_n_arrays (ddaforgit.py:615-830)

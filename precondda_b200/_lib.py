@@ -61,12 +61,13 @@ class dda_instance(C.Structure):
 
 
 SHAPE_SPHERE, SHAPE_ELLIPSOID, SHAPE_RECTANGLE, SHAPE_CYLINDER, SHAPE_PRISM = range(5)
+SHAPE_WINDOW, SHAPE_GEOMETRIC_AXES = 1, 2
 
 
 class dda_shape(C.Structure):
-    _fields_ = [("type", C.c_int), ("axis", C.c_int), ("sides", C.c_int), ("reserved", C.c_int),
+    _fields_ = [("type", C.c_int), ("axis", C.c_int), ("sides", C.c_int), ("flags", C.c_int),
                 ("center", C.c_double * 3), ("p", C.c_double * 4), ("rot", C.c_double * 9),
-                ("inv_alpha", C.c_double * 2)]
+                ("inv_alpha", C.c_double * 2), ("win", C.c_int * 6), ("reserved", C.c_int * 2)]
 
 
 class dda_result(C.Structure):

@@ -139,7 +139,8 @@ struct InstState {
   int cur_x;           // which of XA/XB/XC holds the current iterate (0..2)
   int best_x;          // which holds the best iterate (0..2), -1 = none yet
   int active;          // 1 while the instance takes part in the batch
-  int pad_[3];
+  int fault;           // set by a kernel whose bounded wait for its staged input gave up
+  int pad_[2];
 };
 
 __device__ __forceinline__ bool cond_ok(const InstState& s, int cond) {

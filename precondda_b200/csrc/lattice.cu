@@ -5,8 +5,15 @@
 // sphere :439-448, ellipsoid :450-459, rectangle :461-475, cylinder :477-509,
 // prism :511-572) evaluated at voxel centres origin + (i+0.5) d
 // (ddaforgit.py:617, :643-647); later shapes overwrite earlier ones as in
-// mark_shapes (:656-661).  Extensions: an ellipsoid may carry a rotation
-// (body -> lab matrix), and a sphere list expresses aggregates.
+// mark_shapes (:656-661), and a shape with DDA_SHAPE_WINDOW marks only the
+// index window mark_shapes evaluates it on (:626-649).  The reference's
+// cylinder takes its radial distance in the (x, y) plane for every axis and,
+// for the x and y axes, tests the signed z offset against height/2; that is
+// the default here too (DDA_SHAPE_GEOMETRIC_AXES selects the perpendicular
+// split).  The cylinder arithmetic uses round-to-nearest intrinsics, so no
+// multiply-add is contracted and each operation rounds as the reference's
+// does.  Extensions: an ellipsoid may carry a rotation (body -> lab matrix),
+// and a sphere list expresses aggregates.
 // The incident field is e exp(i k.r) with r = (i,j,k) d, no half-voxel offset
 // (ddaforgit.py:1626-1632).
 #include <algorithm>
@@ -45,6 +52,14 @@ __device__ bool inside(const dda_shape& s, double x, double y, double z) {
       return in || edge;
     }
     case DDA_SHAPE_CYLINDER:
+      if (!(s.flags & DDA_SHAPE_GEOMETRIC_AXES)) {
+        const double r = s.p[0], hh = s.p[1] / 2;
+        const double rd = sqrt(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        const double h = s.axis == 2 ? fabs(dz) : dz;
+        const bool inr = rd <= r, onr = fabs(rd - r) < kEps, inh = h <= hh, cap = fabs(h - hh) < kEps;
+        return (inr && inh) || (onr && inh) || (inr && cap);
+      }
+      [[fallthrough]];
     case DDA_SHAPE_PRISM: {
       double u, v, h;      // in-plane offsets and axial distance
       if (s.axis == 0) { u = dy; v = dz; h = fabs(dx); }
@@ -91,8 +106,13 @@ __global__ void k_voxelize(const dda_shape* __restrict__ shapes, int nshape, int
     const int iy = (int)(r % ny), ix = (int)(r / ny);
     const double x = ox + (ix + 0.5) * d, y = oy + (iy + 0.5) * d, z = oz + (iz + 0.5) * d;
     C v = czero<C>();
-    for (int s = 0; s < nshape; ++s)
-      if (inside(shapes[s], x, y, z)) v = mk<C>(shapes[s].inv_alpha[0], shapes[s].inv_alpha[1]);
+    for (int s = 0; s < nshape; ++s) {
+      const dda_shape& sh = shapes[s];
+      if ((sh.flags & DDA_SHAPE_WINDOW) && (ix < sh.win[0] || ix >= sh.win[1] || iy < sh.win[2] ||
+                                            iy >= sh.win[3] || iz < sh.win[4] || iz >= sh.win[5]))
+        continue;
+      if (inside(sh, x, y, z)) v = mk<C>(sh.inv_alpha[0], sh.inv_alpha[1]);
+    }
     ia[i] = v;
   }
 }

@@ -26,6 +26,24 @@ bool fused_zy_enabled(bool inverse) {
   return true;
 }
 
+bool p3_pipe_enabled() {
+  const char* e = getenv("DDA_NO_P3PIPE");
+  return !(e && *e == '1');
+}
+
+int device_sms() {
+  static std::mutex mu;
+  static int sms[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!sms[dev]) {
+    int v = 0;
+    sms[dev] = (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) ? v : 148;
+  }
+  return sms[dev];
+}
+
 cudaError_t mv_prepare(const void* const* ks, int n) {
   static std::mutex mu;
   static std::set<std::pair<int, const void*>> done;

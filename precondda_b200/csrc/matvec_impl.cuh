@@ -22,6 +22,7 @@
 #include "fftreg.cuh"
 #include "krylov_ctrl.cuh"
 #include "fft_sizes.h"
+#include "bulk.cuh"
 #include <cooperative_groups.h>
 #include <cstdlib>
 #include <type_traits>
@@ -408,6 +409,161 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
 }
 
 // ---------------------------------------------------------------------------
+// pass 3, staged and persistent (cubic boxes, one component per thread):
+// the same arithmetic as k_mv_pass3s, but every CTA loops over tiles (one
+// pencil row ky x TZ kz columns) and its input tile -- the NC kept x rows of
+// 3 TZ complex each, contiguous in T2 -- arrives in shared memory through
+// bulk async copies issued one tile ahead, so the transform of tile i runs
+// while tile i+1 is in flight.  Two input buffers alternate; the exchange /
+// tensor area is that of k_mv_pass3s.  Outputs go straight to T2 from the
+// inverse transform's last stage (rows x < NC).
+// ---------------------------------------------------------------------------
+template <typename R, int LX, int V, int TZ>
+struct P3Pipe {
+  typedef typename CT<R>::T C;
+  typedef P3Shape<R, LX, V> SH;
+  static constexpr int NC = LX / 2;              // kept x rows (box edge)
+  static constexpr int W = 3 * TZ;               // complex per row segment
+  static constexpr int TH = W * SH::T;           // threads
+  static constexpr int ROWB = W * (int)sizeof(C);
+  static constexpr size_t XS = (size_t)W * SH::LP * sizeof(C);     // exchange / tensor area
+  static constexpr size_t IB = (size_t)NC * W * sizeof(C);         // one input buffer
+  static constexpr size_t smem = XS + 2 * IB + 16;                 // + two mbarriers
+  static_assert(ROWB % 16 == 0, "bulk copies move multiples of 16 bytes");
+  static_assert(XS % 16 == 0 && IB % 16 == 0, "16-byte aligned buffers");
+  static_assert(TH <= 1024, "threads per CTA");
+};
+
+template <typename R, int LX, int V, int NC, int TZ, int MINB>
+__global__ void __launch_bounds__(P3Pipe<R, LX, V, TZ>::TH, MINB)
+    k_mv_pass3p(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int cond, int tz_,
+                int ntz_, R gscale, int op) {
+  grid_dep_begin();
+  typedef typename CT<R>::T C;
+  typedef P3Pipe<R, LX, V, TZ> PP;
+  typedef typename PP::SH::P P;
+  typedef RevPlan<P> Q;
+  static_assert(NC == LX / 2 && NC > 0, "cubic boxes on the (2n)^3 grid");
+  static_assert(LX % TZ == 0, "whole kz tiles");
+  constexpr bool ZH = P::r[0] % 2 == 0;
+  constexpr bool DH = half_store_ok<Q>();
+  static_assert(ZH && DH, "zero-half loads and half stores");
+  constexpr int W = PP::W, NTZ = LX / TZ, NT = LX * NTZ;
+  constexpr long long rs = (long long)LX * LX * 3;          // x-row stride of T2
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* s = reinterpret_cast<C*>(smem_raw);
+  // input buffer b at smem_raw + XS + b IB
+  auto ibuf = [&](int b) -> C* { return reinterpret_cast<C*>(smem_raw + PP::XS + (size_t)b * PP::IB); };
+  uint64_t* mb = reinterpret_cast<uint64_t*>(smem_raw + PP::XS + 2 * PP::IB);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  C* __restrict__ t2 = (C*)S.t2;
+  const C* __restrict__ gh = (const C*)(op ? S.pghat : S.ghat);
+  constexpr int H = (LX / 2 + 1) * (LX / 2 + 1) * (LX / 2 + 1);
+  constexpr int hy = LX / 2 + 1, hz = LX / 2 + 1;
+  const int w = threadIdx.x % W, t = threadIdx.x / W;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    mbar_init(&mb[0], 1);
+    mbar_init(&mb[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  // bulk copies of tile `tile` into buffer b by warp 0 (one row per copy)
+  auto issue = [&](int tile, int b) {
+    const int ky = pencil_ky(tile / NTZ, LX), kz0 = (tile % NTZ) * TZ;
+    if (lane == 0) mbar_arrive_expect_tx(&mb[b], (uint32_t)(NC * PP::ROWB));
+    __syncwarp();
+    const C* src = t2 + ((long long)ky * LX + kz0) * 3;
+    C* dst = ibuf(b);
+    for (int pos = lane; pos < NC; pos += 32) bulk_g2s(dst + pos * W, src + pos * rs, PP::ROWB, &mb[b]);
+  };
+  int tile = blockIdx.x;
+  if (warp == 0 && tile < NT) issue(tile, 0);
+  for (int it = 0; tile < NT; ++it, tile += gridDim.x) {
+    const int b = it & 1;
+    const int next = tile + gridDim.x;
+    // the other buffer was last read by tile it-1, which has passed several
+    // CTA barriers since
+    if (warp == 0 && next < NT) issue(next, b ^ 1);
+    const bool ok_wait = mbar_wait_bounded(&mb[b], (uint32_t)((it >> 1) & 1), 2000000000LL);
+    if (__syncthreads_or(!ok_wait)) {
+      // give up on this instance: flag it, let the other buffer's copies
+      // (if any) land before the CTA's shared memory goes away
+      if (threadIdx.x == 0) {
+        atomicExch(&S.fault, 1);
+        if (next < NT) mbar_wait_bounded(&mb[b ^ 1], (uint32_t)(((it + 1) >> 1) & 1), 2000000000LL);
+      }
+      return;
+    }
+    const int ky = pencil_ky(tile / NTZ, LX), kz0 = (tile % NTZ) * TZ;
+    const C* in = ibuf(b) + w;
+    C* col = t2 + ((long long)ky * LX + kz0) * 3 + w;
+    C* sw = s + w;
+    auto ld = [&](int, int pos) -> C { return in[pos * W]; };
+    auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
+    C a[P::E];
+    rload<P, 1, ZH>(a, t, ld);
+    rstage<P, 0, ZH>(a, t, tw);
+    rrest<P, 1, 0>(a, t, sm, tw);
+    constexpr int RL = P::r[P::S - 1];
+#pragma unroll
+    for (int bb = 0; bb < P::E / RL; ++bb)
+#pragma unroll
+      for (int q = 0; q < RL; ++q) sm(0, ppad(rout_pos<P, P::S - 1>(t, bb, q))) = a[bb * RL + q];
+    __syncthreads();
+    {
+      // thread -> (kzl fastest, mirror pair j), as in k_mv_pass3s
+      const int kzl = threadIdx.x % TZ;
+      constexpr int js = PP::TH / TZ;
+      const int kz = kz0 + kzl;
+      const bool fy = ky > LX / 2, fz = kz > LX / 2;
+      const int my = fy ? LX - ky : ky;
+      const int mz = fz ? LX - kz : kz;
+      const R sd = gscale;
+      const R sxy = fy ? -gscale : gscale, sxz = fz ? -gscale : gscale;
+      const R syz = (fy != fz) ? -gscale : gscale;
+      const C* __restrict__ q0 = gh + my * hz + mz;
+      for (int j = threadIdx.x / TZ; j <= LX / 2; j += js) {
+        const C* q = q0 + j * (hy * hz);
+        const C gxx = cscale(__ldg(q), sd), gxy = cscale(__ldg(q + H), sxy), gxz = cscale(__ldg(q + 2 * H), sxz);
+        const C gyy = cscale(__ldg(q + 3 * H), sd), gyz = cscale(__ldg(q + 4 * H), syz);
+        const C gzz = cscale(__ldg(q + 5 * H), sd);
+        {
+          C* v = s + ppad(j) * W + 3 * kzl;
+          const C a0 = v[0], a1 = v[1], a2 = v[2];
+          v[0] = cadd(cadd(cmul(gxx, a0), cmul(gxy, a1)), cmul(gxz, a2));
+          v[1] = cadd(cadd(cmul(gxy, a0), cmul(gyy, a1)), cmul(gyz, a2));
+          v[2] = cadd(cadd(cmul(gxz, a0), cmul(gyz, a1)), cmul(gzz, a2));
+        }
+        if (j > 0 && j < LX / 2) {
+          C* v = s + ppad(LX - j) * W + 3 * kzl;
+          const C a0 = v[0], a1 = v[1], a2 = v[2];
+          v[0] = csub(csub(cmul(gxx, a0), cmul(gxy, a1)), cmul(gxz, a2));
+          v[1] = cadd(csub(cmul(gyy, a1), cmul(gxy, a0)), cmul(gyz, a2));
+          v[2] = cadd(csub(cmul(gyz, a1), cmul(gxz, a0)), cmul(gzz, a2));
+        }
+      }
+    }
+    __syncthreads();
+    const int ti = opaque(t);
+    C* colo = opaque_ptr(col);
+    C* swo = opaque_ptr(sw);
+    auto smo = [&](int, int pp) -> C& { return swo[pp * W]; };
+    auto stf = [&](int, int pos, C v) { __stcg(colo + pos * rs, cswap(v)); };
+    constexpr int R0 = Q::r[0];
+#pragma unroll
+    for (int bb = 0; bb < Q::E / R0; ++bb)
+#pragma unroll
+      for (int m = 0; m < R0; ++m) a[bb * R0 + m] = cswap(smo(0, ppad(rin_pos<Q, 0>(ti, bb, m))));
+    __syncthreads();
+    rstage<Q, 0>(a, ti, tw);
+    rrest<Q, 1, 0>(a, ti, smo, tw);
+    rstore<Q, 1, DH>(a, ti, stf);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // pass 5: inverse z on nl lines, keep z < nz, fused combine:
 //   MV_AX           y = ia*x - mask*conv        (interaction_mult)
 //   MV_RESIDUAL     y = b - (ia*x - mask*conv)  (b already masked)
@@ -632,6 +788,11 @@ template <typename R> struct MvSet {
   PF kf = nullptr; PI ki = nullptr;
   int cl = 0, thf = 0, gridf = 0;
   size_t smemf = 0, smemi = 0;
+  // staged persistent x pass (cubic sets only): threads, tiles per
+  // instance, dynamic shared memory, CTAs per SM it is built for
+  P3 k3p = nullptr;
+  int th3p = 0, nt3p = 0, minb3p = 1;
+  size_t smem3p = 0;
 };
 
 // General kernels (sizes from Geo), defined with the instantiations.
@@ -708,6 +869,16 @@ void mv_cube_fill(MvSet<R>& o) {
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
   o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
   o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+  if constexpr (sizeof(R) == 4 && V == 0 && (L == 128 || L == 256)) {
+    // complex64 64^3 / 128^3: the staged persistent x pass, same tile shape
+    constexpr int TZ = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+    typedef P3Pipe<R, L, V, TZ> PP;
+    o.k3p = (typename M::P3)k_mv_pass3p<R, L, V, NC, TZ, 2>;
+    o.th3p = PP::TH;
+    o.nt3p = L * (L / TZ);
+    o.minb3p = 2;
+    o.smem3p = PP::smem;
+  }
   if constexpr (sizeof(R) == 4 && L == 128) {
     // complex64 64^3: both fused buffers fit two CTAs per SM
     typedef FusedZY<R, L> F;
@@ -739,6 +910,11 @@ cudaError_t mv_prepare(const void* const* ks, int n);
 // Whether the cluster-fused z/y passes run (DDA_NO_FUSED_ZY=1 turns both
 // off, DDA_NO_FUSED_INV=1 the inverse one only); read at every launch.
 bool fused_zy_enabled(bool inverse);
+// Whether the staged persistent x pass runs where compiled (DDA_NO_P3PIPE=1:
+// the one-tile-per-CTA kernel); read at every launch.
+bool p3_pipe_enabled();
+// Streaming multiprocessors of the current device (cached per device).
+int device_sms();
 
 // Launch on clusters of `cl` CTAs along x, with programmatic stream
 // serialization unless DDA_NO_PDL=1.
@@ -767,9 +943,9 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                           const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
                           const MvFuse& fz = MvFuse()) {
-  const void* ks[7] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
-                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki};
-  cudaError_t e = mv_prepare(ks, 7);
+  const void* ks[8] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
+                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki, (const void*)k.k3p};
+  cudaError_t e = mv_prepare(ks, 8);
   if (e != cudaSuccess) return e;
   // The fused z/y kernels take the place of passes 1+2 / 4+5 in launches of
   // one instance with no Krylov step fused into those passes (cubic sets use
@@ -793,9 +969,17 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                         pc.ntz2)))
       return e;
   }
-  if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond, pc.tz3,
-                      pc.ntz3, (R)gscale, fz.tensor)))
+  if (k.k3p && p3_pipe_enabled()) {
+    // persistent: about minb3p resident CTAs per SM over all instances
+    const int want = (k.minb3p * device_sms() + nb - 1) / nb;
+    const int gx = std::max(1, std::min(k.nt3p, want));
+    if ((e = launch_pdl(k.k3p, dim3((unsigned)gx, nb), dim3(k.th3p), k.smem3p, s, g, twx, st, act, cond, pc.tz3,
+                        pc.ntz3, (R)gscale, fz.tensor)))
+      return e;
+  } else if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond,
+                             pc.tz3, pc.ntz3, (R)gscale, fz.tensor))) {
     return e;
+  }
   if (fi) {
     if ((e = launch_cluster(k.ki, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemi, s, g, twz, st, act,
                             in_id, out_id, mode, cond)))

@@ -410,8 +410,12 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
       }
       I.outer += 1;
       I.bnorm = std::sqrt(p->h_norm[p->n + j]);
-      I.relres = I.bnorm > 0 ? std::sqrt(p->h_norm[j]) / I.bnorm : 0.0;
-      if (I.relres <= I.tol || std::isnan(I.relres)) finish(j, std::isnan(I.relres) ? DDA_ERR_NAN : DDA_OK);
+      // zero right-hand side: P = 0 solves it; NaN / infinite: NaN status
+      I.relres = !std::isfinite(I.bnorm) ? NAN : (I.bnorm > 0 ? std::sqrt(p->h_norm[j]) / I.bnorm : 0.0);
+      if (std::isnan(I.relres)) {
+        I.iters = -I.iters;        // the reference's sign convention for a NaN exit
+        finish(j, DDA_ERR_NAN);
+      } else if (I.relres <= I.tol) finish(j, DDA_OK);
       else if (I.outer >= I.max_outer) finish(j, DDA_NOT_CONVERGED);
       else rearm.push_back(j);
     }

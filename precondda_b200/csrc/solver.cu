@@ -574,7 +574,11 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
   std::vector<double> first_rel(nb, NAN), lowest_rel(nb, NAN);
   for (int j = 0; j < nb; ++j) {
     bnorm[j] = std::sqrt(w128->h_out[j]);
-    if (!(bnorm[j] > 0)) { active[j] = 0; relres[j] = 0.0; }
+    // a zero right-hand side is solved by P = 0; a NaN or infinite one ends
+    // at once with the NaN status (the reference returns -1 there: its first
+    // residual norm is NaN)
+    if (!std::isfinite(bnorm[j])) { active[j] = 0; relres[j] = NAN; total[j] = 1; }
+    else if (!(bnorm[j] > 0)) { active[j] = 0; relres[j] = 0.0; }
   }
   // residual r = b (x = 0)
   for (int j = 0; j < nb; ++j)
@@ -638,8 +642,9 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
   for (int j = 0; j < nb; ++j) {
     if (!res) break;
     dda_result& r = res[j];
-    r.iters = total[j];
     r.status = (relres[j] <= tol) ? DDA_OK : (std::isnan(relres[j]) ? DDA_ERR_NAN : DDA_NOT_CONVERGED);
+    // the reference's sign convention: -(iterations) when the solve ended on NaN
+    r.iters = r.status == DDA_ERR_NAN ? -total[j] : total[j];
     r.lowest_rel = lowest_rel[j];
     r.first_rel = first_rel[j];
     r.true_relres = relres[j];

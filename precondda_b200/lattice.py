@@ -43,12 +43,21 @@ class Sphere(Shape):
 
 
 class Cylinder(Shape):
-    def __init__(self, shape_id, center, radius, height, axis="z", n=1.5, group=None, priority=0):
+    """Cylinder of the given axis.  ``geometric=False`` (the default) keeps
+    the reference's membership test (ddaforgit.py:477-509) bit for bit: the
+    radial distance is taken in the (x, y) plane whatever the axis, and for
+    the x and y axes the height test compares the signed z offset with
+    height/2, so such a cylinder fills its mark_shapes window below
+    z = c_z + height/2.  ``geometric=True`` splits the axes as the axis
+    names say."""
+
+    def __init__(self, shape_id, center, radius, height, axis="z", n=1.5, group=None, priority=0, geometric=False):
         super().__init__(shape_id, n, group, priority)
         self.center = center
         self.radius = radius
         self.height = height
         self.axis = axis
+        self.geometric = bool(geometric)
 
 
 class Ellipsoid(Shape):
@@ -83,30 +92,36 @@ _SHAPES = {"sphere": Sphere, "cylinder": Cylinder, "ellipsoid": Ellipsoid, "rect
 # --------------------------------------------------------------------------
 # polarizability (ddaforgit.py:403-437)
 # --------------------------------------------------------------------------
+# lattice-dispersion-relation coefficients (Draine & Goodman 1993)
+_LDR_B = (-1.891531, 0.1648469, -1.7700004)
+
+
 def calculate_alpha(refractive_index, lattice_spacing, wave_number, incident_direction=None,
                     polarization_direction=None, method="LDR"):
     """Clausius-Mossotti polarizability with optional radiative-reaction (RR)
     or lattice-dispersion-relation (LDR) correction; LDR keeps the reference's
-    S = (a.e)^2 (ddaforgit.py:432)."""
-    n = np.complex128(refractive_index)
+    S = (a.e)^2 (ddaforgit.py:432).  Each formula is evaluated in the
+    reference's operation order (ddaforgit.py:403-437), so the values agree
+    bit for bit."""
+    m = np.complex128(refractive_index)
     d = np.float64(lattice_spacing)
     k = np.float64(wave_number)
-    eps = n ** 2
-    alpha_cm = (3 * d ** 3 / (4 * np.pi)) * (eps - 1) / (eps + 2)
+    eps = m ** 2
+    cm = (3 * d ** 3 / (4 * np.pi)) * (eps - 1) / (eps + 2)
     if method == "CM":
-        return alpha_cm
-    rr_term = (2 / 3) * 1j * (k * d) ** 3
+        return cm
+    radiative = (2 / 3) * 1j * (k * d) ** 3
     if method == "RR":
-        return alpha_cm / (1 + (alpha_cm / d ** 3) * (-rr_term))
+        return cm / (1 + (cm / d ** 3) * (-radiative))
     if method == "LDR":
         if incident_direction is None or polarization_direction is None:
             raise ValueError("incident_direction and polarization_direction required for LDR method")
-        a = np.asarray(incident_direction, dtype=np.float64)
-        e = np.asarray(polarization_direction, dtype=np.float64)
-        b1, b2, b3 = -1.891531, 0.1648469, -1.7700004
-        S = np.sum(np.dot(a, e) ** 2)
-        ldr_term = (b1 + n ** 2 * b2 + n ** 2 * b3 * S) * (k * d) ** 2
-        return alpha_cm / (1 + (alpha_cm / d ** 3) * (ldr_term - rr_term))
+        a_hat = np.asarray(incident_direction, dtype=np.float64)
+        e_hat = np.asarray(polarization_direction, dtype=np.float64)
+        b1, b2, b3 = _LDR_B
+        S = np.sum(np.dot(a_hat, e_hat) ** 2)
+        dispersion = (b1 + m ** 2 * b2 + m ** 2 * b3 * S) * (k * d) ** 2
+        return cm / (1 + (cm / d ** 3) * (dispersion - radiative))
     raise ValueError("method must be 'CM', 'RR', or 'LDR'")
 
 
@@ -143,10 +158,17 @@ def _axis_split(p, center, axis):
     return p[:, o], np.asarray(center)[o], p[:, ax], np.asarray(center)[ax]
 
 
-def inside_cylinder(p, center, radius, height, axis="z", eps=EPS):
-    p2, c2, h, ch = _axis_split(p, center, axis)
-    rd = np.sqrt(((p2 - c2) ** 2).sum(-1))
-    dz = np.abs(h - ch)
+def inside_cylinder(p, center, radius, height, axis="z", eps=EPS, geometric=False):
+    if geometric:
+        p2, c2, h, ch = _axis_split(p, center, axis)
+        rd = np.sqrt(((p2 - c2) ** 2).sum(-1))
+        dz = np.abs(h - ch)
+    else:
+        # the reference's form: radial distance in (x, y) for every axis;
+        # signed z offset in the height test of the x and y axes
+        off = p - np.asarray(center, dtype=np.float64)
+        rd = np.sqrt(off[:, 0] * off[:, 0] + off[:, 1] * off[:, 1])
+        dz = np.abs(off[:, 2]) if axis == "z" else off[:, 2]
     hh = height / 2
     inr = rd <= radius
     onr = np.abs(rd - radius) < eps
@@ -191,7 +213,8 @@ def shape_membership(shape, points):
     if isinstance(shape, Rectangle):
         return inside_rectangle(points, shape.center, shape.dimensions)
     if isinstance(shape, Cylinder):
-        return inside_cylinder(points, shape.center, shape.radius, shape.height, shape.axis)
+        return inside_cylinder(points, shape.center, shape.radius, shape.height, shape.axis,
+                               geometric=getattr(shape, "geometric", False))
     if isinstance(shape, Prism):
         return inside_prism(points, shape.center, shape.radius, shape.height, shape.sides, shape.axis)
     raise ValueError(f"Unsupported shape type: {type(shape)}")
@@ -401,9 +424,25 @@ def ellipsoid_occupancy(box, semi_axes_d, rotation=None):
 # --------------------------------------------------------------------------
 # device builders: the same lattice built by the engine's kernels
 # --------------------------------------------------------------------------
-def _shape_struct(s, inv_alpha):
+def _reference_window(s, d, box, shift=(0, 0, 0)):
+    """mark_shapes' index window of shape s (ddaforgit.py:626-649) in the
+    site indices of a box whose site 0 is the reference grid's site ``shift``."""
+    c = np.array(s.center, dtype=np.float64)
+    mg = int(float(_max_dist(s) + EPS) / d) + 1
+    ci = (c / d).astype(int)
+    lo = [max(0, int(ci[a]) - mg - shift[a]) for a in range(3)]
+    hi = [min(int(box[a]), int(ci[a]) + mg + 1 - shift[a]) for a in range(3)]
+    return lo, hi
+
+
+def _shape_struct(s, inv_alpha, window=None):
     from . import _lib as L
     st = L.dda_shape()
+    if window is not None:
+        lo, hi = window
+        st.flags |= L.SHAPE_WINDOW
+        for a in range(3):
+            st.win[2 * a], st.win[2 * a + 1] = int(lo[a]), int(hi[a])
     st.inv_alpha[0], st.inv_alpha[1] = float(np.real(inv_alpha)), float(np.imag(inv_alpha))
     for i in range(9):
         st.rot[i] = 1.0 if i in (0, 4, 8) else 0.0
@@ -426,6 +465,8 @@ def _shape_struct(s, inv_alpha):
             st.p[i] = float(s.dimensions[i])
     elif isinstance(s, Cylinder):
         st.type, st.p[0], st.p[1], st.axis = L.SHAPE_CYLINDER, float(s.radius), float(s.height), ax[s.axis]
+        if getattr(s, "geometric", False):
+            st.flags |= L.SHAPE_GEOMETRIC_AXES
     elif isinstance(s, Prism):
         st.type, st.p[0], st.p[1] = L.SHAPE_PRISM, float(s.radius), float(s.height)
         st.axis, st.sides = ax[s.axis], int(s.sides)
@@ -434,10 +475,13 @@ def _shape_struct(s, inv_alpha):
     return st
 
 
-def voxelize_device(shapes, inv_alphas, box, d, origin=(0.0, 0.0, 0.0), dtype=None, device=None):
+def voxelize_device(shapes, inv_alphas, box, d, origin=(0.0, 0.0, 0.0), dtype=None, device=None, window=True):
     """inv_alpha (nx,ny,nz) on the device: voxel centres origin + (i+0.5) d,
     each site takes the inverse polarizability of the last shape containing
-    it (the reference's mark_shapes order), 0 elsewhere."""
+    it (the reference's mark_shapes order), 0 elsewhere.  ``window`` limits
+    each shape to the index window mark_shapes evaluates it on (origin taken
+    as a whole number of spacings); it bounds the reference's x- and y-axis
+    cylinders and changes no other shape."""
     import ctypes as C
     import torch
     from . import _lib as L
@@ -445,7 +489,9 @@ def voxelize_device(shapes, inv_alphas, box, d, origin=(0.0, 0.0, 0.0), dtype=No
     dtype = dtype or torch.complex128
     dev = _device(device)
     n = len(shapes)
-    arr = (L.dda_shape * n)(*[_shape_struct(s, a) for s, a in zip(shapes, inv_alphas)])
+    shift = [int(round(float(o) / d)) for o in origin]
+    wins = [_reference_window(s, d, box, shift) if window else None for s in shapes]
+    arr = (L.dda_shape * n)(*[_shape_struct(s, a, w) for s, a, w in zip(shapes, inv_alphas, wins)])
     out = torch.empty(tuple(int(b) for b in box), dtype=dtype, device=dev)
     org = (C.c_double * 3)(*[float(v) for v in origin])
     ctx = L.context(dev.index)
@@ -453,6 +499,14 @@ def voxelize_device(shapes, inv_alphas, box, d, origin=(0.0, 0.0, 0.0), dtype=No
         L.check(L.lib().dda_voxelize(ctx.handle, _dt_code(dtype), arr, n, *out.shape, float(d), org,
                                      out.data_ptr(), stream_handle(dev)))
     return out
+
+
+def mark_shapes_device(grid_shape, lattice_spacing, shapes, values="value", device=None):
+    """mark_shapes (ddaforgit.py:615-661) on the device: the value (or the
+    refractive index, values="n") of the last shape containing each voxel
+    centre, within each shape's index window; complex128 (nx,ny,nz)."""
+    vals = [s.value if values == "value" else s.n for s in shapes]
+    return voxelize_device(shapes, vals, grid_shape, lattice_spacing, device=device)
 
 
 def incident_field_device(box, d, k_vec, polarization, dtype=None, device=None):

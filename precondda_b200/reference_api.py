@@ -91,22 +91,86 @@ def _inv_alpha_box(alpha_inv, nx, ny, nz, dt, dev):
     return t.reshape(nx, ny, nz)
 
 
-def _check_mask(mask, ia):
-    if mask is None:
-        return
-    m = as_device(mask, torch.bool, ia.device).reshape(ia.shape) if not isinstance(mask, torch.Tensor) \
-        else mask.to(ia.device).reshape(ia.shape).bool()
-    if not torch.equal(m, ia != 0):
-        raise ValueError("mask must equal (inv_alpha != 0), as prepare_interaction_matrices builds it")
+def _mask_tensor(mask, ia):
+    if isinstance(mask, torch.Tensor):
+        return mask.to(ia.device).reshape(ia.shape).bool()
+    return as_device(mask, torch.bool, ia.device).reshape(ia.shape)
 
 
-def _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dt):
+# Operators built from the reference's arrays, cached so that a caller who
+# loops on interaction_mult / solve_gpbicgstab with the same device arrays
+# (as the reference's callers do) pays the octant layout conversion, the
+# scratch allocation and the mask check once.  Only arrays the engine reads
+# in place (device arrays of the compute dtype) are cached, keyed by address,
+# shape, dtype and torch's in-place version counter; an entry keeps those
+# arrays alive, so an address cannot be reused while it is cached.  Arrays
+# changed in place by a library other than torch between calls are not
+# detected: pass new arrays, or call clear_operator_cache().
+_OP_CACHE: "OrderedDict" = None
+_OP_CACHE_SIZE = 4
+
+
+def clear_operator_cache():
+    """Drop every cached operator."""
+    global _OP_CACHE
+    _OP_CACHE = None
+
+
+def _in_place(orig, t):
+    """Whether the device tensor t reads orig's memory (no copy was made)."""
+    if isinstance(orig, torch.Tensor):
+        return orig.is_cuda and orig.data_ptr() == t.data_ptr()
+    cai = getattr(orig, "__cuda_array_interface__", None)
+    return cai is not None and cai["data"][0] == t.data_ptr()
+
+
+def _key(t):
+    return (t.data_ptr(), tuple(t.shape), t.dtype, t._version)
+
+
+def _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dt, mask=None, ia_tag=None, hold=None):
+    """Operator of the reference's arrays (cached, see above).  ia_tag, when
+    given, identifies inv_alpha in the cache instead of its address (for
+    arrays the wrapper derives itself from a mask or a constant); ``hold``
+    is kept alive with the entry (the array the tag's address belongs to)."""
+    global _OP_CACHE
+    from collections import OrderedDict
     dev = _device()
-    ia = _inv_alpha_box(alpha_inv, nx, ny, nz, dt, dev)
     G = as_device(interaction_matrix, dt, dev)
     if tuple(G.shape) != _reference_octant_dims(nx, ny, nz):
         raise ValueError(f"interaction matrix shape {tuple(G.shape)} != {_reference_octant_dims(nx, ny, nz)}")
-    return DDAOperator(ia, 1.0, 1.0, dtype=dt, L_=(2 * nx, 2 * ny, 2 * nz), ghat=G, device=dev)
+    if ia_tag is not None and _OP_CACHE is not None and _in_place(interaction_matrix, G):
+        ent = _OP_CACHE.get((_key(G), ia_tag, (nx, ny, nz), dt))
+        if ent is not None:
+            return ent["op"]
+    ia = _inv_alpha_box(alpha_inv() if callable(alpha_inv) else alpha_inv, nx, ny, nz, dt, dev)
+    if ia_tag is not None:
+        cacheable = _in_place(interaction_matrix, G)
+        key = (_key(G), ia_tag, (nx, ny, nz), dt) if cacheable else None
+    else:
+        cacheable = _in_place(interaction_matrix, G) and _in_place(alpha_inv, ia)
+        key = (_key(G), _key(ia), (nx, ny, nz), dt) if cacheable else None
+    if _OP_CACHE is None:
+        _OP_CACHE = OrderedDict()
+    ent = _OP_CACHE.get(key) if key is not None else None
+    if ent is None:
+        op = DDAOperator(ia, 1.0, 1.0, dtype=dt, L_=(2 * nx, 2 * ny, 2 * nz), ghat=G, device=dev)
+        ent = {"op": op, "arrays": (G, ia, hold), "mask": None}
+        if key is not None:
+            _OP_CACHE[key] = ent
+            while len(_OP_CACHE) > _OP_CACHE_SIZE:
+                _OP_CACHE.popitem(last=False)
+    elif key is not None:
+        _OP_CACHE.move_to_end(key)
+    if mask is not None:
+        m = _mask_tensor(mask, ent["op"].inv_alpha)
+        mk = _key(m) if _in_place(mask, m) else None
+        if mk is None or mk != ent["mask"]:
+            if not torch.equal(m, ent["op"].inv_alpha != 0):
+                raise ValueError("mask must equal (inv_alpha != 0), as prepare_interaction_matrices builds it")
+            ent["mask"] = mk
+            ent["mask_ref"] = m
+    return ent["op"]
 
 
 def interaction_mult(in_array, out_array, interaction_matrix, alpha_inv, mask, chunk_params, nx, ny, nz,
@@ -114,8 +178,7 @@ def interaction_mult(in_array, out_array, interaction_matrix, alpha_inv, mask, c
     """A.x = alpha_inv*x - mask*conv(x) (Gpbicgstab.py:828-830), flattened
     to 3N like the reference.  out_array and chunk_params are accepted and
     ignored (the engine needs no chunking)."""
-    op = _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dtype)
-    _check_mask(mask, op.inv_alpha)
+    op = _op_from_reference(interaction_matrix, alpha_inv, nx, ny, nz, dtype, mask)
     return op.matvec(in_array).reshape(-1)
 
 
@@ -123,8 +186,10 @@ def fft_matvec(in_array, out_array, matrix, mask, chunk_params, nx, ny, nz, dtyp
     """mask * IFFT[Ghat FFT(pad x)] cropped (Gpbicgstab.py:742-772), 3N flat."""
     dev = _device()
     m = as_device(mask, torch.bool, dev).reshape(nx, ny, nz)
-    ia = torch.where(m, torch.ones((), dtype=dtype, device=dev), torch.zeros((), dtype=dtype, device=dev))
-    op = _op_from_reference(matrix, ia, nx, ny, nz, dtype)
+    tag = ("mask",) + _key(m) if _in_place(mask, m) else None
+    op = _op_from_reference(matrix, lambda: torch.where(m, torch.ones((), dtype=dtype, device=dev),
+                                                        torch.zeros((), dtype=dtype, device=dev)),
+                            nx, ny, nz, dtype, ia_tag=tag, hold=m)
     return op.conv_masked(in_array).reshape(-1)
 
 
@@ -159,8 +224,8 @@ def E_field_solver(polarization, interaction_matrix, grid_size, dtype=_C64):
     if size != expected:
         raise ValueError(f"Polarization size {size} doesn't match expected size {expected}")
     dev = _device()
-    ones = torch.ones((nx, ny, nz), dtype=dtype, device=dev)
-    op = _op_from_reference(interaction_matrix, ones, nx, ny, nz, dtype)
+    op = _op_from_reference(interaction_matrix, lambda: torch.ones((nx, ny, nz), dtype=dtype, device=dev),
+                            nx, ny, nz, dtype, ia_tag=("ones",))
     return op.conv(polarization)
 
 
@@ -180,8 +245,7 @@ def solve_gpbicgstab(grid_size, inv_alpha, interaction_matrix, preconditioner, E
     if is_2d:
         raise NotImplementedError("the 2D preconditioned path is not part of the engine")
     nx, ny, nz = grid_size
-    op = _op_from_reference(interaction_matrix, inv_alpha, nx, ny, nz, dtype)
-    _check_mask(mask, op.inv_alpha)
+    op = _op_from_reference(interaction_matrix, inv_alpha, nx, ny, nz, dtype, mask)
     pre = _pre_from_reference(preconditioner, op.inv_alpha.to(_C128)) if precon else None
     P, info = op.solve(E_inc, tol=target, max_iter=max_iter, ratio=ratio, preconditioner=pre)
     return info.iters, P, info.lowest_rel, info.first_rel

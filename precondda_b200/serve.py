@@ -344,12 +344,15 @@ class DDAServer:
             raise ValueError("inv_alpha must have shape (nx, ny, nz)")
         req.shape = shape
         req.bucket = self.bucket_for(shape)
+        # the bucket's pool first: a request its budget cannot hold is refused
+        # (MemoryError) before anything is allocated or registered
+        b = self._bucket(req.bucket)
         req.rid = self._next
         self._next += 1
         req.t_submit = time.perf_counter()
         if self.precondition and req.pre_key is not None:
             self._pre.setdefault(req.pre_key, [None, 0])[1] += 1
-        self._bucket(req.bucket).queue.append(req)
+        b.queue.append(req)
         return req
 
     def _preconditioner(self, req, ia, L_):

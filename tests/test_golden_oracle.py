@@ -147,3 +147,49 @@ def test_precondition_apply_is_the_dense_circulant_inverse():
     xp[:shape[0], :shape[1], :shape[2]] = x
     y = (Ci @ xp.reshape(-1)).reshape(L + (3,))[:shape[0], :shape[1], :shape[2]] * occ[..., None]
     assert _rel(O.precondition_apply(x, pre, occ), y) < 1e-10
+
+
+SHAPES = os.path.join(os.path.dirname(__file__), "golden", "shape_fixtures.npz")
+
+
+def _shape_cases():
+    import json
+    with open(SHAPES.replace(".npz", ".json")) as f:
+        cases = json.load(f)["cases"]
+    out = []
+    for name, c in cases.items():
+        shapes = []
+        for s in c["shapes"]:
+            s = dict(s)
+            if isinstance(s["n"], str):
+                s["n"] = complex(s["n"])
+            shapes.append(s)
+        out.append((name, shapes, c))
+    return out
+
+
+@pytest.mark.parametrize("name,shapes,case", _shape_cases(), ids=[c[0] for c in _shape_cases()])
+def test_shape_lattices_match_reference(name, shapes, case):
+    """Rectangle, cylinder (every axis, with the reference's own x/y-axis
+    handling) and prism lattices, site for site, against the reference's
+    build_problem_from_shapes (tests/golden/make_shape_fixtures.py)."""
+    from precondda_b200 import build_problem_from_shapes
+    ref = np.load(SHAPES)[f"{name}_alpha"]
+    pr = build_problem_from_shapes(shapes, np.array(case["k_direction"]), case["polarization"],
+                                   case["wavelength"], case["spacing"])
+    assert pr["alpha_array"].shape == ref.shape
+    assert np.array_equal(pr["alpha_array"], ref)
+
+
+def test_geometric_cylinder_flag_differs_from_reference_axes():
+    """geometric=True is the axis-true cylinder; the default reproduces the
+    reference (which fills the window below c_z + h/2 for the x/y axes)."""
+    from precondda_b200.lattice import Cylinder, inside_cylinder
+    pts = np.stack(np.meshgrid(*[np.arange(-10, 10) + 0.5] * 3, indexing="ij"), -1).reshape(-1, 3)
+    ref = inside_cylinder(pts, (0, 0, 0), 4.0, 6.0, "x")
+    geo = inside_cylinder(pts, (0, 0, 0), 4.0, 6.0, "x", geometric=True)
+    assert ref.sum() != geo.sum()
+    # geometric x-axis cylinder: |x| <= 3 and y^2 + z^2 <= 16
+    exp = (np.abs(pts[:, 0]) <= 3.0) & (pts[:, 1] ** 2 + pts[:, 2] ** 2 <= 16.0)
+    assert np.array_equal(geo, exp)
+    assert Cylinder("c", (0, 0, 0), 1, 1, "y").geometric is False

@@ -99,6 +99,34 @@ def test_cubic_kernels_launch_and_match_general(n, dtype, tol, monkeypatch):
     assert _rel(cube, general) < tol
 
 
+@pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
+def test_staged_x_pass_equals_one_tile_kernel(n, nb, monkeypatch):
+    """The staged persistent x pass (bulk-copied input tiles, one tile
+    ahead) does the arithmetic of the one-tile-per-CTA kernel: equal bit for
+    bit, alone and in batched launches (several instances per launch), in
+    the interaction and preconditioner products."""
+    P = _pkg()
+    ops, xs = [], []
+    for j in range(nb):
+        k, d, alpha, x = _rand_problem((n,) * 3, seed=n + j, fill=0.5)
+        ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+        ops.append(P.DDAOperator(ia, k, d, dtype=C64))
+        xs.append(torch.as_tensor(x, device="cuda").to(C64))
+    monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
+    a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    monkeypatch.setenv("DDA_NO_P3PIPE", "1")
+    b = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    for u, v in zip(a, b):
+        assert torch.equal(u, v)
+    if nb == 1 and n == 64:
+        pre = ops[0].preconditioner()
+        monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
+        pa = pre.apply(xs[0], C64)
+        monkeypatch.setenv("DDA_NO_P3PIPE", "1")
+        pb = pre.apply(xs[0], C64)
+        assert torch.equal(pa, pb)
+
+
 def test_matvec_dense_tiny():
     P = _pkg()
     k, d, alpha, x = _rand_problem((4, 4, 4), seed=3)
@@ -223,10 +251,12 @@ def test_device_voxelizer_matches_host_membership():
     shapes = [Rectangle("r", (0.7, 0.6, 0.5), (0.6, 0.5, 0.4), 1.5),
               Ellipsoid("e", (0.75, 0.65, 0.55), (0.5, 0.35, 0.25), 1.7, rotation=R),
               Cylinder("c", (0.5, 0.7, 0.5), 0.2, 0.5, "y", 1.4),
+              Cylinder("g", (0.6, 0.5, 0.6), 0.15, 0.45, "x", 1.45, geometric=True),
               Prism("p", (1.0, 0.6, 0.6), 0.2, 6, 0.4, 1.3, axis="x"),
               Sphere("s", (0.4, 0.4, 0.4), 0.23, 1.6)]
-    vals = [1.0 + 0.5j, 2.0 - 1.0j, 3.0 + 0.25j, 4.0, 5.0 - 0.125j]
-    got = voxelize_device(shapes, vals, box, d).cpu().numpy()
+    vals = [1.0 + 0.5j, 2.0 - 1.0j, 3.0 + 0.25j, 3.5 + 1j, 4.0, 5.0 - 0.125j]
+    # whole-box membership (no mark_shapes window)
+    got = voxelize_device(shapes, vals, box, d, window=False).cpu().numpy()
     pts = O.voxel_centres(box, d).reshape(-1, 3)
     ref = np.zeros(box, np.complex128).reshape(-1)
     for s, v in zip(shapes, vals):
