@@ -37,6 +37,7 @@ DDAFORGIT_DEFS = (
     "calculate_alpha", "sphere", "ellipsoid", "rectangle", "cylinder", "prism", "create_shape_data",
     "shape_calculators", "mark_shapes", "mark_shapes_n", "create_alpha_and_n_arrays", "trim_zero_faces",
     "greens_kernel_single", "greens_kernel_double", "generate_interaction_row", "build_problem_from_shapes",
+    "save_results_to_file",
 )
 
 

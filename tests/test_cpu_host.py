@@ -192,3 +192,37 @@ def test_results_file_layout(tmp_path):
     assert "Iterations: 17" in txt and "Final norm: 3.200000e-07" in txt and "Status: Converged" in txt
     assert "Polarization array shape: (2, 3, 4, 3)" in txt and "C_sca: 7.500000000e-01" in txt
     assert np.array_equal(np.load(files[1]), P)
+
+
+def test_result_files_match_reference(tmp_path):
+    """save_results_to_file against the reference's own writer
+    (tests/golden/make_results_fixture.py): every line but the time stamp,
+    and the polarisation arrays exactly."""
+    import json
+    import sys as _sys
+    from precondda_b200 import build_problem_from_shapes
+    from precondda_b200.results import save_results_to_file
+    gold = os.path.join(os.path.dirname(__file__), "golden", "ref_results")
+    _sys.path.insert(0, os.path.join(os.path.dirname(__file__), "golden"))
+    import make_results_fixture as M
+    with open(os.path.join(gold, "cases.json")) as f:
+        meta = json.load(f)
+    pr = build_problem_from_shapes(M.SHAPES, np.array(meta["k_direction"]), meta["polarization"],
+                                   meta["wavelength"], meta["spacing"])
+    assert list(pr["grid_size"]) == meta["grid_size"]
+    P = M.polarization(tuple(pr["grid_size"]))
+    for name, c in M.CASES.items():
+        fn = str(tmp_path / f"{name}.txt")
+        save_results_to_file(fn, pr, np.array(c["prediction"]), M.SHAPES, (c["iterations"], P, c["final_norm"]))
+        got = open(fn).read().splitlines()
+        ref = open(os.path.join(gold, f"{name}.txt")).read().splitlines()
+        assert len(got) == len(ref), name
+        for g, r in zip(got, ref):
+            if r.startswith("Results saved on:"):
+                continue
+            if r.startswith("Full polarization array saved to:"):
+                assert os.path.basename(g.split(": ", 1)[1]) == os.path.basename(r.split(": ", 1)[1])
+                continue
+            assert g == r, (name, g, r)
+        assert np.array_equal(np.load(fn.replace(".txt", "_polarization.npy")),
+                              np.load(os.path.join(gold, f"{name}_polarization.npy")))
