@@ -380,6 +380,11 @@ def run_ours(args, ws, rank, local):
     # preconditioner on the operator's grid, built once per geometry like the
     # Green octant (inside the e2e step below)
     pre = op.preconditioner()
+    # launch variants of the buckets the timed work runs, measured before it
+    from precondda_b200.batch import LaunchTuner
+    tuner = LaunchTuner(device=dev)
+    tuner.tune(op.shape, op.L, torch.complex64, 2)
+    tuner.tune((128,) * 3, (256,) * 3, torch.complex64, 16)
 
     def step(precision="mixed", preconditioner=pre, tol=TOL):
         return P.solve_many([op, op], Es_dev, tol=tol, max_iter=MAX_ITER, ratio=RATIO, precision=precision,
@@ -516,7 +521,9 @@ def run_ours(args, ws, rank, local):
                          "algorithmic_bytes": Bb}
             del opb
         del flush
-        out = {"north_star_128": north_star_128(dev), "config1_plain_32": config1_plain(dev)}
+        out = {"north_star_128": north_star_128(dev), "config1_plain_32": config1_plain(dev),
+               "launch_tuning": {json.dumps(list(k)): {"flags": v, "seconds": tuner.times.get(k)}
+                                 for k, v in tuner.best.items()}}
         out.update({"roofline": roof, "matvec_128": big, "plain_c128_solves_per_s": plain,
                "mixed_over_plain": value / ws / plain,
                "unpreconditioned": {"mixed_solves_per_s": mixed_np, "plain_c128_solves_per_s": plain_np,
@@ -703,7 +710,14 @@ def run_batch64(args, ws, rank, local):
     rng = np.random.default_rng(40 + rank)
     specs = [random_ellipsoid_spec(rng) for _ in range(args.geometries)]
     tuner = PaddingTuner("mixed", device=dev)
-    tuner.plan([tuple(s["box"]) for s in specs])          # autotune outside the timed region
+    plan = tuner.plan([tuple(s["box"]) for s in specs])   # autotune outside the timed region
+    from precondda_b200.batch import LaunchTuner
+    ltun = LaunchTuner(device=dev)
+    per_bucket = {}
+    for s_, (box, L_) in zip(specs, plan):
+        per_bucket[(box, L_)] = per_bucket.get((box, L_), 0) + len(s_["dirs"]) * s_.get("pols", 2)
+    for (box, L_), nrhs in per_bucket.items():
+        ltun.tune(box, L_, torch.complex64, nrhs)
     # untimed warm-up: every geometry's bucket with one right-hand side, so the
     # timed pass does not pay first launches of its kernel sizes, pool graph
     # captures or the memory pool's first growth
@@ -770,99 +784,127 @@ def run_batch64(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def serve_stream(srv, stream, dev, tol=1e-5):
+    """Replay one Poisson stream through the server: each request's
+    right-hand sides are submitted at its arrival time as lazy requests (the
+    lattice and incident fields are built on the device when a request
+    enters a slot, once per request group), steps run until all finish.
+    Returns (groups {q: (arrival, [Request])}, wall seconds)."""
+    import torch
+    from precondda_b200.serve import Request
+    from precondda_b200.workloads import build_geometry
+    groups = {}
+    t0 = time.perf_counter()
+    q = 0
+    while q < len(stream) or srv.pending():
+        now = time.perf_counter() - t0
+        while q < len(stream) and stream[q][0] <= now:
+            arr, sp = stream[q]
+            cache = {}
+
+            def make(j, sp=sp, cache=cache):
+                def build():
+                    if "geo" not in cache:
+                        cache["geo"] = build_geometry(sp, dev)
+                    ia, k_, d_, Es = cache["geo"]
+                    E = Es[j]
+                    cache["left"] = cache.get("left", len(Es)) - 1
+                    if cache["left"] == 0:
+                        cache.clear()
+                    return ia, E
+                return build
+
+            lam, m = sp["wavelength"], sp["m"]
+            k = 2 * math.pi / lam
+            d = sp["mkd"] / (abs(m) * k)
+            reqs = []
+            n_rhs = len(sp["dirs"]) * (len(sp["fixed_pols"]) if "fixed_pols" in sp else sp.get("pols", 2))
+            for j in range(n_rhs):
+                r = srv.submit(Request(inv_alpha=None, E_inc=None, k=k, d=d, tol=tol, shape=tuple(sp["box"]),
+                                       build=make(j), pre_key=("group", q)))
+                r.t_submit = t0 + arr
+                reqs.append(r)
+            groups[q] = (t0 + arr, reqs)
+            q += 1
+        if srv.pending():
+            for r in srv.step():
+                r.P = r.inv_alpha = r.E_inc = None          # results are not kept
+        elif q < len(stream):
+            time.sleep(min(1e-3, max(0.0, stream[q][0] - now)))
+    torch.cuda.synchronize()
+    return groups, time.perf_counter() - t0
+
+
+def serve_summary(groups, span):
+    lat_req = np.array([max(r.t_done for r in reqs) - ta for ta, reqs in groups.values()])
+    rhs = [r for _, reqs in groups.values() for r in reqs]
+    lat_rhs = np.array([r.t_done - r.t_submit for r in rhs])
+    return {"requests": len(groups), "rhs": len(rhs), "seconds": span, "rhs_per_s": len(rhs) / span,
+            "requests_per_s": len(groups) / span,
+            "request_p50_ms": float(np.percentile(lat_req, 50) * 1e3),
+            "request_p99_ms": float(np.percentile(lat_req, 99) * 1e3),
+            "rhs_p50_ms": float(np.percentile(lat_rhs, 50) * 1e3),
+            "rhs_p99_ms": float(np.percentile(lat_rhs, 99) * 1e3),
+            "converged": sum(r.info.status == "converged" for r in rhs)}, rhs
+
+
 def run_serve(args, ws, rank, local):
-    """Poisson request stream (20/s), 40% spheres, 40% ellipsoids, 20%
-    random-walk aggregates, boxes 16^3-128^3, 1-16 incidences each, served
-    by continuous batching with HBM admission and Green-tensor reuse."""
+    """Poisson request streams, 40% spheres, 40% ellipsoids, 20% random-walk
+    aggregates, boxes 16^3-128^3, 1-16 incidences each, served by continuous
+    batching with HBM admission and Green-tensor reuse.  One stream per
+    offered rate in --rates (the value and latency keys are the last rate's;
+    every rate's solves/s and p50/p99 go in the "curve" key)."""
     import torch
     from precondda_b200 import _lib as L
     from precondda_b200.serve import DDAServer, Request
     from precondda_b200.workloads import serving_stream, build_geometry
     dev = torch.device("cuda", local)
-    stream = serving_stream(50 + rank, rate=args.rate, duration=args.duration)
+    rates = [float(v) for v in str(args.rates).split(",")] if args.rates else [args.rate]
+    from precondda_b200.batch import LaunchTuner
     srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=args.chunk, device=dev,
-                    precondition=not args.no_precondition)
+                    precondition=not args.no_precondition, launch_tuner=LaunchTuner(device=dev))
     # warm the kernels of every bucket outside the timed region
-    warm = sorted({srv.bucket_for(sp["box"]) for _, sp in stream})
+    warm = sorted({srv.bucket_for(sp["box"]) for r in rates
+                   for _, sp in serving_stream(50 + rank, rate=r, duration=args.duration)})
     for b in warm:
         ia, k, d, Es = build_geometry({"kind": "sphere", "box": (b, b, b), "radius_d": b / 2.0, "m": 1.5 + 0.01j,
                                        "wavelength": 0.5, "mkd": 0.5, "dirs": np.array([[0.0, 0.0, 1.0]]),
                                        "pols": 1}, dev)
         srv.submit(Request(inv_alpha=ia, E_inc=Es[0], k=k, d=d, tol=1e-5))
     srv.drain()
-    srv.done.clear()
-    srv.green.hits = srv.green.misses = 0
-    torch.cuda.synchronize()
+    curve = []
     lc0 = L.lib().dda_kernel_launches()
-    groups = {}
     with ClockSampler(dev.index) as clk:
-        barrier(ws)
-        t0 = time.perf_counter()
-        q = 0
-        while q < len(stream) or srv.pending():
-            now = time.perf_counter() - t0
-            while q < len(stream) and stream[q][0] <= now:
-                arr, sp = stream[q]
-                # lazy requests: the lattice and incident fields are built on
-                # the device when a request enters a slot (the lattice once
-                # per request group), so the queue holds no device memory
-                cache = {}
-
-                def make(j, sp=sp, cache=cache):
-                    def build():
-                        if "geo" not in cache:
-                            cache["geo"] = build_geometry(sp, dev)
-                        ia, k_, d_, Es = cache["geo"]
-                        E = Es[j]
-                        cache["left"] = cache.get("left", len(Es)) - 1
-                        if cache["left"] == 0:
-                            cache.clear()
-                        return ia, E
-                    return build
-
-                lam, m = sp["wavelength"], sp["m"]
-                k = 2 * math.pi / lam
-                d = sp["mkd"] / (abs(m) * k)
-                reqs = []
-                n_rhs = len(sp["dirs"]) * (len(sp["fixed_pols"]) if "fixed_pols" in sp else sp.get("pols", 2))
-                for j in range(n_rhs):
-                    r = srv.submit(Request(inv_alpha=None, E_inc=None, k=k, d=d, tol=1e-5, shape=tuple(sp["box"]),
-                                           build=make(j), pre_key=("group", q)))
-                    r.t_submit = t0 + arr
-                    reqs.append(r)
-                groups[q] = (t0 + arr, reqs)
-                q += 1
-            if srv.pending():
-                for r in srv.step():
-                    r.P = r.inv_alpha = r.E_inc = None          # results are not kept
-            elif q < len(stream):
-                time.sleep(min(1e-3, max(0.0, stream[q][0] - now)))
-        torch.cuda.synchronize()
-        span = time.perf_counter() - t0
+        for rate in rates:
+            srv.done.clear()
+            srv.green.hits = srv.green.misses = 0
+            stream = serving_stream(50 + rank, rate=rate, duration=args.duration)
+            torch.cuda.synchronize()
+            barrier(ws)
+            groups, span = serve_stream(srv, stream, dev)
+            summ, rhs = serve_summary(groups, span)
+            summ.update({"offered_requests_per_s": rate, "green_hits": srv.green.hits,
+                         "green_misses": srv.green.misses})
+            curve.append(summ)
     launches = L.lib().dda_kernel_launches() - lc0
     if rank != 0:
         return
-    lat_req = np.array([max(r.t_done for r in reqs) - ta for ta, reqs in groups.values()])
-    rhs = [r for _, reqs in groups.values() for r in reqs]
-    lat_rhs = np.array([r.t_done - r.t_submit for r in rhs])
+    last = curve[-1]
     st = srv.stats(rhs)
-    line = _line(METRIC, len(rhs) / span, "solves/s", args, ws, span,
-                 {"workload": f"serve: Poisson {args.rate}/s over {args.duration} s ({len(stream)} requests, "
-                              f"{len(rhs)} RHS), 40% spheres / 40% ellipsoids / 20% aggregates (K 4-32, r 6-12 d), "
+    line = _line(METRIC, last["rhs_per_s"], "solves/s", args, ws, last["seconds"],
+                 {"workload": f"serve: Poisson {rates[-1]}/s over {args.duration} s ({last['requests']} requests, "
+                              f"{last['rhs']} RHS), 40% spheres / 40% ellipsoids / 20% aggregates (K 4-32, r 6-12 d), "
                               f"boxes 16^3-128^3, m Re U[1.3,2] Im U[0,0.5], lambda U[0.4,0.8] um, 1-16 incidences, "
                               f"mixed precision to 1e-5, continuous batching",
                   "parallelism": "replicas" if ws > 1 else "single", "slots_per_bucket": args.slots,
                   "preconditioner": "none (precon=False)" if args.no_precondition else
                                     "precon=True: occupancy-weighted circulant per request group on its bucket's grid",
                   "pools": {str(k): v for k, v in st.get("pools", {}).items()}},
-                 latency_ms={"request_p50": float(np.percentile(lat_req, 50) * 1e3),
-                             "request_p99": float(np.percentile(lat_req, 99) * 1e3),
-                             "rhs_p50": float(np.percentile(lat_rhs, 50) * 1e3),
-                             "rhs_p99": float(np.percentile(lat_rhs, 99) * 1e3)},
-                 requests_per_s=len(stream) / span,
-                 green_cache={"hits": srv.green.hits, "misses": srv.green.misses},
-                 converged=sum(r.info.status == "converged" for r in rhs),
-                 gpu_launches=int(launches), clocks=clk.summary())
+                 latency_ms={"request_p50": last["request_p50_ms"], "request_p99": last["request_p99_ms"],
+                             "rhs_p50": last["rhs_p50_ms"], "rhs_p99": last["rhs_p99_ms"]},
+                 requests_per_s=last["requests_per_s"], curve=curve,
+                 green_cache={"hits": last["green_hits"], "misses": last["green_misses"]},
+                 converged=last["converged"], gpu_launches=int(launches), clocks=clk.summary())
     srv.close()
     print(json.dumps(line), flush=True)
 
@@ -883,7 +925,8 @@ def main():
                          "batch64: 64 geometries x 16 RHS; serve: Poisson request stream")
     ap.add_argument("--geometries", type=int, default=64, help="batch64: number of geometries")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: arrivals per second")
-    ap.add_argument("--duration", type=float, default=10.0, help="serve: seconds of arrivals")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve: seconds of arrivals per rate")
+    ap.add_argument("--rates", default="", help="serve: comma-separated offered rates (requests/s), one stream each")
     ap.add_argument("--slots", type=int, default=16, help="serve: slots per size bucket")
     ap.add_argument("--chunk", type=int, default=8, help="batch64 / serve: iterations per pool chunk between polls")
     ap.add_argument("--no-precondition", action="store_true",

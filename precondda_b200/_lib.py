@@ -45,7 +45,10 @@ EXPORTS = (
     "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
     "dda_far_field", "dda_matvec_batch", "dda_precond_build", "dda_precond_op_create", "dda_gpbicgstab_pre",
     "dda_solve_batch_pre", "dda_solve_mixed_batch_pre", "dda_slots_create_pre", "dda_slots_admit_pre",
+    "dda_tuning_set", "dda_tuning_get",
 )
+
+DDA_TUNE_NO_P3PIPE, DDA_TUNE_P3PIPE_1SM, DDA_TUNE_NO_FUSED_ZY, DDA_TUNE_NO_FUSED_INV = 1, 2, 4, 8
 
 
 class DDAError(RuntimeError):
@@ -96,6 +99,8 @@ def _declare(lib):
     lib.dda_op_destroy.restype = None
     lib.dda_matvec.argtypes = [vp, i, vp, vp, vp, vp]
     lib.dda_matvec_noalloc.argtypes = [i, i, i, i, i, i, i, vp, d, vp, i, vp, vp, vp, vp]
+    lib.dda_tuning_set.argtypes = [i, i, i, i, i, i, i, i, i]
+    lib.dda_tuning_get.argtypes = [i, i, i, i, i, i, i, i, C.POINTER(C.c_int)]
     lib.dda_gpbicgstab.argtypes = [vp, vp, d, i, d, vp, C.POINTER(dda_result), vp]
     lib.dda_solve_batch.argtypes = [vp, i, i, i, i, i, i, i, d, C.POINTER(dda_instance), i, d, i, d,
                                     C.POINTER(dda_result), vp]

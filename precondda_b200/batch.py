@@ -15,6 +15,9 @@ Gpbicgstab.py:879-1201).  The synthetic workloads live in workloads.py.
 candidate shape (per-axis padding to the next bucket edge, or the enclosing
 cube, whose kernels are specialised at compile time) it times the batched
 matvec on the device once and keeps the cheapest per right-hand side.
+``LaunchTuner`` then picks, per bucket and batch width, the matvec launch
+variant (x-pass kernel and CTAs per SM, fused or separate z/y passes) the
+same way and records it in the engine's tuning table.
 """
 from __future__ import annotations
 
@@ -132,6 +135,99 @@ class PaddingTuner:
             best = min(self.candidates(s), key=lambda b: self.cost(b))
             out.append((best, self.lengths(best)))
         return out
+
+
+# --------------------------------------------------------------------------
+# launch-variant autotuner
+# --------------------------------------------------------------------------
+def launch_candidates(box, L_, dtype, nb):
+    """DDA_TUNE_* flag sets worth timing for one bucket: the staged x pass
+    on two or one CTA per SM, or the one-tile x pass (cubic complex64 boxes
+    on the (2n)^3 grid of 64^3 and 128^3, where the staged kernel is built),
+    each with and without the cluster-fused z/y passes (one-instance 64^3
+    complex64 launches, where those are built)."""
+    cube = box[0] == box[1] == box[2] and L_[0] == L_[1] == L_[2] == 2 * box[0]
+    x_opts = [0]
+    if cube and dtype == _C64 and L_[0] in (128, 256):
+        x_opts = [0, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_NO_P3PIPE]
+    zy_opts = [0]
+    if cube and dtype == _C64 and L_[0] == 128 and nb == 1:
+        zy_opts = [0, L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV]
+    return [a | b for a in x_opts for b in zy_opts]
+
+
+class LaunchTuner:
+    """Picks the matvec launch variant (block shapes: which x-pass kernel
+    and how many of its CTAs per SM, fused or separate z/y passes) per
+    (dtype, padded box, FFT lengths, batch-width class) by timing a batched
+    matvec of each candidate on the device, L2 flushed between launches.
+    The winner goes into the engine's tuning table (dda_tuning_set), and
+    into an optional JSON cache so later runs skip the timing.  ``timer``
+    replaces the device timing (tests)."""
+
+    def __init__(self, device=None, cache_path=None, reps=5, timer=None):
+        self.device = _device(device) if timer is None else None
+        self.cache_path = cache_path
+        self.reps = int(reps)
+        self.timer = timer
+        self.best: dict = {}
+        self.times: dict = {}
+        if cache_path and os.path.exists(cache_path):
+            with open(cache_path) as f:
+                self.best = {tuple(json.loads(k)): v for k, v in json.load(f).items()}
+
+    @staticmethod
+    def key(box, L_, dtype, nb):
+        return (0 if dtype == _C64 else 1,) + tuple(int(v) for v in box) + tuple(int(v) for v in L_) + \
+            (int(nb),)
+
+    def tune(self, box, L_, dtype, nb):
+        """Flags chosen for this bucket (measured once, then cached)."""
+        k = self.key(box, L_, dtype, nb)
+        if k not in self.best:
+            cands = launch_candidates(box, L_, dtype, nb)
+            if len(cands) == 1:
+                self.best[k] = cands[0]
+            else:
+                t = {f: self._time(box, L_, dtype, nb, f) for f in cands}
+                self.times[k] = t
+                self.best[k] = min(t, key=t.get)
+            if self.cache_path:
+                with open(self.cache_path, "w") as f:
+                    json.dump({json.dumps(list(kk)): v for kk, v in self.best.items()}, f)
+        self.apply(box, L_, dtype, nb, self.best[k])
+        return self.best[k]
+
+    def apply(self, box, L_, dtype, nb, flags):
+        if self.timer is not None:
+            return
+        code = L.DDA_C64 if dtype == _C64 else L.DDA_C128
+        L.check(L.lib().dda_tuning_set(code, *[int(v) for v in box], *[int(v) for v in L_], int(nb), int(flags)))
+
+    def _time(self, box, L_, dtype, nb, flags):
+        if self.timer is not None:
+            return self.timer(box, L_, dtype, nb, flags)
+        from .engine import DDAOperator, matvec_batch
+        dev = self.device
+        self.apply(box, L_, dtype, nb, flags)
+        ia = torch.full(box, 1.0 / (0.02 + 0.002j), dtype=_C128, device=dev)
+        op = DDAOperator(ia, 6.0, 0.05, dtype=dtype, L_=L_, device=dev)
+        xs = [torch.randn(*box, 3, dtype=dtype, device=dev) for _ in range(nb)]
+        flush = torch.empty(48 << 20, dtype=torch.float32, device=dev)      # 192 MB > L2
+        run = (lambda: matvec_batch([op] * nb, xs)) if nb > 1 else (lambda: op.matvec(xs[0]))
+        for _ in range(2):
+            run()
+        ts = []
+        for _ in range(self.reps):
+            flush.add_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            run()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        return float(np.median(ts))
 
 
 # --------------------------------------------------------------------------

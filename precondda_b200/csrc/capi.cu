@@ -135,6 +135,29 @@ int dda_ctx_trim(dda_ctx* ctx) {
 
 int dda_fft_length_ok(int L, int dtype) { return length_ok(L, dtype) ? 1 : 0; }
 
+int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int flags) {
+  if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
+  if (nb < 1) { set_error("nb must be >= 1"); return DDA_ERR_ARG; }
+  if (flags > (DDA_TUNE_NO_P3PIPE | DDA_TUNE_P3PIPE_1SM | DDA_TUNE_NO_FUSED_ZY | DDA_TUNE_NO_FUSED_INV)) {
+    set_error("unknown tuning flags");
+    return DDA_ERR_ARG;
+  }
+  Geo g;
+  int rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g, 1);
+  if (rc) return rc;
+  tune_set(dtype, g, nb, flags);
+  return DDA_OK;
+}
+
+int dda_tuning_get(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int* flags) {
+  if (!flags || nb < 1) { set_error("null flags or nb < 1"); return DDA_ERR_ARG; }
+  Geo g;
+  int rc = make_geo(nx, ny, nz, Lx, Ly, Lz, dtype, &g, 1);
+  if (rc) return rc;
+  if (!tune_get(dtype, g, nb, flags)) { set_error("no tuning entry"); return DDA_ERR_ARG; }
+  return DDA_OK;
+}
+
 int dda_green_build(dda_ctx* ctx, int nx, int ny, int nz, int Lx, int Ly, int Lz, double k, double d, double scale,
                     int layout, void* out_c128, void* out_c64, void* stream) {
   int rc = check_ctx(ctx);

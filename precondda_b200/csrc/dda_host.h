@@ -101,6 +101,13 @@ struct PassCfg {
 
 PassCfg make_pass_cfg(const Geo& g, bool dbl);
 
+// Launch tuning table (DDA_TUNE_* flags of include/dda_b200.h) keyed by
+// dtype, geometry and batch-width class (1, 2-3, 4-7, 8-15, 16+).
+int nb_class(int nb);
+int tune_flags(int dtype, const Geo& g, int nb);
+void tune_set(int dtype, const Geo& g, int nb, int flags);
+bool tune_get(int dtype, const Geo& g, int nb, int* flags);
+
 // Preconditioner of a batched solve (the reference's right-preconditioned
 // GPBiCGSTAB, precon=True): per-instance octants (engine layout) on the grid
 // g.Lx/Ly/Lz (box g.nx/ny/nz, the solve's), applied as

@@ -2,6 +2,7 @@
 #include "matvec_impl.cuh"
 
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <set>
 #include <utility>
@@ -42,6 +43,52 @@ int device_sms() {
     sms[dev] = (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0) ? v : 148;
   }
   return sms[dev];
+}
+
+// ---------------------------------------------------------------------------
+// Launch tuning table: per (dtype, box, FFT lengths, batch-width class) the
+// launch variant an autotuner measured fastest (DDA_TUNE_* flags).  Looked
+// up at every matvec launch; absent entries mean the defaults.
+// ---------------------------------------------------------------------------
+namespace {
+struct TuneKey {
+  int dtype, nx, ny, nz, Lx, Ly, Lz, nbc;
+  bool operator<(const TuneKey& o) const {
+    const int a[8] = {dtype, nx, ny, nz, Lx, Ly, Lz, nbc};
+    const int b[8] = {o.dtype, o.nx, o.ny, o.nz, o.Lx, o.Ly, o.Lz, o.nbc};
+    for (int i = 0; i < 8; ++i)
+      if (a[i] != b[i]) return a[i] < b[i];
+    return false;
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, int> g_tune;
+TuneKey tune_key(int dtype, const Geo& g, int nb) {
+  return TuneKey{dtype, g.nx, g.ny, g.nz, g.Lx, g.Ly, g.Lz, nb_class(nb)};
+}
+}  // namespace
+
+int nb_class(int nb) { return nb <= 1 ? 1 : nb <= 3 ? 2 : nb <= 7 ? 4 : nb <= 15 ? 8 : 16; }
+
+int tune_flags(int dtype, const Geo& g, int nb) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (g_tune.empty()) return 0;
+  auto it = g_tune.find(tune_key(dtype, g, nb));
+  return it == g_tune.end() ? 0 : it->second;
+}
+
+void tune_set(int dtype, const Geo& g, int nb, int flags) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  if (flags < 0) g_tune.erase(tune_key(dtype, g, nb));
+  else g_tune[tune_key(dtype, g, nb)] = flags;
+}
+
+bool tune_get(int dtype, const Geo& g, int nb, int* flags) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(dtype, g, nb));
+  if (it == g_tune.end()) return false;
+  *flags = it->second;
+  return true;
 }
 
 cudaError_t mv_prepare(const void* const* ks, int n) {

@@ -879,6 +879,18 @@ void mv_cube_fill(MvSet<R>& o) {
     o.minb3p = 2;
     o.smem3p = PP::smem;
   }
+  if constexpr (sizeof(R) == 8 && V == 2 && (L == 128 || L == 256)) {
+    // complex128 64^3 / 128^3: tiles of 8 kz columns (384-byte row
+    // segments against 96 bytes in the one-tile kernel's 2-column tiles)
+    constexpr int TZ = 8;
+    constexpr int MB = L == 256 ? 1 : 2;
+    typedef P3Pipe<R, L, V, TZ> PP;
+    o.k3p = (typename M::P3)k_mv_pass3p<R, L, V, NC, TZ, MB>;
+    o.th3p = PP::TH;
+    o.nt3p = L * (L / TZ);
+    o.minb3p = MB;
+    o.smem3p = PP::smem;
+  }
   if constexpr (sizeof(R) == 4 && L == 128) {
     // complex64 64^3: both fused buffers fit two CTAs per SM
     typedef FusedZY<R, L> F;
@@ -915,6 +927,7 @@ bool fused_zy_enabled(bool inverse);
 bool p3_pipe_enabled();
 // Streaming multiprocessors of the current device (cached per device).
 int device_sms();
+
 
 // Launch on clusters of `cl` CTAs along x, with programmatic stream
 // serialization unless DDA_NO_PDL=1.
@@ -954,9 +967,10 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   // 0.138 ms (the separate passes already fill the GPU there and the fused
   // kernels hold two CTAs per SM), so batched launches keep the separate
   // passes.
+  const int tf = tune_flags(sizeof(R) == 8 ? DDA_C128 : DDA_C64, g, nb);
   const bool one = nb == 1;
-  const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false);
-  const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true);
+  const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) && !(tf & DDA_TUNE_NO_FUSED_ZY);
+  const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
   if (ff) {
     if ((e = launch_cluster(k.kf, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemf, s, g, twz, st, act,
                             in_id, cond)))
@@ -969,9 +983,11 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                         pc.ntz2)))
       return e;
   }
-  if (k.k3p && p3_pipe_enabled()) {
-    // persistent: about minb3p resident CTAs per SM over all instances
-    const int want = (k.minb3p * device_sms() + nb - 1) / nb;
+  if (k.k3p && p3_pipe_enabled() && !(tf & DDA_TUNE_NO_P3PIPE)) {
+    // persistent: about minb3p resident CTAs per SM over all instances (one
+    // per SM when tuned so)
+    const int per_sm = (tf & DDA_TUNE_P3PIPE_1SM) ? 1 : k.minb3p;
+    const int want = (per_sm * device_sms() + nb - 1) / nb;
     const int gx = std::max(1, std::min(k.nt3p, want));
     if ((e = launch_pdl(k.k3p, dim3((unsigned)gx, nb), dim3(k.th3p), k.smem3p, s, g, twx, st, act, cond, pc.tz3,
                         pc.ntz3, (R)gscale, fz.tensor)))

@@ -287,7 +287,7 @@ class DDAServer:
 
     def __init__(self, precision="mixed", buckets=DEFAULT_BUCKETS, slots_per_bucket=16, chunk_iters=8,
                  hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None,
-                 precondition=False):
+                 precondition=False, launch_tuner=None):
         if precision not in PRECISIONS:
             raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         self.device = _device(device)
@@ -307,6 +307,9 @@ class DDAServer:
         self._next = 0
         self.done: list[Request] = []
         self._pre: dict = {}       # pre_key -> [Preconditioner or None, requests not yet finished]
+        # optional batch.LaunchTuner: each new bucket's matvec launch variant
+        # is measured (complex64 sweeps, or the c128 solve) for its slot count
+        self.launch_tuner = launch_tuner
 
     # -- buckets ------------------------------------------------------------
     def bucket_for(self, shape) -> int:
@@ -324,6 +327,8 @@ class DDAServer:
         if ns < 1:
             raise MemoryError(f"bucket {n}^3 needs {per / 2**20:.0f} MiB per slot; "
                               f"{room / 2**20:.0f} MiB of the HBM budget is left")
+        if self.launch_tuner is not None:
+            self.launch_tuner.tune(box, L_, _C128 if self.precision == "c128" else _C64, ns)
         pool = SlotPool(box, L_, ns, self.precision, 1.0, self.device, precond_L=L_ if pre else None)
         self.hbm_used += ns * per
         b = _Bucket(n, L_, pool)

@@ -99,8 +99,9 @@ def test_cubic_kernels_launch_and_match_general(n, dtype, tol, monkeypatch):
     assert _rel(cube, general) < tol
 
 
+@pytest.mark.parametrize("dtype", [C64, C128])
 @pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
-def test_staged_x_pass_equals_one_tile_kernel(n, nb, monkeypatch):
+def test_staged_x_pass_equals_one_tile_kernel(n, nb, dtype, monkeypatch):
     """The staged persistent x pass (bulk-copied input tiles, one tile
     ahead) does the arithmetic of the one-tile-per-CTA kernel: equal bit for
     bit, alone and in batched launches (several instances per launch), in
@@ -110,8 +111,8 @@ def test_staged_x_pass_equals_one_tile_kernel(n, nb, monkeypatch):
     for j in range(nb):
         k, d, alpha, x = _rand_problem((n,) * 3, seed=n + j, fill=0.5)
         ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
-        ops.append(P.DDAOperator(ia, k, d, dtype=C64))
-        xs.append(torch.as_tensor(x, device="cuda").to(C64))
+        ops.append(P.DDAOperator(ia, k, d, dtype=dtype))
+        xs.append(torch.as_tensor(x, device="cuda").to(dtype))
     monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
     a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
     monkeypatch.setenv("DDA_NO_P3PIPE", "1")
@@ -121,9 +122,9 @@ def test_staged_x_pass_equals_one_tile_kernel(n, nb, monkeypatch):
     if nb == 1 and n == 64:
         pre = ops[0].preconditioner()
         monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
-        pa = pre.apply(xs[0], C64)
+        pa = pre.apply(xs[0], dtype)
         monkeypatch.setenv("DDA_NO_P3PIPE", "1")
-        pb = pre.apply(xs[0], C64)
+        pb = pre.apply(xs[0], dtype)
         assert torch.equal(pa, pb)
 
 
