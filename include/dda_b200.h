@@ -156,20 +156,24 @@ int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz
  * code).  A table, per (dtype, box nx,ny,nz, FFT lengths, batch-width class
  * of nb: 1, 2-3, 4-7, 8-15, 16+), of the matvec launch variant to use, as an
  * autotuner measured it (precondda_b200.batch.LaunchTuner).  Flags:
- *   DDA_TUNE_NO_P3PIPE     the one-tile-per-CTA x pass instead of the staged
- *                          persistent one (where that is compiled)
- *   DDA_TUNE_P3PIPE_1SM    staged x pass on one CTA per SM instead of two
+ *   DDA_TUNE_P3PIPE        the staged persistent x pass (input tiles bulk-
+ *                          copied one tile ahead, two CTAs per SM) instead of
+ *                          the one-tile-per-CTA kernel, where it is compiled
+ *   DDA_TUNE_P3PIPE_1SM    the staged x pass on one CTA per SM
  *   DDA_TUNE_NO_FUSED_ZY   separate z and y forward passes instead of the
  *                          cluster-fused kernel (one-instance launches)
  *   DDA_TUNE_NO_FUSED_INV  separate y and z inverse passes likewise
+ *   DDA_TUNE_P3PAIR        the x pass on packed pairs of transforms (FP32x2
+ *                          arithmetic, complex64 cubic 64^3 / 128^3 boxes)
  * dda_tuning_set with flags < 0 removes the entry; dda_tuning_get returns
  * DDA_ERR_ARG when there is none.  Entries apply to launches made after
  * the call (a captured iteration graph keeps the variant it was captured
  * with). */
-#define DDA_TUNE_NO_P3PIPE 1
+#define DDA_TUNE_P3PIPE 1
 #define DDA_TUNE_P3PIPE_1SM 2
 #define DDA_TUNE_NO_FUSED_ZY 4
 #define DDA_TUNE_NO_FUSED_INV 8
+#define DDA_TUNE_P3PAIR 16
 int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int flags);
 int dda_tuning_get(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int* flags);
 

@@ -48,7 +48,7 @@ EXPORTS = (
     "dda_tuning_set", "dda_tuning_get",
 )
 
-DDA_TUNE_NO_P3PIPE, DDA_TUNE_P3PIPE_1SM, DDA_TUNE_NO_FUSED_ZY, DDA_TUNE_NO_FUSED_INV = 1, 2, 4, 8
+DDA_TUNE_P3PIPE, DDA_TUNE_P3PIPE_1SM, DDA_TUNE_NO_FUSED_ZY, DDA_TUNE_NO_FUSED_INV, DDA_TUNE_P3PAIR = 1, 2, 4, 8, 16
 
 
 class DDAError(RuntimeError):

@@ -138,7 +138,8 @@ int dda_fft_length_ok(int L, int dtype) { return length_ok(L, dtype) ? 1 : 0; }
 int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int flags) {
   if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
   if (nb < 1) { set_error("nb must be >= 1"); return DDA_ERR_ARG; }
-  if (flags > (DDA_TUNE_NO_P3PIPE | DDA_TUNE_P3PIPE_1SM | DDA_TUNE_NO_FUSED_ZY | DDA_TUNE_NO_FUSED_INV)) {
+  if (flags > (DDA_TUNE_P3PIPE | DDA_TUNE_P3PIPE_1SM | DDA_TUNE_NO_FUSED_ZY | DDA_TUNE_NO_FUSED_INV |
+                DDA_TUNE_P3PAIR)) {
     set_error("unknown tuning flags");
     return DDA_ERR_ARG;
   }

@@ -100,8 +100,8 @@ __host__ __device__ constexpr int ppad_len(int L) { return DDA_PPAD ? L + (L >> 
 // s > 0).  Always the forward transform: inverse transforms are run as
 // swap(FFT(swap(x))), swap(a + ib) = b + ia, which costs no instructions.
 // ZH (stage 0 only): the upper half of every butterfly's inputs is zero.
-template <class P, int s, bool ZH = false, class C>
-__device__ __forceinline__ void rstage(C* a, int t, const C* __restrict__ tw) {
+template <class P, int s, bool ZH = false, class C, class TW>
+__device__ __forceinline__ void rstage(C* a, int t, const TW* __restrict__ tw) {
   static_assert(!ZH || s == 0, "zero-half inputs only at stage 0");
   constexpr int R = P::r[s];
   constexpr int NS = P::ns(s);
@@ -146,8 +146,8 @@ __device__ __forceinline__ int rout_pos(int t, int b, int q) {
 // `sm(c, ppos)` returns the shared-memory slot of padded position ppos of
 // component c of this thread's transform.  All threads of the CTA must call
 // this together (it contains barriers).
-template <class P, int NC, int s, class C, class SM>
-__device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const C* __restrict__ tw) {
+template <class P, int NC, int s, class C, class SM, class TW>
+__device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const TW* __restrict__ tw) {
   constexpr int R = P::r[s];
   constexpr int R2 = P::r[s + 1];
 #pragma unroll
@@ -169,8 +169,8 @@ __device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const C* __
 }
 
 // Stages s+1..S-1 (stage 0 is computed by the caller after its global load).
-template <class P, int NC, int s, class C, class SM>
-__device__ __forceinline__ void rrest(C* a, int t, const SM& sm, const C* __restrict__ tw) {
+template <class P, int NC, int s, class C, class SM, class TW>
+__device__ __forceinline__ void rrest(C* a, int t, const SM& sm, const TW* __restrict__ tw) {
   if constexpr (s + 1 < P::S) {
     rexchange<P, NC, s>(a, t, sm, tw);
     rrest<P, NC, s + 1>(a, t, sm, tw);

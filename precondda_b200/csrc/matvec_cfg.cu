@@ -27,9 +27,14 @@ bool fused_zy_enabled(bool inverse) {
   return true;
 }
 
-bool p3_pipe_enabled() {
-  const char* e = getenv("DDA_NO_P3PIPE");
-  return !(e && *e == '1');
+bool p3_pair_forced() {
+  const char* e = getenv("DDA_P3PAIR");
+  return e && *e == '1';
+}
+
+bool p3_pipe_forced() {
+  const char* e = getenv("DDA_P3PIPE");
+  return e && *e == '1';
 }
 
 int device_sms() {

@@ -23,6 +23,7 @@
 #include "krylov_ctrl.cuh"
 #include "fft_sizes.h"
 #include "bulk.cuh"
+#include "cpair.cuh"
 #include <cooperative_groups.h>
 #include <cstdlib>
 #include <type_traits>
@@ -397,6 +398,158 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   C* swo = opaque_ptr(sw);
   auto smo = [&](int, int pp) -> C& { return swo[pp * W]; };
   auto stf = [&](int, int pos, C v) { if (ok && (DH || pos < nx)) __stcg(colo + pos * rs, cswap(v)); };
+  constexpr int R0 = Q::r[0];
+#pragma unroll
+  for (int b = 0; b < Q::E / R0; ++b)
+#pragma unroll
+    for (int m = 0; m < R0; ++m) a[b * R0 + m] = cswap(smo(0, ppad(rin_pos<Q, 0>(ti, b, m))));
+  __syncthreads();
+  rstage<Q, 0>(a, ti, tw);
+  rrest<Q, 1, 0>(a, ti, smo, tw);
+  rstore<Q, 1, DH>(a, ti, stf);
+}
+
+// ---------------------------------------------------------------------------
+// pass 3 on packed pairs (complex64 cubic boxes): every thread transforms two
+// columns of the tile at once -- column p and column p + W/2, one per lane of
+// the cp2 pair (cpair.cuh) -- so each butterfly add, twiddle product and
+// exchange store / load covers two transforms in one packed FP32x2 or 128-bit
+// shared-memory instruction.  Columns p and p + W/2 are the same component of
+// the kz points kzl and kzl + TZ/2 (w = 3 kzl + c), so the tensor product
+// also runs on pairs: the cp2 slot p = 3 kzl + c holds component c of both
+// points, and each 3x3 product updates two points.  Tile shape, mirror rule
+// and octant reads are those of k_mv_pass3s; results agree with it to
+// complex64 rounding (the packed rotations round like the scalar ones, the
+// grouping of a few sums differs).
+// ---------------------------------------------------------------------------
+template <int LX, int TZ>
+struct P3Pair {
+  typedef typename PlanFor<LX, float>::type P;
+  static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
+  static constexpr int LP = ppad_len(LX);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2);
+  static_assert(TZ % 2 == 0 && LX % TZ == 0, "pairs of kz columns");
+  static_assert(TH <= 1024, "threads per CTA");
+};
+
+// A 3x3 entry of the octant for two points, scaled: (re, im, -re, -im).
+struct G2 {
+  float2 re, im, nre, nim;
+};
+__device__ __forceinline__ G2 g2_load(const float2* qa, const float2* qb, float2 s) {
+  const cp2 g = cpack(__ldg(qa), __ldg(qb));
+  G2 o;
+  o.re = f2mul(g.re, s);
+  o.im = f2mul(g.im, s);
+  o.nre = f2mul(g.re, make_float2(-s.x, -s.y));
+  o.nim = f2mul(g.im, make_float2(-s.x, -s.y));
+  return o;
+}
+// sum of three products g_k a_k on pairs; NEG_k takes -g_k
+template <bool N0, bool N1, bool N2>
+__device__ __forceinline__ cp2 g2_dot3(const G2& g0, cp2 a0, const G2& g1, cp2 a1, const G2& g2, cp2 a2) {
+  const float2 r0 = N0 ? g0.nre : g0.re, i0 = N0 ? g0.nim : g0.im, m0 = N0 ? g0.im : g0.nim;
+  const float2 r1 = N1 ? g1.nre : g1.re, i1 = N1 ? g1.nim : g1.im, m1 = N1 ? g1.im : g1.nim;
+  const float2 r2 = N2 ? g2.nre : g2.re, i2 = N2 ? g2.nim : g2.im, m2 = N2 ? g2.im : g2.nim;
+  cp2 o;
+  // re = sum r a.re - i a.im ; im = sum r a.im + i a.re   (m = -i)
+  o.re = f2fma(r0, a0.re, f2fma(m0, a0.im, f2fma(r1, a1.re, f2fma(m1, a1.im, f2fma(r2, a2.re, f2mul(m2, a2.im))))));
+  o.im = f2fma(r0, a0.im, f2fma(i0, a0.re, f2fma(r1, a1.im, f2fma(i1, a1.re, f2fma(r2, a2.im, f2mul(i2, a2.re))))));
+  return o;
+}
+
+template <int LX, int NC, int TZ, int MINB>
+__global__ void __launch_bounds__(P3Pair<LX, TZ>::TH, MINB)
+    k_mv_pass3x(Geo g, const float2* __restrict__ tw, InstState* st, const int* act, int cond, int tz_, int ntz_,
+                float gscale, int op) {
+  grid_dep_begin();
+  typedef float2 C;
+  typedef P3Pair<LX, TZ> PS;
+  typedef typename PS::P P;
+  typedef RevPlan<P> Q;
+  static_assert(NC == LX / 2, "cubic boxes on the (2n)^3 grid");
+  constexpr bool ZH = P::r[0] % 2 == 0;
+  constexpr bool DH = half_store_ok<Q>();
+  static_assert(ZH && DH, "zero-half loads and half stores");
+  constexpr int WP = PS::WP, NTZ = LX / TZ;
+  constexpr long long rs = (long long)LX * LX * 3;
+  constexpr int hy = LX / 2 + 1, hz = LX / 2 + 1, H = hy * hy * hz;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cp2* s = reinterpret_cast<cp2*>(smem_raw);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  C* __restrict__ t2 = (C*)S.t2;
+  const C* __restrict__ gh = (const C*)(op ? S.pghat : S.ghat);
+  const int p = threadIdx.x % WP, t = threadIdx.x / WP;
+  const int pen = blockIdx.x / NTZ, kzt = blockIdx.x - pen * NTZ;
+  const int ky = pencil_ky(pen, LX);
+  const int kz0 = kzt * TZ;
+  C* col = t2 + ((long long)ky * LX + kz0) * 3;
+  cp2* sw = s + p;
+  auto ld = [&](int, int pos) -> cp2 {
+    const C* r = col + pos * rs;
+    return cpack(__ldcg(r + p), __ldcg(r + p + WP));
+  };
+  auto sm = [&](int, int pp) -> cp2& { return sw[pp * WP]; };
+  cp2 a[P::E];
+  rload<P, 1, ZH>(a, t, ld);
+  rstage<P, 0, ZH>(a, t, tw);
+  rrest<P, 1, 0>(a, t, sm, tw);
+  constexpr int RL = P::r[P::S - 1];
+#pragma unroll
+  for (int b = 0; b < P::E / RL; ++b)
+#pragma unroll
+    for (int q = 0; q < RL; ++q) sm(0, ppad(rout_pos<P, P::S - 1>(t, b, q))) = a[b * RL + q];
+  __syncthreads();
+  {
+    // thread -> (kzl in [0, TZ/2), mirror pair j); lanes: kz0 + kzl, kz0 + kzl + TZ/2
+    constexpr int TH2 = TZ / 2;
+    constexpr int js = PS::TH / TH2;
+    const int kzl = threadIdx.x % TH2;
+    const int kza = kz0 + kzl, kzb = kza + TH2;
+    const bool fy = ky > LX / 2, fza = kza > LX / 2, fzb = kzb > LX / 2;
+    const int my = fy ? LX - ky : ky;
+    const int mza = fza ? LX - kza : kza, mzb = fzb ? LX - kzb : kzb;
+    const float2 sd = f2(gscale);
+    const float2 sxy = f2(fy ? -gscale : gscale);
+    const float2 sxz = make_float2(fza ? -gscale : gscale, fzb ? -gscale : gscale);
+    const float2 syz = make_float2((fy != fza) ? -gscale : gscale, (fy != fzb) ? -gscale : gscale);
+    const C* __restrict__ qa0 = gh + my * hz + mza;
+    const C* __restrict__ qb0 = gh + my * hz + mzb;
+    for (int j = threadIdx.x / TH2; j <= LX / 2; j += js) {
+      const C* qa = qa0 + j * (hy * hz);
+      const C* qb = qb0 + j * (hy * hz);
+      const G2 gxx = g2_load(qa, qb, sd), gxy = g2_load(qa + H, qb + H, sxy);
+      const G2 gxz = g2_load(qa + 2 * H, qb + 2 * H, sxz), gyy = g2_load(qa + 3 * H, qb + 3 * H, sd);
+      const G2 gyz = g2_load(qa + 4 * H, qb + 4 * H, syz), gzz = g2_load(qa + 5 * H, qb + 5 * H, sd);
+      {
+        cp2* v = s + ppad(j) * WP + 3 * kzl;
+        const cp2 a0 = v[0], a1 = v[1], a2 = v[2];
+        v[0] = g2_dot3<false, false, false>(gxx, a0, gxy, a1, gxz, a2);
+        v[1] = g2_dot3<false, false, false>(gxy, a0, gyy, a1, gyz, a2);
+        v[2] = g2_dot3<false, false, false>(gxz, a0, gyz, a1, gzz, a2);
+      }
+      if (j > 0 && j < LX / 2) {
+        // kx = LX - j: the x mirror flips the xy and xz entries
+        cp2* v = s + ppad(LX - j) * WP + 3 * kzl;
+        const cp2 a0 = v[0], a1 = v[1], a2 = v[2];
+        v[0] = g2_dot3<false, true, true>(gxx, a0, gxy, a1, gxz, a2);
+        v[1] = g2_dot3<true, false, false>(gxy, a0, gyy, a1, gyz, a2);
+        v[2] = g2_dot3<true, false, false>(gxz, a0, gyz, a1, gzz, a2);
+      }
+    }
+  }
+  __syncthreads();
+  const int ti = opaque(t);
+  C* colo = opaque_ptr(col);
+  cp2* swo = opaque_ptr(sw);
+  auto smo = [&](int, int pp) -> cp2& { return swo[pp * WP]; };
+  auto stf = [&](int, int pos, cp2 v) {
+    v = cswap(v);
+    C* r = colo + pos * rs;
+    __stcg(r + p, clo(v));
+    __stcg(r + p + WP, chi(v));
+  };
   constexpr int R0 = Q::r[0];
 #pragma unroll
   for (int b = 0; b < Q::E / R0; ++b)
@@ -793,6 +946,11 @@ template <typename R> struct MvSet {
   P3 k3p = nullptr;
   int th3p = 0, nt3p = 0, minb3p = 1;
   size_t smem3p = 0;
+  // packed-pair x pass (complex64 cubic sets): threads, CTAs per instance,
+  // dynamic shared memory
+  P3 k3x = nullptr;
+  int th3x = 0, grid3x = 0;
+  size_t smem3x = 0;
 };
 
 // General kernels (sizes from Geo), defined with the instantiations.
@@ -879,6 +1037,16 @@ void mv_cube_fill(MvSet<R>& o) {
     o.minb3p = 2;
     o.smem3p = PP::smem;
   }
+  if constexpr (sizeof(R) == 4 && V == 0 && (L == 128 || L == 256)) {
+    // the packed-pair x pass on the same tiles (192 threads; 4 CTAs per SM
+    // at L = 256, 3 at L = 128, where the 16 x 8 plan needs more registers)
+    constexpr int TZ = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+    typedef P3Pair<L, TZ> PX;
+    o.k3x = (typename M::P3)k_mv_pass3x<L, NC, TZ, (L == 256 ? 4 : 3)>;
+    o.th3x = PX::TH;
+    o.grid3x = L * (L / TZ);
+    o.smem3x = PX::smem;
+  }
   if constexpr (sizeof(R) == 8 && V == 2 && (L == 128 || L == 256)) {
     // complex128 64^3 / 128^3: tiles of 8 kz columns (384-byte row
     // segments against 96 bytes in the one-tile kernel's 2-column tiles)
@@ -922,9 +1090,14 @@ cudaError_t mv_prepare(const void* const* ks, int n);
 // Whether the cluster-fused z/y passes run (DDA_NO_FUSED_ZY=1 turns both
 // off, DDA_NO_FUSED_INV=1 the inverse one only); read at every launch.
 bool fused_zy_enabled(bool inverse);
-// Whether the staged persistent x pass runs where compiled (DDA_NO_P3PIPE=1:
-// the one-tile-per-CTA kernel); read at every launch.
-bool p3_pipe_enabled();
+// Whether the staged persistent x pass is forced where compiled
+// (DDA_P3PIPE=1; otherwise it runs only where the tuning table selects
+// it: on B200 it measured slower than the one-tile kernel at 64^3 and
+// 128^3); read at every launch.
+bool p3_pipe_forced();
+// Whether the packed-pair x pass is forced where compiled (DDA_P3PAIR=1;
+// otherwise DDA_TUNE_P3PAIR in the tuning table selects it).
+bool p3_pair_forced();
 // Streaming multiprocessors of the current device (cached per device).
 int device_sms();
 
@@ -956,9 +1129,10 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                           const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
                           const MvFuse& fz = MvFuse()) {
-  const void* ks[8] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
-                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki, (const void*)k.k3p};
-  cudaError_t e = mv_prepare(ks, 8);
+  const void* ks[9] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
+                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki, (const void*)k.k3p,
+                       (const void*)k.k3x};
+  cudaError_t e = mv_prepare(ks, 9);
   if (e != cudaSuccess) return e;
   // The fused z/y kernels take the place of passes 1+2 / 4+5 in launches of
   // one instance with no Krylov step fused into those passes (cubic sets use
@@ -983,7 +1157,11 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                         pc.ntz2)))
       return e;
   }
-  if (k.k3p && p3_pipe_enabled() && !(tf & DDA_TUNE_NO_P3PIPE)) {
+  if (k.k3x && (p3_pair_forced() || (tf & DDA_TUNE_P3PAIR))) {
+    if ((e = launch_pdl(k.k3x, dim3((unsigned)k.grid3x, nb), dim3(k.th3x), k.smem3x, s, g, twx, st, act, cond,
+                        pc.tz3, pc.ntz3, (R)gscale, fz.tensor)))
+      return e;
+  } else if (k.k3p && (p3_pipe_forced() || (tf & (DDA_TUNE_P3PIPE | DDA_TUNE_P3PIPE_1SM)))) {
     // persistent: about minb3p resident CTAs per SM over all instances (one
     // per SM when tuned so)
     const int per_sm = (tf & DDA_TUNE_P3PIPE_1SM) ? 1 : k.minb3p;

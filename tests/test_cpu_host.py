@@ -236,25 +236,24 @@ def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     from precondda_b200 import _lib as L
     from precondda_b200.batch import LaunchTuner, launch_candidates
     c64, c128 = torch.complex64, torch.complex128
-    assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [
-        0, L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV, L.DDA_TUNE_P3PIPE_1SM,
-        L.DDA_TUNE_P3PIPE_1SM | L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV, L.DDA_TUNE_NO_P3PIPE,
-        L.DDA_TUNE_NO_P3PIPE | L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV]
-    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == [0, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_NO_P3PIPE]
+    zy = L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV
+    xs = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_P3PAIR]
+    assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [x | z for x in xs for z in (0, zy)]
+    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == xs
     assert launch_candidates((40, 30, 20), (80, 64, 40), c64, 4) == [0]
     assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0]
     calls = []
 
     def timer(box, L_, dtype, nb, flags):
         calls.append(flags)
-        return {0: 3.0, L.DDA_TUNE_P3PIPE_1SM: 2.0, L.DDA_TUNE_NO_P3PIPE: 2.5}[flags]
+        return {0: 3.0, L.DDA_TUNE_P3PIPE_1SM: 2.0, L.DDA_TUNE_P3PIPE: 2.5, L.DDA_TUNE_P3PAIR: 2.2}[flags]
 
     path = str(tmp_path / "launch.json")
     t = LaunchTuner(cache_path=path, timer=timer)
     assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
-    assert sorted(calls) == sorted([0, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_NO_P3PIPE])
+    assert sorted(calls) == sorted(xs)
     assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
-    assert len(calls) == 3                       # cached
-    assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == 3   # single candidate: no timing
+    assert len(calls) == 4                       # cached
+    assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == 4   # single candidate: no timing
     t2 = LaunchTuner(cache_path=path, timer=lambda *a: 1 / 0)
     assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM      # from the JSON cache

@@ -144,7 +144,7 @@ def test_server_reports_statuses_and_refuses_over_budget():
     # a budget that holds no slot: the request is refused before any allocation
     torch.cuda.synchronize()
     before = torch.cuda.memory_allocated()
-    tiny = DDAServer(precision="c128", buckets=(8,), slots_per_bucket=4, hbm_budget=1 << 20)
+    tiny = DDAServer(precision="c128", buckets=(8,), slots_per_bucket=4, hbm_budget=1 << 10)
     with pytest.raises(MemoryError):
         tiny.submit(Request(ia, E, k, d, tol=1e-6))
     assert tiny.pending() == 0 and not tiny._b

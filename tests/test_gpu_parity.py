@@ -113,19 +113,52 @@ def test_staged_x_pass_equals_one_tile_kernel(n, nb, dtype, monkeypatch):
         ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
         ops.append(P.DDAOperator(ia, k, d, dtype=dtype))
         xs.append(torch.as_tensor(x, device="cuda").to(dtype))
-    monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
+    monkeypatch.setenv("DDA_P3PIPE", "1")
     a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
-    monkeypatch.setenv("DDA_NO_P3PIPE", "1")
+    monkeypatch.delenv("DDA_P3PIPE", raising=False)
     b = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
     for u, v in zip(a, b):
         assert torch.equal(u, v)
     if nb == 1 and n == 64:
         pre = ops[0].preconditioner()
-        monkeypatch.delenv("DDA_NO_P3PIPE", raising=False)
+        monkeypatch.setenv("DDA_P3PIPE", "1")
         pa = pre.apply(xs[0], dtype)
-        monkeypatch.setenv("DDA_NO_P3PIPE", "1")
+        monkeypatch.delenv("DDA_P3PIPE", raising=False)
         pb = pre.apply(xs[0], dtype)
         assert torch.equal(pa, pb)
+
+
+@pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
+def test_pair_x_pass_matches_one_tile_kernel(n, nb, monkeypatch):
+    """The packed-pair x pass (two transforms per thread in FP32x2 lanes)
+    against the one-tile kernel and the oracle: complex64 rounding only,
+    alone and batched, in the interaction and preconditioner products."""
+    P = _pkg()
+    ops, xs, xn = [], [], []
+    for j in range(nb):
+        k, d, alpha, x = _rand_problem((n,) * 3, seed=2 * n + j, fill=0.5)
+        ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+        ops.append(P.DDAOperator(ia, k, d, dtype=C64))
+        xs.append(torch.as_tensor(x, device="cuda").to(C64))
+        xn.append((ia, k, d, x))
+    monkeypatch.setenv("DDA_P3PAIR", "1")
+    a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    monkeypatch.delenv("DDA_P3PAIR", raising=False)
+    b = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    for u, v in zip(a, b):
+        assert _rel(u.cpu().numpy(), v.cpu().numpy()) < 2e-6
+    if n == 64:
+        ia, k, d, x = xn[0]
+        mask = ia != 0
+        ref = O.interaction_mult(x, O.generate_interaction_row(n, n, n, k, d), ia, mask)
+        assert _rel(a[0].cpu().numpy(), ref) < 2e-5
+        if nb == 1:
+            pre = ops[0].preconditioner()
+            monkeypatch.setenv("DDA_P3PAIR", "1")
+            pa = pre.apply(xs[0], C64)
+            monkeypatch.delenv("DDA_P3PAIR", raising=False)
+            pb = pre.apply(xs[0], C64)
+            assert _rel(pa.cpu().numpy(), pb.cpu().numpy()) < 2e-6
 
 
 def test_matvec_dense_tiny():
