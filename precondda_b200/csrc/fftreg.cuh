@@ -216,9 +216,9 @@ __device__ __forceinline__ void rstore(const C* a, int t, const ST& st) {
 // inverse (unnormalised) transform, as swap(FFT(swap(x))).
 // ZH / DH: zero upper half of the input / only the lower half of the output
 // wanted (see rload / rstore).
-template <class P, int NC, bool INV, bool ZH = false, bool DH = false, class C, class LD, class SM, class ST>
+template <class P, int NC, bool INV, bool ZH = false, bool DH = false, class C, class LD, class SM, class ST, class TW>
 __device__ __forceinline__ void rfft(C* a, int t, const LD& ld, const SM& sm, const ST& st,
-                                     const C* __restrict__ tw) {
+                                     const TW* __restrict__ tw) {
   if constexpr (INV) {
     rload<P, NC, ZH>(a, t, [&](int c, int pos) -> C { return cswap(ld(c, pos)); });
   } else {

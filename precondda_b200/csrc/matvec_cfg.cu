@@ -27,6 +27,16 @@ bool fused_zy_enabled(bool inverse) {
   return true;
 }
 
+bool z_pair_forced() {
+  const char* e = getenv("DDA_ZPAIR");
+  return e && *e == '1';
+}
+
+bool y_pair_forced() {
+  const char* e = getenv("DDA_YPAIR");
+  return e && *e == '1';
+}
+
 bool p3_pair_forced() {
   const char* e = getenv("DDA_P3PAIR");
   return e && *e == '1';

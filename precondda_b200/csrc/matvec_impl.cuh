@@ -717,6 +717,177 @@ __global__ void __launch_bounds__(P3Pipe<R, LX, V, TZ>::TH, MINB)
 }
 
 // ---------------------------------------------------------------------------
+// passes 2 / 4 on packed pairs (complex64 cubic boxes): as k_mv_pass_y, with
+// each thread transforming columns p and p + W/2 of the tile in the two
+// lanes of a cp2 (FP32x2 butterflies, 128-bit exchanges).
+// ---------------------------------------------------------------------------
+template <int LY, int TZ>
+struct PYPair {
+  typedef typename PlanFor<LY, float>::type P;
+  static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
+  static constexpr int LP = ppad_len(LY);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2);
+  static_assert(TZ % 2 == 0 && LY % TZ == 0, "pairs of kz columns");
+};
+
+template <bool INV, int LY, int NC, int TZ, int MINB>
+__global__ void __launch_bounds__(PYPair<LY, TZ>::TH, MINB)
+    k_mv_pass_yx(Geo g, const float2* __restrict__ tw, InstState* st, const int* act, int cond, int tz_,
+                 int ntz_) {
+  grid_dep_begin();
+  typedef float2 C;
+  typedef PYPair<LY, TZ> PS;
+  typedef typename PS::P P;
+  static_assert(NC == LY / 2, "cubic boxes on the (2n)^3 grid");
+  constexpr bool ZH = !INV && P::r[0] % 2 == 0;
+  constexpr bool DH = INV && half_store_ok<P>();
+  static_assert(INV ? DH : ZH, "zero-half loads / half stores");
+  constexpr int WP = PS::WP, NTZ = LY / TZ;
+  constexpr long long rs = (long long)LY * 3;                 // row stride of T1/T2 (Lz = LY)
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cp2* s = reinterpret_cast<cp2*>(smem_raw);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  C* __restrict__ t1 = (C*)S.t1;
+  C* __restrict__ t2 = (C*)S.t2;
+  const int p = threadIdx.x % WP, t = threadIdx.x / WP;
+  const int ix = blockIdx.x / NTZ, kzt = blockIdx.x - ix * NTZ;
+  const int kz0 = kzt * TZ;
+  const C* src = (INV ? t2 + (long long)ix * LY * rs : t1 + (long long)ix * NC * rs) + kz0 * 3 + p;
+  C* dst = (INV ? t1 + (long long)ix * NC * rs : t2 + (long long)ix * LY * rs) + kz0 * 3 + p;
+  cp2* sw = s + p;
+  auto ld = [&](int, int pos) -> cp2 { return cpack(__ldcg(src + pos * rs), __ldcg(src + pos * rs + WP)); };
+  auto sm = [&](int, int pp) -> cp2& { return sw[pp * WP]; };
+  auto stf = [&](int, int pos, cp2 v) {
+    __stcg(dst + pos * rs, clo(v));
+    __stcg(dst + pos * rs + WP, chi(v));
+  };
+  cp2 a[P::E];
+  rfft<P, 1, INV, ZH, DH>(a, t, ld, sm, stf, tw);
+}
+
+// ---------------------------------------------------------------------------
+// passes 1 / 5 on packed pairs (complex64 cubic boxes, no Krylov step fused
+// into the pass): as k_mv_pass1 / k_mv_pass5, with each thread transforming
+// component c of lines l and l + NL/2 of the tile in the two lanes of a cp2.
+// Pass 5 runs its combine per lane, as the scalar kernel does.
+// ---------------------------------------------------------------------------
+template <int LZ>
+struct PZPair {
+  typedef typename PlanFor<LZ, float>::type P;
+  static constexpr int NC = LZ / 2;
+  static constexpr int NL = cmin_i(mv_tiles<float, P::T>(), NC * NC);   // lines per CTA
+  static constexpr int NLP = NL / 2, T = P::T, TH = 3 * T * NLP;
+  static constexpr int LP = ppad_len(LZ);
+  static constexpr size_t smem = (size_t)NLP * 3 * LP * sizeof(cp2);
+  static_assert(NL % 2 == 0 && (NC * NC) % NL == 0, "pairs of lines");
+};
+
+template <int LZ, int MINB>
+__global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
+    k_mv_pass1x(Geo g, const float2* __restrict__ tw, InstState* st, const int* act, int in_id, int cond, int nl_,
+                int pre) {
+  grid_dep_begin();
+  typedef float2 C;
+  typedef PZPair<LZ> PS;
+  typedef typename PS::P P;
+  constexpr int NC = PS::NC, NL = PS::NL, NLP = PS::NLP;
+  constexpr bool ZH = P::r[0] % 2 == 0;
+  static_assert(ZH, "zero-half loads");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cp2* s = reinterpret_cast<cp2*>(smem_raw);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  const C* __restrict__ x = (const C*)S.vec[in_id];
+  C* __restrict__ t1 = (C*)S.t1;
+  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
+  const int t = rest % PS::T, lp = rest / PS::T;
+  const long long la = (long long)blockIdx.x * NL + lp, lb = la + NLP;
+  const int* __restrict__ cid = S.cidx;
+  auto eidx = [&](long long line, int pos) -> long long {
+    if (!cid) return (line * NC + pos) * 3 + c;
+    const int k = cid[line * NC + pos];
+    return k < 0 ? -1 : 3LL * k + c;
+  };
+  auto ld = [&](int, int pos) -> cp2 {
+    const long long ia = eidx(la, pos), ib = eidx(lb, pos);
+    return cpack(ia < 0 ? czero<C>() : __ldcg(x + ia), ib < 0 ? czero<C>() : __ldcg(x + ib));
+  };
+  cp2* sl = s + lp * 3 * PS::LP + c;
+  auto sm = [&](int, int pp) -> cp2& { return sl[pp * 3]; };
+  C* ta = t1 + la * (long long)LZ * 3 + c;
+  C* tb = t1 + lb * (long long)LZ * 3 + c;
+  auto stf = [&](int, int pos, cp2 v) {
+    __stcg(ta + pos * 3, clo(v));
+    __stcg(tb + pos * 3, chi(v));
+  };
+  cp2 a[P::E];
+  rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
+}
+
+template <int LZ, int MINB>
+__global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
+    k_mv_pass5x(Geo g, const float2* __restrict__ tw, InstState* st, const int* act, int in_id, int out_id,
+                int mode, int cond, int nl_, int post, double* red, unsigned* cnt) {
+  grid_dep_begin();
+  typedef float2 C;
+  typedef PZPair<LZ> PS;
+  typedef typename PS::P P;
+  constexpr int NC = PS::NC, NL = PS::NL, NLP = PS::NLP;
+  constexpr bool DH = half_store_ok<P>();
+  static_assert(DH, "half stores");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cp2* s = reinterpret_cast<cp2*>(smem_raw);
+  InstState& S = st[inst_of(act)];
+  if (!cond_ok(S, cond)) return;
+  const C* __restrict__ t1 = (const C*)S.t1;
+  const int c = threadIdx.x % 3, rest = threadIdx.x / 3;
+  const int t = rest % PS::T, lp = rest / PS::T;
+  const long long la = (long long)blockIdx.x * NL + lp, lb = la + NLP;
+  const C* tla = t1 + la * (long long)LZ * 3 + c;
+  const C* tlb = t1 + lb * (long long)LZ * 3 + c;
+  const C* __restrict__ xg = (const C*)S.vec[in_id];
+  C* __restrict__ yg = (C*)S.vec[out_id];
+  const C* __restrict__ iag = (const C*)S.inva;
+  const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] : nullptr;
+  const int* __restrict__ cid = S.cidx;
+  auto ld = [&](int, int pos) -> cp2 { return cpack(__ldcg(tla + pos * 3), __ldcg(tlb + pos * 3)); };
+  cp2* sl = s + lp * 3 * PS::LP + c;
+  auto sm = [&](int, int pp) -> cp2& { return sl[pp * 3]; };
+  // the combine of pass 5 for one element of one line
+  auto comb = [&](long long line, int pos, C v) {
+    const long long site = line * NC + pos;
+    long long e = site * 3 + c;
+    if (cid) {
+      const int k = cid[site];
+      if (k < 0) return;
+      e = 3LL * k + c;
+    }
+    C r;
+    if (mode == MV_CONV) {
+      r = v;
+    } else {
+      const C a_ = __ldg(iag + site);
+      const bool msk = (a_.x != 0.f) || (a_.y != 0.f);
+      if (!msk) v = czero<C>();
+      if (mode == MV_CONV_MASKED) {
+        r = v;
+      } else {
+        r = csub(cmul(a_, __ldcg(xg + e)), v);
+        if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + e), r);
+      }
+    }
+    __stcg(yg + e, r);
+  };
+  auto stf = [&](int, int pos, cp2 v) {
+    comb(la, pos, clo(v));
+    comb(lb, pos, chi(v));
+  };
+  cp2 a[P::E];
+  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
+}
+
+// ---------------------------------------------------------------------------
 // pass 5: inverse z on nl lines, keep z < nz, fused combine:
 //   MV_AX           y = ia*x - mask*conv        (interaction_mult)
 //   MV_RESIDUAL     y = b - (ia*x - mask*conv)  (b already masked)
@@ -951,6 +1122,15 @@ template <typename R> struct MvSet {
   P3 k3x = nullptr;
   int th3x = 0, grid3x = 0;
   size_t smem3x = 0;
+  // packed-pair y passes (complex64 cubic sets)
+  PY k2x = nullptr, k4x = nullptr;
+  int th2x = 0, grid2x = 0;
+  size_t smem2x = 0;
+  // packed-pair z passes (complex64 cubic sets)
+  P1 k1x = nullptr;
+  P5 k5x = nullptr;
+  int th1x = 0, grid1x = 0;
+  size_t smem1x = 0;
 };
 
 // General kernels (sizes from Geo), defined with the instantiations.
@@ -1046,6 +1226,19 @@ void mv_cube_fill(MvSet<R>& o) {
     o.th3x = PX::TH;
     o.grid3x = L * (L / TZ);
     o.smem3x = PX::smem;
+    constexpr int TY = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
+    typedef PYPair<L, TY> PY2;
+    o.k2x = (typename M::PY)k_mv_pass_yx<false, L, NC, TY, (L == 256 ? 4 : 3)>;
+    o.k4x = (typename M::PY)k_mv_pass_yx<true, L, NC, TY, (L == 256 ? 4 : 3)>;
+    o.th2x = PY2::TH;
+    o.grid2x = NC * (L / TY);
+    o.smem2x = PY2::smem;
+    typedef PZPair<L> PZ2;
+    o.k1x = k_mv_pass1x<L, (L == 256 ? 4 : 3)>;
+    o.k5x = k_mv_pass5x<L, (L == 256 ? 4 : 3)>;
+    o.th1x = PZ2::TH;
+    o.grid1x = NC * NC / PZ2::NL;
+    o.smem1x = PZ2::smem;
   }
   if constexpr (sizeof(R) == 8 && V == 2 && (L == 128 || L == 256)) {
     // complex128 64^3 / 128^3: tiles of 8 kz columns (384-byte row
@@ -1098,6 +1291,10 @@ bool p3_pipe_forced();
 // Whether the packed-pair x pass is forced where compiled (DDA_P3PAIR=1;
 // otherwise DDA_TUNE_P3PAIR in the tuning table selects it).
 bool p3_pair_forced();
+// Likewise for the packed-pair y passes (DDA_YPAIR=1 / DDA_TUNE_YPAIR).
+bool y_pair_forced();
+// Likewise for the packed-pair z passes (DDA_ZPAIR=1 / DDA_TUNE_ZPAIR).
+bool z_pair_forced();
 // Streaming multiprocessors of the current device (cached per device).
 int device_sms();
 
@@ -1129,10 +1326,11 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                           const typename CT<R>::T* twx, const typename CT<R>::T* twy, const typename CT<R>::T* twz,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
                           const MvFuse& fz = MvFuse()) {
-  const void* ks[9] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
-                       (const void*)k.k5, (const void*)k.kf, (const void*)k.ki, (const void*)k.k3p,
-                       (const void*)k.k3x};
-  cudaError_t e = mv_prepare(ks, 9);
+  const void* ks[13] = {(const void*)k.k1, (const void*)k.k2, (const void*)k.k3, (const void*)k.k4,
+                        (const void*)k.k5, (const void*)k.kf, (const void*)k.ki, (const void*)k.k3p,
+                        (const void*)k.k3x, (const void*)k.k2x, (const void*)k.k4x, (const void*)k.k1x,
+                        (const void*)k.k5x};
+  cudaError_t e = mv_prepare(ks, 13);
   if (e != cudaSuccess) return e;
   // The fused z/y kernels take the place of passes 1+2 / 4+5 in launches of
   // one instance with no Krylov step fused into those passes (cubic sets use
@@ -1145,17 +1343,29 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   const bool one = nb == 1;
   const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) && !(tf & DDA_TUNE_NO_FUSED_ZY);
   const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
+  const bool ypair = k.k2x && (y_pair_forced() || (tf & DDA_TUNE_YPAIR));
+  const bool zpair = k.k1x && (z_pair_forced() || (tf & DDA_TUNE_ZPAIR));
   if (ff) {
     if ((e = launch_cluster(k.kf, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemf, s, g, twz, st, act,
                             in_id, cond)))
       return e;
   } else {
-    if ((e = launch_pdl(k.k1, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id, cond,
-                        pc.nl, fz.pre)))
+    if (zpair && fz.pre == MV_PRE_NONE) {
+      if ((e = launch_pdl(k.k1x, dim3((unsigned)k.grid1x, nb), dim3(k.th1x), k.smem1x, s, g, twz, st, act, in_id,
+                          cond, pc.nl, fz.pre)))
+        return e;
+    } else if ((e = launch_pdl(k.k1, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act,
+                               in_id, cond, pc.nl, fz.pre))) {
       return e;
-    if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
-                        pc.ntz2)))
+    }
+    if (ypair) {
+      if ((e = launch_pdl(k.k2x, dim3((unsigned)k.grid2x, nb), dim3(k.th2x), k.smem2x, s, g, twy, st, act, cond,
+                          pc.tz2, pc.ntz2)))
+        return e;
+    } else if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond,
+                               pc.tz2, pc.ntz2))) {
       return e;
+    }
   }
   if (k.k3x && (p3_pair_forced() || (tf & DDA_TUNE_P3PAIR))) {
     if ((e = launch_pdl(k.k3x, dim3((unsigned)k.grid3x, nb), dim3(k.th3x), k.smem3x, s, g, twx, st, act, cond,
@@ -1179,12 +1389,22 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                             in_id, out_id, mode, cond)))
       return e;
   } else {
-    if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond, pc.tz2,
-                        pc.ntz2)))
+    if (ypair) {
+      if ((e = launch_pdl(k.k4x, dim3((unsigned)k.grid2x, nb), dim3(k.th2x), k.smem2x, s, g, twy, st, act, cond,
+                          pc.tz2, pc.ntz2)))
+        return e;
+    } else if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond,
+                               pc.tz2, pc.ntz2))) {
       return e;
-    if ((e = launch_pdl(k.k5, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, in_id,
-                        out_id, mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
+    }
+    if (zpair && fz.post == MV_POST_NONE) {
+      if ((e = launch_pdl(k.k5x, dim3((unsigned)k.grid1x, nb), dim3(k.th1x), k.smem1x, s, g, twz, st, act, in_id,
+                          out_id, mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
+        return e;
+    } else if ((e = launch_pdl(k.k5, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act,
+                               in_id, out_id, mode, cond, pc.nl, fz.post, fz.red, fz.cnt))) {
       return e;
+    }
   }
   note_launch(s, 5 - (ff ? 1 : 0) - (fi ? 1 : 0));
   return cudaGetLastError();

@@ -130,9 +130,12 @@ def test_staged_x_pass_equals_one_tile_kernel(n, nb, dtype, monkeypatch):
 
 @pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
 def test_pair_x_pass_matches_one_tile_kernel(n, nb, monkeypatch):
-    """The packed-pair x pass (two transforms per thread in FP32x2 lanes)
-    against the one-tile kernel and the oracle: complex64 rounding only,
-    alone and batched, in the interaction and preconditioner products."""
+    """The packed-pair x, y and z passes (two transforms per thread in
+    FP32x2 lanes) against the one-component kernels and the oracle:
+    complex64 rounding only, alone and batched, in the interaction and
+    preconditioner products (a single-instance 64^3 matvec uses the
+    cluster-fused z/y kernels, so there only the x pass changes; the
+    preconditioner check turns them off)."""
     P = _pkg()
     ops, xs, xn = [], [], []
     for j in range(nb):
@@ -142,11 +145,17 @@ def test_pair_x_pass_matches_one_tile_kernel(n, nb, monkeypatch):
         xs.append(torch.as_tensor(x, device="cuda").to(C64))
         xn.append((ia, k, d, x))
     monkeypatch.setenv("DDA_P3PAIR", "1")
+    monkeypatch.setenv("DDA_YPAIR", "1")
+    monkeypatch.setenv("DDA_ZPAIR", "1")
     a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
     monkeypatch.delenv("DDA_P3PAIR", raising=False)
+    c = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]     # y and z pairs alone
+    monkeypatch.delenv("DDA_YPAIR", raising=False)
+    monkeypatch.delenv("DDA_ZPAIR", raising=False)
     b = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
-    for u, v in zip(a, b):
+    for u, w, v in zip(a, c, b):
         assert _rel(u.cpu().numpy(), v.cpu().numpy()) < 2e-6
+        assert _rel(w.cpu().numpy(), v.cpu().numpy()) < 2e-6
     if n == 64:
         ia, k, d, x = xn[0]
         mask = ia != 0
@@ -155,9 +164,14 @@ def test_pair_x_pass_matches_one_tile_kernel(n, nb, monkeypatch):
         if nb == 1:
             pre = ops[0].preconditioner()
             monkeypatch.setenv("DDA_P3PAIR", "1")
+            monkeypatch.setenv("DDA_YPAIR", "1")
+            monkeypatch.setenv("DDA_ZPAIR", "1")
+            monkeypatch.setenv("DDA_NO_FUSED_ZY", "1")
             pa = pre.apply(xs[0], C64)
-            monkeypatch.delenv("DDA_P3PAIR", raising=False)
+            for v in ("DDA_P3PAIR", "DDA_YPAIR", "DDA_ZPAIR"):
+                monkeypatch.delenv(v, raising=False)
             pb = pre.apply(xs[0], C64)
+            monkeypatch.delenv("DDA_NO_FUSED_ZY", raising=False)
             assert _rel(pa.cpu().numpy(), pb.cpu().numpy()) < 2e-6
 
 
