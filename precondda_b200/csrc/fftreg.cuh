@@ -96,12 +96,27 @@ template <int L> struct PlanFor<L, double> : Plan8<L> {};
 __device__ __forceinline__ constexpr int ppad(int pos) { return DDA_PPAD ? pos + (pos >> 4) : pos; }
 __host__ __device__ constexpr int ppad_len(int L) { return DDA_PPAD ? L + (L >> 4) + 1 : L; }
 
+// A twiddle table: a global-memory pointer (read through the read-only
+// path) or a copy of it in the CTA's shared memory.
+template <class C> struct ShTw {
+  const C* p;
+};
+template <class C> __device__ __forceinline__ C twget(const C* tw, int i) { return __ldg(tw + i); }
+template <class C> __device__ __forceinline__ C twget(ShTw<C> tw, int i) { return tw.p[i]; }
+
+// Copy a length-L table into shared memory (all threads of the CTA; the
+// first exchange's barrier publishes it before any stage reads it).
+template <class C> __device__ __forceinline__ ShTw<C> tw_to_shared(const C* __restrict__ tw, C* dst, int L) {
+  for (int i = threadIdx.x; i < L; i += blockDim.x) dst[i] = __ldg(tw + i);
+  return ShTw<C>{dst};
+}
+
 // Compute stage s of plan P on the thread's registers a[E] (twiddles for
 // s > 0).  Always the forward transform: inverse transforms are run as
 // swap(FFT(swap(x))), swap(a + ib) = b + ia, which costs no instructions.
 // ZH (stage 0 only): the upper half of every butterfly's inputs is zero.
 template <class P, int s, bool ZH = false, class C, class TW>
-__device__ __forceinline__ void rstage(C* a, int t, const TW* __restrict__ tw) {
+__device__ __forceinline__ void rstage(C* a, int t, TW tw) {
   static_assert(!ZH || s == 0, "zero-half inputs only at stage 0");
   constexpr int R = P::r[s];
   constexpr int NS = P::ns(s);
@@ -116,7 +131,7 @@ __device__ __forceinline__ void rstage(C* a, int t, const TW* __restrict__ tw) {
       constexpr int ST = P::L / (NS * R);
       const int k = (t + b * P::T) % NS;
 #pragma unroll
-      for (int m = 1; m < R; ++m) v[m] = cmul(v[m], __ldg(tw + m * k * ST));
+      for (int m = 1; m < R; ++m) v[m] = cmul(v[m], twget(tw, m * k * ST));
     }
     if constexpr (ZH) dft_zh<R>(v);
     else dft<R>(v);
@@ -147,7 +162,7 @@ __device__ __forceinline__ int rout_pos(int t, int b, int q) {
 // component c of this thread's transform.  All threads of the CTA must call
 // this together (it contains barriers).
 template <class P, int NC, int s, class C, class SM, class TW>
-__device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const TW* __restrict__ tw) {
+__device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, TW tw) {
   constexpr int R = P::r[s];
   constexpr int R2 = P::r[s + 1];
 #pragma unroll
@@ -170,7 +185,7 @@ __device__ __forceinline__ void rexchange(C* a, int t, const SM& sm, const TW* _
 
 // Stages s+1..S-1 (stage 0 is computed by the caller after its global load).
 template <class P, int NC, int s, class C, class SM, class TW>
-__device__ __forceinline__ void rrest(C* a, int t, const SM& sm, const TW* __restrict__ tw) {
+__device__ __forceinline__ void rrest(C* a, int t, const SM& sm, TW tw) {
   if constexpr (s + 1 < P::S) {
     rexchange<P, NC, s>(a, t, sm, tw);
     rrest<P, NC, s + 1>(a, t, sm, tw);
@@ -217,8 +232,7 @@ __device__ __forceinline__ void rstore(const C* a, int t, const ST& st) {
 // ZH / DH: zero upper half of the input / only the lower half of the output
 // wanted (see rload / rstore).
 template <class P, int NC, bool INV, bool ZH = false, bool DH = false, class C, class LD, class SM, class ST, class TW>
-__device__ __forceinline__ void rfft(C* a, int t, const LD& ld, const SM& sm, const ST& st,
-                                     const TW* __restrict__ tw) {
+__device__ __forceinline__ void rfft(C* a, int t, const LD& ld, const SM& sm, const ST& st, TW tw) {
   if constexpr (INV) {
     rload<P, NC, ZH>(a, t, [&](int c, int pos) -> C { return cswap(ld(c, pos)); });
   } else {

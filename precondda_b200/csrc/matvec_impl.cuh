@@ -34,6 +34,24 @@ namespace cg = cooperative_groups;
 
 constexpr int kMvMaxThreads = 384;
 
+// DDA_SMEM_TW=1: the transform passes copy their twiddle table into shared
+// memory at entry (after the pass's exchange area) and read it from there
+// instead of through the read-only global path (an A/B build option).
+#ifndef DDA_SMEM_TW
+#define DDA_SMEM_TW 0
+#endif
+// The twiddle source of a pass: the global table, or its shared copy at
+// `at` (n entries).
+template <class C>
+__device__ __forceinline__ auto pass_tw(const C* __restrict__ tw, void* at, int n) {
+#if DDA_SMEM_TW
+  return tw_to_shared(tw, reinterpret_cast<C*>(at), n);
+#else
+  (void)at; (void)n;
+  return tw;
+#endif
+}
+
 template <typename R, int L>
 struct MvShape {
   typedef typename PlanFor<L, R>::type P;
@@ -340,12 +358,13 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   const long long rs = (long long)Ly * Lz * 3;
   C* col = t2 + ((long long)ky * Lz + kz0) * 3 + w;
   C* sw = s + w;
+  const auto twk = pass_tw(tw, s + W * SH::LP, LX);
   auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nx)) ? __ldcg(col + pos * rs) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
   C a[P::E];
   rload<P, 1, ZH>(a, t, ld);
-  rstage<P, 0, ZH>(a, t, tw);
-  rrest<P, 1, 0>(a, t, sm, tw);
+  rstage<P, 0, ZH>(a, t, twk);
+  rrest<P, 1, 0>(a, t, sm, twk);
   constexpr int RL = P::r[P::S - 1];
 #pragma unroll
   for (int b = 0; b < P::E / RL; ++b)
@@ -404,8 +423,8 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
 #pragma unroll
     for (int m = 0; m < R0; ++m) a[b * R0 + m] = cswap(smo(0, ppad(rin_pos<Q, 0>(ti, b, m))));
   __syncthreads();
-  rstage<Q, 0>(a, ti, tw);
-  rrest<Q, 1, 0>(a, ti, smo, tw);
+  rstage<Q, 0>(a, ti, twk);
+  rrest<Q, 1, 0>(a, ti, smo, twk);
   rstore<Q, 1, DH>(a, ti, stf);
 }
 
@@ -427,7 +446,7 @@ struct P3Pair {
   typedef typename PlanFor<LX, float>::type P;
   static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
   static constexpr int LP = ppad_len(LX);
-  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (DDA_SMEM_TW ? LX * sizeof(float2) : 0);
   static_assert(TZ % 2 == 0 && LX % TZ == 0, "pairs of kz columns");
   static_assert(TH <= 1024, "threads per CTA");
 };
@@ -486,6 +505,7 @@ __global__ void __launch_bounds__(P3Pair<LX, TZ>::TH, MINB)
   const int kz0 = kzt * TZ;
   C* col = t2 + ((long long)ky * LX + kz0) * 3;
   cp2* sw = s + p;
+  const auto twk = pass_tw(tw, s + PS::LP * WP, LX);
   auto ld = [&](int, int pos) -> cp2 {
     const C* r = col + pos * rs;
     return cpack(__ldcg(r + p), __ldcg(r + p + WP));
@@ -493,8 +513,8 @@ __global__ void __launch_bounds__(P3Pair<LX, TZ>::TH, MINB)
   auto sm = [&](int, int pp) -> cp2& { return sw[pp * WP]; };
   cp2 a[P::E];
   rload<P, 1, ZH>(a, t, ld);
-  rstage<P, 0, ZH>(a, t, tw);
-  rrest<P, 1, 0>(a, t, sm, tw);
+  rstage<P, 0, ZH>(a, t, twk);
+  rrest<P, 1, 0>(a, t, sm, twk);
   constexpr int RL = P::r[P::S - 1];
 #pragma unroll
   for (int b = 0; b < P::E / RL; ++b)
@@ -556,8 +576,8 @@ __global__ void __launch_bounds__(P3Pair<LX, TZ>::TH, MINB)
 #pragma unroll
     for (int m = 0; m < R0; ++m) a[b * R0 + m] = cswap(smo(0, ppad(rin_pos<Q, 0>(ti, b, m))));
   __syncthreads();
-  rstage<Q, 0>(a, ti, tw);
-  rrest<Q, 1, 0>(a, ti, smo, tw);
+  rstage<Q, 0>(a, ti, twk);
+  rrest<Q, 1, 0>(a, ti, smo, twk);
   rstore<Q, 1, DH>(a, ti, stf);
 }
 
@@ -726,7 +746,7 @@ struct PYPair {
   typedef typename PlanFor<LY, float>::type P;
   static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
   static constexpr int LP = ppad_len(LY);
-  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (DDA_SMEM_TW ? LY * sizeof(float2) : 0);
   static_assert(TZ % 2 == 0 && LY % TZ == 0, "pairs of kz columns");
 };
 
@@ -756,6 +776,7 @@ __global__ void __launch_bounds__(PYPair<LY, TZ>::TH, MINB)
   const C* src = (INV ? t2 + (long long)ix * LY * rs : t1 + (long long)ix * NC * rs) + kz0 * 3 + p;
   C* dst = (INV ? t1 + (long long)ix * NC * rs : t2 + (long long)ix * LY * rs) + kz0 * 3 + p;
   cp2* sw = s + p;
+  const auto twk = pass_tw(tw, s + PS::LP * WP, LY);
   auto ld = [&](int, int pos) -> cp2 { return cpack(__ldcg(src + pos * rs), __ldcg(src + pos * rs + WP)); };
   auto sm = [&](int, int pp) -> cp2& { return sw[pp * WP]; };
   auto stf = [&](int, int pos, cp2 v) {
@@ -763,7 +784,7 @@ __global__ void __launch_bounds__(PYPair<LY, TZ>::TH, MINB)
     __stcg(dst + pos * rs + WP, chi(v));
   };
   cp2 a[P::E];
-  rfft<P, 1, INV, ZH, DH>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, INV, ZH, DH>(a, t, ld, sm, stf, twk);
 }
 
 // ---------------------------------------------------------------------------
@@ -779,7 +800,7 @@ struct PZPair {
   static constexpr int NL = cmin_i(mv_tiles<float, P::T>(), NC * NC);   // lines per CTA
   static constexpr int NLP = NL / 2, T = P::T, TH = 3 * T * NLP;
   static constexpr int LP = ppad_len(LZ);
-  static constexpr size_t smem = (size_t)NLP * 3 * LP * sizeof(cp2);
+  static constexpr size_t smem = (size_t)NLP * 3 * LP * sizeof(cp2) + (DDA_SMEM_TW ? LZ * sizeof(float2) : 0);
   static_assert(NL % 2 == 0 && (NC * NC) % NL == 0, "pairs of lines");
 };
 
@@ -813,6 +834,7 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
     const long long ia = eidx(la, pos), ib = eidx(lb, pos);
     return cpack(ia < 0 ? czero<C>() : __ldcg(x + ia), ib < 0 ? czero<C>() : __ldcg(x + ib));
   };
+  const auto twk = pass_tw(tw, s + NLP * 3 * PS::LP, LZ);
   cp2* sl = s + lp * 3 * PS::LP + c;
   auto sm = [&](int, int pp) -> cp2& { return sl[pp * 3]; };
   C* ta = t1 + la * (long long)LZ * 3 + c;
@@ -822,7 +844,7 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
     __stcg(tb + pos * 3, chi(v));
   };
   cp2 a[P::E];
-  rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, false, ZH, false>(a, t, ld, sm, stf, twk);
 }
 
 template <int LZ, int MINB>
@@ -852,6 +874,7 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
   const C* __restrict__ bg = (mode == MV_RESIDUAL) ? (const C*)S.vec[V_B] : nullptr;
   const int* __restrict__ cid = S.cidx;
   auto ld = [&](int, int pos) -> cp2 { return cpack(__ldcg(tla + pos * 3), __ldcg(tlb + pos * 3)); };
+  const auto twk = pass_tw(tw, s + NLP * 3 * PS::LP, LZ);
   cp2* sl = s + lp * 3 * PS::LP + c;
   auto sm = [&](int, int pp) -> cp2& { return sl[pp * 3]; };
   // the combine of pass 5 for one element of one line
@@ -884,7 +907,7 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
     comb(lb, pos, chi(v));
   };
   cp2 a[P::E];
-  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, tw);
+  rfft<P, 1, true, false, DH>(a, t, ld, sm, stf, twk);
 }
 
 // ---------------------------------------------------------------------------
@@ -1485,13 +1508,13 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   const long long nlines = (long long)g.nx * g.ny;
   c.nl = (int)std::min<long long>(std::max(1, LN / T), nlines);
   c.th1 = 3 * T * c.nl;
-  c.smem1 = (size_t)c.nl * 3 * LP * esz;
+  c.smem1 = (size_t)c.nl * 3 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Lz * esz : 0);
   c.grid1 = (nlines + c.nl - 1) / c.nl;
   // y passes: tz kz columns, 3*tz transforms of T threads
   tile_dims<R>(g.Ly, T, LP);
   c.tz2 = std::min(std::max(1, LN / T), g.Lz);
   c.th2 = 3 * c.tz2 * T;
-  c.smem2 = (size_t)3 * c.tz2 * LP * esz;
+  c.smem2 = (size_t)3 * c.tz2 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Ly * esz : 0);
   c.ntz2 = (g.Lz + c.tz2 - 1) / c.tz2;
   c.grid2 = (long long)g.nx * c.ntz2;
   // x pass
@@ -1500,7 +1523,7 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   c.p3reg = c.p3var == 1;
   c.tz3 = std::min(std::max(1, LN / T), g.Lz);
   c.th3 = (c.p3reg ? 1 : 3) * c.tz3 * T;
-  c.smem3 = (size_t)3 * c.tz3 * LP * esz;
+  c.smem3 = (size_t)3 * c.tz3 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Lx * esz : 0);
   c.ntz3 = (g.Lz + c.tz3 - 1) / c.tz3;
   c.grid3 = (long long)g.Ly * c.ntz3;
   return c;
