@@ -34,22 +34,30 @@ namespace cg = cooperative_groups;
 
 constexpr int kMvMaxThreads = 384;
 
-// DDA_SMEM_TW=1: the transform passes copy their twiddle table into shared
-// memory at entry (after the pass's exchange area) and read it from there
-// instead of through the read-only global path (an A/B build option).
-#ifndef DDA_SMEM_TW
-#define DDA_SMEM_TW 0
+// Twiddle tables in shared memory: the transform passes of a precision
+// with the switch on copy their table there at entry (after the pass's
+// exchange area) and read it from there instead of through the read-only
+// global path.  B200, 128^3 matvec: complex128 1.434 -> 1.322 ms (on);
+// complex64 0.5412 -> 0.5406 ms (off: no gain).  DDA_SMEM_TW_C64 /
+// DDA_SMEM_TW_C128 override.
+#ifndef DDA_SMEM_TW_C64
+#define DDA_SMEM_TW_C64 0
 #endif
+#ifndef DDA_SMEM_TW_C128
+#define DDA_SMEM_TW_C128 1
+#endif
+// whether the passes of complex elements of `bytes` bytes stage twiddles
+__host__ __device__ constexpr bool smem_tw(int bytes) { return bytes == 16 ? DDA_SMEM_TW_C128 : DDA_SMEM_TW_C64; }
 // The twiddle source of a pass: the global table, or its shared copy at
 // `at` (n entries).
 template <class C>
 __device__ __forceinline__ auto pass_tw(const C* __restrict__ tw, void* at, int n) {
-#if DDA_SMEM_TW
-  return tw_to_shared(tw, reinterpret_cast<C*>(at), n);
-#else
-  (void)at; (void)n;
-  return tw;
-#endif
+  if constexpr (smem_tw((int)sizeof(C))) {
+    return tw_to_shared(tw, reinterpret_cast<C*>(at), n);
+  } else {
+    (void)at; (void)n;
+    return tw;
+  }
 }
 
 template <typename R, int L>
@@ -77,7 +85,11 @@ __device__ __forceinline__ int inst_of(const int* act) { return act ? act[blockI
 // about 128 (complex64) or 64 (complex128) transforms' worth of threads per
 // CTA.
 // ---------------------------------------------------------------------------
-template <typename R> constexpr int mv_lanes() { return sizeof(R) == 4 ? 128 : 64; }
+// DDA_C128_LANES overrides the complex128 width (an A/B build option).
+#ifndef DDA_C128_LANES
+#define DDA_C128_LANES 64
+#endif
+template <typename R> constexpr int mv_lanes() { return sizeof(R) == 4 ? 128 : DDA_C128_LANES; }
 constexpr int cmin_i(int a, int b) { return a < b ? a : b; }
 template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T > 1 ? mv_lanes<R>() / T : 1; }
 
@@ -446,7 +458,7 @@ struct P3Pair {
   typedef typename PlanFor<LX, float>::type P;
   static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
   static constexpr int LP = ppad_len(LX);
-  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (DDA_SMEM_TW ? LX * sizeof(float2) : 0);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (smem_tw(8) ? LX * sizeof(float2) : 0);
   static_assert(TZ % 2 == 0 && LX % TZ == 0, "pairs of kz columns");
   static_assert(TH <= 1024, "threads per CTA");
 };
@@ -746,7 +758,7 @@ struct PYPair {
   typedef typename PlanFor<LY, float>::type P;
   static constexpr int W = 3 * TZ, WP = W / 2, T = P::T, TH = WP * T;
   static constexpr int LP = ppad_len(LY);
-  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (DDA_SMEM_TW ? LY * sizeof(float2) : 0);
+  static constexpr size_t smem = (size_t)LP * WP * sizeof(cp2) + (smem_tw(8) ? LY * sizeof(float2) : 0);
   static_assert(TZ % 2 == 0 && LY % TZ == 0, "pairs of kz columns");
 };
 
@@ -800,7 +812,7 @@ struct PZPair {
   static constexpr int NL = cmin_i(mv_tiles<float, P::T>(), NC * NC);   // lines per CTA
   static constexpr int NLP = NL / 2, T = P::T, TH = 3 * T * NLP;
   static constexpr int LP = ppad_len(LZ);
-  static constexpr size_t smem = (size_t)NLP * 3 * LP * sizeof(cp2) + (DDA_SMEM_TW ? LZ * sizeof(float2) : 0);
+  static constexpr size_t smem = (size_t)NLP * 3 * LP * sizeof(cp2) + (smem_tw(8) ? LZ * sizeof(float2) : 0);
   static_assert(NL % 2 == 0 && (NC * NC) % NL == 0, "pairs of lines");
 };
 
@@ -1508,13 +1520,13 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   const long long nlines = (long long)g.nx * g.ny;
   c.nl = (int)std::min<long long>(std::max(1, LN / T), nlines);
   c.th1 = 3 * T * c.nl;
-  c.smem1 = (size_t)c.nl * 3 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Lz * esz : 0);
+  c.smem1 = (size_t)c.nl * 3 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Lz * esz : 0);
   c.grid1 = (nlines + c.nl - 1) / c.nl;
   // y passes: tz kz columns, 3*tz transforms of T threads
   tile_dims<R>(g.Ly, T, LP);
   c.tz2 = std::min(std::max(1, LN / T), g.Lz);
   c.th2 = 3 * c.tz2 * T;
-  c.smem2 = (size_t)3 * c.tz2 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Ly * esz : 0);
+  c.smem2 = (size_t)3 * c.tz2 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Ly * esz : 0);
   c.ntz2 = (g.Lz + c.tz2 - 1) / c.tz2;
   c.grid2 = (long long)g.nx * c.ntz2;
   // x pass
@@ -1523,7 +1535,7 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   c.p3reg = c.p3var == 1;
   c.tz3 = std::min(std::max(1, LN / T), g.Lz);
   c.th3 = (c.p3reg ? 1 : 3) * c.tz3 * T;
-  c.smem3 = (size_t)3 * c.tz3 * LP * esz + (DDA_SMEM_TW ? (size_t)g.Lx * esz : 0);
+  c.smem3 = (size_t)3 * c.tz3 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Lx * esz : 0);
   c.ntz3 = (g.Lz + c.tz3 - 1) / c.tz3;
   c.grid3 = (long long)g.Ly * c.ntz3;
   return c;

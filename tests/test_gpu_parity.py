@@ -103,9 +103,11 @@ def test_cubic_kernels_launch_and_match_general(n, dtype, tol, monkeypatch):
 @pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
 def test_staged_x_pass_equals_one_tile_kernel(n, nb, dtype, monkeypatch):
     """The staged persistent x pass (bulk-copied input tiles, one tile
-    ahead) does the arithmetic of the one-tile-per-CTA kernel: equal bit for
-    bit, alone and in batched launches (several instances per launch), in
-    the interaction and preconditioner products."""
+    ahead) does the arithmetic of the one-tile-per-CTA kernel: equal to
+    rounding (the compiler may contract a complex product's multiply-add
+    differently in the two kernels), alone and in batched launches (several
+    instances per launch), in the interaction and preconditioner
+    products."""
     P = _pkg()
     ops, xs = [], []
     for j in range(nb):
@@ -117,15 +119,16 @@ def test_staged_x_pass_equals_one_tile_kernel(n, nb, dtype, monkeypatch):
     a = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
     monkeypatch.delenv("DDA_P3PIPE", raising=False)
     b = P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    tol = 2e-6 if dtype == C64 else 1e-13
     for u, v in zip(a, b):
-        assert torch.equal(u, v)
+        assert _rel(u.cpu().numpy(), v.cpu().numpy()) < tol
     if nb == 1 and n == 64:
         pre = ops[0].preconditioner()
         monkeypatch.setenv("DDA_P3PIPE", "1")
         pa = pre.apply(xs[0], dtype)
         monkeypatch.delenv("DDA_P3PIPE", raising=False)
         pb = pre.apply(xs[0], dtype)
-        assert torch.equal(pa, pb)
+        assert _rel(pa.cpu().numpy(), pb.cpu().numpy()) < tol
 
 
 @pytest.mark.parametrize("n,nb", [(64, 1), (64, 3), (128, 1), (128, 2)])
