@@ -89,9 +89,18 @@ __device__ __forceinline__ int inst_of(const int* act) { return act ? act[blockI
 #ifndef DDA_C128_LANES
 #define DDA_C128_LANES 64
 #endif
-template <typename R> constexpr int mv_lanes() { return sizeof(R) == 4 ? 128 : DDA_C128_LANES; }
+// Complex128 transforms of 32 or more threads (the radix-8 plans of L >=
+// 256) take twice the lanes: 4-column tiles, 192-byte row segments.  B200,
+// 128^3 complex128 matvec 1.323 -> 1.255 ms; at L = 128 the wider tiles were
+// slower (64^3: 0.150 -> 0.154 ms), so shorter transforms keep 64.
+#ifndef DDA_C128_WIDE_LANES
+#define DDA_C128_WIDE_LANES 128
+#endif
+template <typename R> constexpr int mv_lanes_t(int T) {
+  return sizeof(R) == 4 ? 128 : (T >= 32 ? DDA_C128_WIDE_LANES : DDA_C128_LANES);
+}
 constexpr int cmin_i(int a, int b) { return a < b ? a : b; }
-template <typename R, int T> constexpr int mv_tiles() { return mv_lanes<R>() / T > 1 ? mv_lanes<R>() / T : 1; }
+template <typename R, int T> constexpr int mv_tiles() { return mv_lanes_t<R>(T) / T > 1 ? mv_lanes_t<R>(T) / T : 1; }
 
 // NC > 0 selects the cubic specialisation of a pass: box NC^3 on the FFT
 // grid (2 NC)^3, every size a compile-time constant, so shared-memory and
@@ -963,7 +972,10 @@ template <typename R, int L>
 struct FusedZY {
   typedef MvShape<R, L> SH;
   typedef typename SH::P P;
-  static constexpr int CL = 4;                  // CTAs per cluster (one x slab)
+  // CTAs per cluster (one x slab) and CTAs per SM: 4 and 2 for L = 128
+  // (64^3), 8 and 1 for L = 256 (128^3; about 200 KB of shared memory each)
+  static constexpr int CL = L >= 256 ? 8 : 4;
+  static constexpr int MINB = L >= 256 ? 1 : 2;
   static constexpr int NC = L / 2;              // box edge
   static constexpr int YR = NC / CL;            // z lines (rows y) per CTA
   static constexpr int KB = L / CL;             // kz columns per CTA
@@ -976,14 +988,15 @@ struct FusedZY {
   typedef typename CT<R>::T C;
   static constexpr size_t smem_fwd = (size_t)(NC * BWF + XS) * sizeof(C);
   static constexpr size_t smem_inv = (size_t)(YR * BWI + XS) * sizeof(C);
-  static_assert(NC % CL == 0 && KB % TZ == 0 && TH <= kMvMaxThreads, "cluster tiling");
+  static_assert(NC % CL == 0 && KB % TZ == 0 && TH <= 1024, "cluster tiling");
   static_assert(P::r[0] % 2 == 0 && half_store_ok<P>(), "zero-half loads and half stores");
-  // two CTAs per SM: shared memory for both, registers capped by the launch bounds
-  static_assert(smem_fwd <= 110 * 1024 && smem_inv <= 110 * 1024, "two CTAs per SM");
+  // MINB CTAs per SM: shared memory for all of them, registers capped by the launch bounds
+  static_assert(smem_fwd <= (MINB == 2 ? 110 : 226) * 1024 && smem_inv <= (MINB == 2 ? 110 : 226) * 1024,
+                "CTAs per SM");
 };
 
 template <typename R, int L>
-__global__ void __launch_bounds__(FusedZY<R, L>::TH, 2) k_mv_fwd_zy(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void __launch_bounds__(FusedZY<R, L>::TH, FusedZY<R, L>::MINB) k_mv_fwd_zy(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                                  InstState* st, const int* act, int in_id,
                                                                  int cond) {
   grid_dep_begin();
@@ -1045,7 +1058,7 @@ __global__ void __launch_bounds__(FusedZY<R, L>::TH, 2) k_mv_fwd_zy(Geo g, const
 }
 
 template <typename R, int L>
-__global__ void __launch_bounds__(FusedZY<R, L>::TH, 2) k_mv_inv_yz(Geo g, const typename CT<R>::T* __restrict__ tw,
+__global__ void __launch_bounds__(FusedZY<R, L>::TH, FusedZY<R, L>::MINB) k_mv_inv_yz(Geo g, const typename CT<R>::T* __restrict__ tw,
                                                                  InstState* st, const int* act, int in_id,
                                                                  int out_id, int mode, int cond) {
   grid_dep_begin();
@@ -1147,6 +1160,7 @@ template <typename R> struct MvSet {
   PF kf = nullptr; PI ki = nullptr;
   int cl = 0, thf = 0, gridf = 0;
   size_t smemf = 0, smemi = 0;
+  bool fused_any = false;        // fused passes also in batched launches
   // staged persistent x pass (cubic sets only): threads, tiles per
   // instance, dynamic shared memory, CTAs per SM it is built for
   P3 k3p = nullptr;
@@ -1287,9 +1301,12 @@ void mv_cube_fill(MvSet<R>& o) {
     o.minb3p = MB;
     o.smem3p = PP::smem;
   }
-  if constexpr (sizeof(R) == 4 && L == 128) {
-    // complex64 64^3: both fused buffers fit two CTAs per SM
+  if constexpr (sizeof(R) == 4 && (L == 128 || L == 256)) {
+    // complex64 64^3: both fused buffers fit two CTAs per SM; 128^3: one CTA
+    // per SM in clusters of eight, and T1 (151 MB, beyond L2) is neither
+    // written nor read, so the fused passes also serve batched launches
     typedef FusedZY<R, L> F;
+    o.fused_any = L == 256;
     o.kf = k_mv_fwd_zy<R, L>;
     o.ki = k_mv_inv_yz<R, L>;
     o.cl = F::CL;
@@ -1375,7 +1392,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   // kernels hold two CTAs per SM), so batched launches keep the separate
   // passes.
   const int tf = tune_flags(sizeof(R) == 8 ? DDA_C128 : DDA_C64, g, nb);
-  const bool one = nb == 1;
+  const bool one = nb == 1 || k.fused_any;
   const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) && !(tf & DDA_TUNE_NO_FUSED_ZY);
   const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
   const bool ypair = k.k2x && (y_pair_forced() || (tf & DDA_TUNE_YPAIR));
@@ -1473,8 +1490,6 @@ cudaError_t launch_matvec_tw_impl(const Geo& g, const PassCfg& pc, InstState* st
 
 // Tile shapes: about 128 (complex64) or 64 (complex128) transforms' worth of
 // threads per CTA, at most one tile dimension's extent.
-template <typename R>
-static int lanes() { return mv_lanes<R>(); }
 
 template <typename R>
 static bool tile_dims(int L, int& T, int& LP) {
@@ -1514,17 +1529,16 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   PassCfg c{};
   const size_t esz = sizeof(R) * 2;
   int T, LP;
-  const int LN = lanes<R>();
   // z passes: nl lines x 3 components, 3*T threads per line
   tile_dims<R>(g.Lz, T, LP);
   const long long nlines = (long long)g.nx * g.ny;
-  c.nl = (int)std::min<long long>(std::max(1, LN / T), nlines);
+  c.nl = (int)std::min<long long>(std::max(1, mv_lanes_t<R>(T) / T), nlines);
   c.th1 = 3 * T * c.nl;
   c.smem1 = (size_t)c.nl * 3 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Lz * esz : 0);
   c.grid1 = (nlines + c.nl - 1) / c.nl;
   // y passes: tz kz columns, 3*tz transforms of T threads
   tile_dims<R>(g.Ly, T, LP);
-  c.tz2 = std::min(std::max(1, LN / T), g.Lz);
+  c.tz2 = std::min(std::max(1, mv_lanes_t<R>(T) / T), g.Lz);
   c.th2 = 3 * c.tz2 * T;
   c.smem2 = (size_t)3 * c.tz2 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Ly * esz : 0);
   c.ntz2 = (g.Lz + c.tz2 - 1) / c.tz2;
@@ -1533,7 +1547,7 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   c.p3var = p3_variant<R>();
   tile_dims3<R>(g.Lx, c.p3var, T, LP);
   c.p3reg = c.p3var == 1;
-  c.tz3 = std::min(std::max(1, LN / T), g.Lz);
+  c.tz3 = std::min(std::max(1, mv_lanes_t<R>(T) / T), g.Lz);
   c.th3 = (c.p3reg ? 1 : 3) * c.tz3 * T;
   c.smem3 = (size_t)3 * c.tz3 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Lx * esz : 0);
   c.ntz3 = (g.Lz + c.tz3 - 1) / c.tz3;

@@ -450,3 +450,41 @@ def test_cluster_fused_zy_passes_equal_separate(monkeypatch):
     Gref = O.generate_interaction_row(*shape, k, d, L=op.L)
     ref = O.interaction_mult(x, Gref, ia, mask, L=op.L)
     assert _rel(fused[0][0].cpu().numpy(), ref) < 2e-5
+
+
+@pytest.mark.parametrize("nb", [1, 2])
+def test_fused_zy_passes_128_match_separate(nb, monkeypatch):
+    """The 128^3 cluster-fused z/y kernels (clusters of eight, one CTA per
+    SM, T1 kept on chip; used for batched launches too) against the separate
+    passes in every product mode, and the first mode against the oracle."""
+    P = _pkg()
+    from precondda_b200 import _lib as L
+    shape = (128, 128, 128)
+    ops, xs = [], []
+    for j in range(nb):
+        k, d, alpha, x = _rand_problem(shape, seed=128 + j, fill=0.4)
+        ia = np.where(alpha != 0, 1.0 / np.where(alpha != 0, alpha, 1), 0)
+        ops.append(P.DDAOperator(ia, k, d, dtype=C64))
+        xs.append(torch.as_tensor(x, device="cuda").to(C64))
+    assert tuple(ops[0].L) == (256, 256, 256)
+    bs = [x.flip(0).contiguous() for x in xs]
+
+    def run():
+        out = []
+        for m in (L.MV_AX, L.MV_RESIDUAL, L.MV_CONV, L.MV_CONV_MASKED):
+            b = bs if m == L.MV_RESIDUAL else None
+            out.append(P.engine.matvec_batch(ops, xs, mode=m, bs=b) if nb > 1 else
+                       [ops[0]._mv(m, xs[0], b[0] if b else None)])
+        return out
+
+    fused = run()
+    monkeypatch.setenv("DDA_NO_FUSED_ZY", "1")
+    sep = run()
+    for fm, sm in zip(fused, sep):
+        for f, s in zip(fm, sm):
+            assert _rel(f.cpu().numpy(), s.cpu().numpy()) < 2e-6
+    if nb == 1:
+        k, d, alpha, x = _rand_problem(shape, seed=128, fill=0.4)
+        ia = np.where(alpha != 0, 1.0 / np.where(alpha != 0, alpha, 1), 0)
+        ref = O.interaction_mult(x, O.generate_interaction_row(*shape, k, d), ia, ia != 0)
+        assert _rel(fused[0][0].cpu().numpy(), ref) < 2e-5
