@@ -383,8 +383,9 @@ def run_ours(args, ws, rank, local):
     # launch variants of the buckets the timed work runs, measured before it
     from precondda_b200.batch import LaunchTuner
     tuner = LaunchTuner(device=dev)
-    tuner.tune(op.shape, op.L, torch.complex64, 2)
-    tuner.tune((128,) * 3, (256,) * 3, torch.complex64, 16)
+    if not args.no_tune:
+        tuner.tune(op.shape, op.L, torch.complex64, 2)
+        tuner.tune((128,) * 3, (256,) * 3, torch.complex64, 16)
 
     def step(precision="mixed", preconditioner=pre, tol=TOL):
         return P.solve_many([op, op], Es_dev, tol=tol, max_iter=MAX_ITER, ratio=RATIO, precision=precision,
@@ -917,6 +918,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="default workload: no launch-variant tuning (the defaults; for profiler captures, whose "
+                         "serialised timing would mislead the tuner)")
     ap.add_argument("--no-extra", action="store_true",
                     help="default workload: only the timed solves and e2e (no extra blocks; for launch-list captures)")
     ap.add_argument("--profile-matvec", type=int, default=0, help="only run matvecs on an n^3 box (for ncu)")

@@ -167,6 +167,8 @@ int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz
  *                          arithmetic, complex64 cubic 64^3 / 128^3 boxes)
  *   DDA_TUNE_YPAIR         the y passes on packed pairs likewise
  *   DDA_TUNE_ZPAIR         the z passes on packed pairs likewise
+ *   DDA_TUNE_FUSED         the cluster-fused z/y passes where they are off
+ *                          by default (128^3 boxes, launches of any width)
  * dda_tuning_set with flags < 0 removes the entry; dda_tuning_get returns
  * DDA_ERR_ARG when there is none.  Entries apply to launches made after
  * the call (a captured iteration graph keeps the variant it was captured
@@ -178,6 +180,7 @@ int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz
 #define DDA_TUNE_P3PAIR 16
 #define DDA_TUNE_YPAIR 32
 #define DDA_TUNE_ZPAIR 64
+#define DDA_TUNE_FUSED 128
 int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int flags);
 int dda_tuning_get(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int* flags);
 

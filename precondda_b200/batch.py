@@ -146,7 +146,8 @@ def launch_candidates(box, L_, dtype, nb):
     pass, with the plain or packed-pair y and z passes (cubic complex64 boxes on
     the (2n)^3 grid of 64^3 and 128^3, where those kernels are built),
     each with and without the cluster-fused z/y passes (one-instance 64^3
-    and any 128^3 complex64 launches, where those are built)."""
+    complex64 launches, where they are the default, and any 128^3 complex64
+    launch, where they are not)."""
     cube = box[0] == box[1] == box[2] and L_[0] == L_[1] == L_[2] == 2 * box[0]
     x_opts = [0]
     if cube and dtype == _C64 and L_[0] in (128, 256):
@@ -155,8 +156,10 @@ def launch_candidates(box, L_, dtype, nb):
     if cube and dtype == _C64 and L_[0] in (128, 256):
         y_opts = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
     zy_opts = [0]
-    if cube and dtype == _C64 and ((L_[0] == 128 and nb == 1) or L_[0] == 256):
+    if cube and dtype == _C64 and L_[0] == 128 and nb == 1:
         zy_opts = [0, L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV]
+    elif cube and dtype == _C64 and L_[0] == 256:
+        zy_opts = [0, L.DDA_TUNE_FUSED]
     return [a | y | b for a in x_opts for y in y_opts for b in zy_opts]
 
 

@@ -1303,8 +1303,10 @@ void mv_cube_fill(MvSet<R>& o) {
   }
   if constexpr (sizeof(R) == 4 && (L == 128 || L == 256)) {
     // complex64 64^3: both fused buffers fit two CTAs per SM; 128^3: one CTA
-    // per SM in clusters of eight, and T1 (151 MB, beyond L2) is neither
-    // written nor read, so the fused passes also serve batched launches
+    // per SM in clusters of eight (T1, 151 MB and beyond L2, is neither
+    // written nor read), for launches of any width, but only where the
+    // tuning table selects them (DDA_TUNE_FUSED): B200, 128^3 matvec 0.679
+    // against 0.542 ms with the separate passes
     typedef FusedZY<R, L> F;
     o.fused_any = L == 256;
     o.kf = k_mv_fwd_zy<R, L>;
@@ -1392,7 +1394,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   // kernels hold two CTAs per SM), so batched launches keep the separate
   // passes.
   const int tf = tune_flags(sizeof(R) == 8 ? DDA_C128 : DDA_C64, g, nb);
-  const bool one = nb == 1 || k.fused_any;
+  const bool one = k.fused_any ? (tf & DDA_TUNE_FUSED) != 0 : nb == 1;
   const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) && !(tf & DDA_TUNE_NO_FUSED_ZY);
   const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
   const bool ypair = k.k2x && (y_pair_forced() || (tf & DDA_TUNE_YPAIR));

@@ -240,21 +240,22 @@ def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     xs = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_P3PAIR]
     ys = (0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR)
     assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [x | y | z for x in xs for y in ys for z in (0, zy)]
-    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == [x | y | z for x in xs for y in ys for z in (0, zy)]
+    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == [
+        x | y | z for x in xs for y in ys for z in (0, L.DDA_TUNE_FUSED)]
     assert launch_candidates((40, 30, 20), (80, 64, 40), c64, 4) == [0]
     assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0]
     calls = []
 
     def timer(box, L_, dtype, nb, flags):
         calls.append(flags)
-        base = flags & ~(L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR | zy)
+        base = flags & ~(L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR | L.DDA_TUNE_FUSED)
         return {0: 3.0, L.DDA_TUNE_P3PIPE_1SM: 2.0, L.DDA_TUNE_P3PIPE: 2.5, L.DDA_TUNE_P3PAIR: 2.2}[base] + \
-            (0.1 if flags & L.DDA_TUNE_YPAIR else 0.0) + (0.05 if flags & zy else 0.0)
+            (0.1 if flags & L.DDA_TUNE_YPAIR else 0.0) + (0.05 if flags & L.DDA_TUNE_FUSED else 0.0)
 
     path = str(tmp_path / "launch.json")
     t = LaunchTuner(cache_path=path, timer=timer)
     assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
-    assert sorted(calls) == sorted(x | y | z for x in xs for y in ys for z in (0, zy))
+    assert sorted(calls) == sorted(x | y | z for x in xs for y in ys for z in (0, L.DDA_TUNE_FUSED))
     assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
     assert len(calls) == 16                      # cached
     assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == 16  # single candidate: no timing

@@ -455,8 +455,9 @@ def test_cluster_fused_zy_passes_equal_separate(monkeypatch):
 @pytest.mark.parametrize("nb", [1, 2])
 def test_fused_zy_passes_128_match_separate(nb, monkeypatch):
     """The 128^3 cluster-fused z/y kernels (clusters of eight, one CTA per
-    SM, T1 kept on chip; used for batched launches too) against the separate
-    passes in every product mode, and the first mode against the oracle."""
+    SM, T1 kept on chip; for launches of any width, where the tuning table
+    selects them) against the separate passes in every product mode, and
+    the first mode against the oracle."""
     P = _pkg()
     from precondda_b200 import _lib as L
     shape = (128, 128, 128)
@@ -477,9 +478,16 @@ def test_fused_zy_passes_128_match_separate(nb, monkeypatch):
                        [ops[0]._mv(m, xs[0], b[0] if b else None)])
         return out
 
-    fused = run()
-    monkeypatch.setenv("DDA_NO_FUSED_ZY", "1")
     sep = run()
+    from precondda_b200 import _lib as LL
+    code = LL.DDA_C64
+    for nbk in (1, nb):
+        LL.check(LL.lib().dda_tuning_set(code, *shape, 256, 256, 256, nbk, LL.DDA_TUNE_FUSED))
+    try:
+        fused = run()
+    finally:
+        for nbk in (1, nb):
+            LL.lib().dda_tuning_set(code, *shape, 256, 256, 256, nbk, -1)
     for fm, sm in zip(fused, sep):
         for f, s in zip(fm, sm):
             assert _rel(f.cpu().numpy(), s.cpu().numpy()) < 2e-6
