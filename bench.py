@@ -718,8 +718,9 @@ def run_batch64(args, ws, rank, local):
     per_bucket = {}
     for s_, (box, L_) in zip(specs, plan):
         per_bucket[(box, L_)] = per_bucket.get((box, L_), 0) + len(s_["dirs"]) * s_.get("pols", 2)
-    for (box, L_), nrhs in per_bucket.items():
-        ltun.tune(box, L_, torch.complex64, nrhs)
+    if not args.no_tune:
+        for (box, L_), nrhs in per_bucket.items():
+            ltun.tune(box, L_, torch.complex64, nrhs)
     # untimed warm-up: every geometry's bucket with one right-hand side, so the
     # timed pass does not pay first launches of its kernel sizes, pool graph
     # captures or the memory pool's first growth
@@ -864,7 +865,8 @@ def run_serve(args, ws, rank, local):
     rates = [float(v) for v in str(args.rates).split(",")] if args.rates else [args.rate]
     from precondda_b200.batch import LaunchTuner
     srv = DDAServer(precision="mixed", slots_per_bucket=args.slots, chunk_iters=args.chunk, device=dev,
-                    precondition=not args.no_precondition, launch_tuner=LaunchTuner(device=dev))
+                    precondition=not args.no_precondition,
+                    launch_tuner=None if args.no_tune else LaunchTuner(device=dev))
     # warm the kernels of every bucket outside the timed region
     warm = sorted({srv.bucket_for(sp["box"]) for r in rates
                    for _, sp in serving_stream(50 + rank, rate=r, duration=args.duration)})
@@ -919,8 +921,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-tune", action="store_true",
-                    help="default workload: no launch-variant tuning (the defaults; for profiler captures, whose "
-                         "serialised timing would mislead the tuner)")
+                    help="no launch-variant tuning, the defaults (for profiler captures, whose serialised "
+                         "timing would mislead the tuner, and A/B runs)")
     ap.add_argument("--no-extra", action="store_true",
                     help="default workload: only the timed solves and e2e (no extra blocks; for launch-list captures)")
     ap.add_argument("--profile-matvec", type=int, default=0, help="only run matvecs on an n^3 box (for ncu)")

@@ -261,3 +261,6 @@ def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == 16  # single candidate: no timing
     t2 = LaunchTuner(cache_path=path, timer=lambda *a: 1 / 0)
     assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM      # from the JSON cache
+    # within the margin of the default: the default stays
+    t3 = LaunchTuner(timer=lambda box, L_, dt, nb, f: 1.0 - 0.01 * (f == L.DDA_TUNE_P3PAIR))
+    assert t3.tune((128,) * 3, (256,) * 3, c64, 16) == 0
