@@ -342,6 +342,36 @@ def north_star_128(dev, seed=3):
             "seconds": {"mixed_batch": t_mix, "plain_one": t_one, "plain_batch": t_pb}}
 
 
+def batch64_block(args, ws, rank, local):
+    """The batching configuration (64 geometries x 16 right-hand sides)
+    measured inside the default run, summarised (single GPU only)."""
+    if ws != 1:
+        return None
+    a = argparse.Namespace(**vars(args))
+    a.geometries, a.warmup, a.steps = 64, 1, 1
+    ln = run_batch64(a, ws, rank, local, emit=False)
+    return {"workload": ln["config"]["workload"], "solves_per_s": ln["value"], "e2e_solves_per_s": ln["e2e"]["value"],
+            "converged": ln["converged"], "rhs": ln["config"]["global_batch"], "iterations": ln["iterations"],
+            "solve_seconds": ln["solve_seconds"]}
+
+
+def serve_block(args, ws, rank, local, rate=3.0, duration=20.0):
+    """The serving configuration's request mix at a rate one GPU sustains
+    (3 requests/s for 20 s), measured inside the default run: request and
+    right-hand-side p50/p99 latency and solves/s (single GPU only)."""
+    if ws != 1:
+        return None
+    a = argparse.Namespace(**vars(args))
+    a.rates, a.duration = str(rate), duration
+    ln = run_serve(a, ws, rank, local, emit=False)
+    c = ln["curve"][-1]
+    return {"workload": ln["config"]["workload"], "offered_requests_per_s": rate, "seconds": duration,
+            "rhs_per_s": c["rhs_per_s"], "requests_per_s": c["requests_per_s"],
+            "request_p50_ms": c["request_p50_ms"], "request_p99_ms": c["request_p99_ms"],
+            "rhs_p50_ms": c["rhs_p50_ms"], "rhs_p99_ms": c["rhs_p99_ms"], "converged": c["converged"],
+            "rhs": c["rhs"], "green_hits": c["green_hits"], "green_misses": c["green_misses"]}
+
+
 def config1_plain(dev):
     """The plain-method configuration on the GPU: 32^3 sphere (17,256
     dipoles, m = 1.5+0.01i, |m|kd = 0.5), complex128 GPBiCGSTAB from P0 = 0,
@@ -523,6 +553,7 @@ def run_ours(args, ws, rank, local):
             del opb
         del flush
         out = {"north_star_128": north_star_128(dev), "config1_plain_32": config1_plain(dev),
+               "batch64": batch64_block(args, ws, rank, local), "serve": serve_block(args, ws, rank, local),
                "launch_tuning": {json.dumps(list(k)): {"flags": v, "seconds": tuner.times.get(k)}
                                  for k, v in tuner.best.items()}}
         out.update({"roofline": roof, "matvec_128": big, "plain_c128_solves_per_s": plain,
@@ -699,7 +730,7 @@ def run_large128(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def run_batch64(args, ws, rank, local):
+def run_batch64(args, ws, rank, local, emit=True):
     """64 rotated ellipsoids with box edges 16-96, 2 polarisations x 8
     incidence directions each (1024 right-hand sides), mixed precision to
     1e-5, autotuned padding per size bucket, buckets as concurrent slot pools."""
@@ -784,7 +815,9 @@ def run_batch64(args, ws, rank, local):
                  iterations={"mean_inner": float(np.mean(its)), "max_inner": int(max(its)),
                              "mean_outer": float(np.mean([i.outer for i in infos]))},
                  clocks=clk.summary())
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def serve_stream(srv, stream, dev, tol=1e-5):
@@ -851,7 +884,7 @@ def serve_summary(groups, span):
             "converged": sum(r.info.status == "converged" for r in rhs)}, rhs
 
 
-def run_serve(args, ws, rank, local):
+def run_serve(args, ws, rank, local, emit=True):
     """Poisson request streams, 40% spheres, 40% ellipsoids, 20% random-walk
     aggregates, boxes 16^3-128^3, 1-16 incidences each, served by continuous
     batching with HBM admission and Green-tensor reuse.  One stream per
@@ -910,7 +943,9 @@ def run_serve(args, ws, rank, local):
                  green_cache={"hits": last["green_hits"], "misses": last["green_misses"]},
                  converged=last["converged"], gpu_launches=int(launches), clocks=clk.summary())
     srv.close()
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def main():

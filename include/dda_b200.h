@@ -169,6 +169,9 @@ int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz
  *   DDA_TUNE_ZPAIR         the z passes on packed pairs likewise
  *   DDA_TUNE_FUSED         the cluster-fused z/y passes where they are off
  *                          by default (128^3 boxes, launches of any width)
+ *   DDA_TUNE_PREFETCH      the x and y passes of cubic boxes prefetch the
+ *                          input rows of the tiles one resident wave ahead
+ *                          into L2 (bulk prefetches)
  * dda_tuning_set with flags < 0 removes the entry; dda_tuning_get returns
  * DDA_ERR_ARG when there is none.  Entries apply to launches made after
  * the call (a captured iteration graph keeps the variant it was captured
@@ -181,6 +184,7 @@ int dda_matvec_noalloc(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz
 #define DDA_TUNE_YPAIR 32
 #define DDA_TUNE_ZPAIR 64
 #define DDA_TUNE_FUSED 128
+#define DDA_TUNE_PREFETCH 256
 int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int flags);
 int dda_tuning_get(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, int nb, int* flags);
 

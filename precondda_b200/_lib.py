@@ -49,7 +49,7 @@ EXPORTS = (
 )
 
 DDA_TUNE_P3PIPE, DDA_TUNE_P3PIPE_1SM, DDA_TUNE_NO_FUSED_ZY, DDA_TUNE_NO_FUSED_INV, DDA_TUNE_P3PAIR = 1, 2, 4, 8, 16
-DDA_TUNE_YPAIR, DDA_TUNE_ZPAIR, DDA_TUNE_FUSED = 32, 64, 128
+DDA_TUNE_YPAIR, DDA_TUNE_ZPAIR, DDA_TUNE_FUSED, DDA_TUNE_PREFETCH = 32, 64, 128, 256
 
 
 class DDAError(RuntimeError):

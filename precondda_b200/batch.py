@@ -141,26 +141,28 @@ class PaddingTuner:
 # launch-variant autotuner
 # --------------------------------------------------------------------------
 def launch_candidates(box, L_, dtype, nb):
-    """DDA_TUNE_* flag sets worth timing for one bucket: the one-tile x
-    pass, the staged x pass on two or one CTA per SM, or the packed-pair x
-    pass, with the plain or packed-pair y and z passes (cubic complex64 boxes on
-    the (2n)^3 grid of 64^3 and 128^3, where those kernels are built),
-    each with and without the cluster-fused z/y passes (one-instance 64^3
-    complex64 launches, where they are the default, and any 128^3 complex64
-    launch, where they are not)."""
+    """DDA_TUNE_* flag sets worth timing for one bucket.  Cubic boxes on the
+    (2n)^3 grid of 64^3 and 128^3, where the variants are built: for
+    complex64 the one-tile, staged or packed-pair x pass, plain or
+    packed-pair y and z passes, with and without the L2 prefetch of the x
+    and y passes' input, and with and without the cluster-fused z/y passes
+    (one-instance 64^3 launches, where they are the default, and any 128^3
+    launch, where they are not); for complex128 the prefetch alone.  Other
+    buckets have the default only."""
     cube = box[0] == box[1] == box[2] and L_[0] == L_[1] == L_[2] == 2 * box[0]
-    x_opts = [0]
-    if cube and dtype == _C64 and L_[0] in (128, 256):
-        x_opts = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_P3PAIR]
-    y_opts = [0]
-    if cube and dtype == _C64 and L_[0] in (128, 256):
-        y_opts = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
+    if not (cube and L_[0] in (128, 256)):
+        return [0]
+    if dtype != _C64:
+        return [0, L.DDA_TUNE_PREFETCH]
+    x_opts = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PAIR]
+    y_opts = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
+    pf_opts = [0, L.DDA_TUNE_PREFETCH]
     zy_opts = [0]
-    if cube and dtype == _C64 and L_[0] == 128 and nb == 1:
+    if L_[0] == 128 and nb == 1:
         zy_opts = [0, L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV]
-    elif cube and dtype == _C64 and L_[0] == 256:
+    elif L_[0] == 256:
         zy_opts = [0, L.DDA_TUNE_FUSED]
-    return [a | y | b for a in x_opts for y in y_opts for b in zy_opts]
+    return [a | y | p | b for a in x_opts for y in y_opts for p in pf_opts for b in zy_opts]
 
 
 class LaunchTuner:

@@ -139,7 +139,7 @@ int dda_tuning_set(int dtype, int nx, int ny, int nz, int Lx, int Ly, int Lz, in
   if (dtype != DDA_C64 && dtype != DDA_C128) { set_error("bad dtype"); return DDA_ERR_ARG; }
   if (nb < 1) { set_error("nb must be >= 1"); return DDA_ERR_ARG; }
   if (flags > (DDA_TUNE_P3PIPE | DDA_TUNE_P3PIPE_1SM | DDA_TUNE_NO_FUSED_ZY | DDA_TUNE_NO_FUSED_INV |
-                DDA_TUNE_P3PAIR | DDA_TUNE_YPAIR | DDA_TUNE_ZPAIR | DDA_TUNE_FUSED)) {
+                DDA_TUNE_P3PAIR | DDA_TUNE_YPAIR | DDA_TUNE_ZPAIR | DDA_TUNE_FUSED | DDA_TUNE_PREFETCH)) {
     set_error("unknown tuning flags");
     return DDA_ERR_ARG;
   }

@@ -78,6 +78,9 @@ struct Geo {
   int Lx, Ly, Lz;
   int hx, hy, hz;     // octant extents L/2+1
   long long nsite;    // nx*ny*nz
+  // L2 prefetch distance, in CTAs, of the x pass and of the y passes (each
+  // CTA prefetches the input rows of the CTA that far ahead; 0 = none)
+  int pf3 = 0, pf2 = 0;
 };
 
 // Largest number of Stockham stages a length may need (L <= 4096).

@@ -16,8 +16,13 @@ namespace dda {
 void set_error(const std::string& msg);
 
 // Launch with programmatic stream serialization (the kernel must begin with
-// grid_dep_begin()); DDA_NO_PDL=1 launches plainly.
+// grid_dep_begin()); DDA_NO_PDL=1 launches plainly.  Streams registered
+// with set_stream_pdl(s, false) launch plainly too: slot pools run several
+// streams at once, and a kernel launched early holds SM resources while it
+// waits for its predecessor, which other streams' work could use.
 bool pdl_enabled();
+bool stream_pdl(cudaStream_t s);
+void set_stream_pdl(cudaStream_t s, bool on);
 template <typename... KArgs, typename... Args>
 cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args&&... args) {
   cudaLaunchConfig_t cfg = {};
@@ -29,7 +34,7 @@ cudaError_t launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, 
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[0].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  cfg.numAttrs = (pdl_enabled() && stream_pdl(s)) ? 1 : 0;
   return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 // Counts kernels this library enqueues (launches made while a stream is being

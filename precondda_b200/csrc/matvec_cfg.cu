@@ -17,6 +17,22 @@ bool pdl_enabled() {
   return on;
 }
 
+namespace {
+std::mutex g_pdl_mu;
+std::set<cudaStream_t> g_no_pdl;
+}  // namespace
+
+bool stream_pdl(cudaStream_t s) {
+  std::lock_guard<std::mutex> lk(g_pdl_mu);
+  return g_no_pdl.empty() || !g_no_pdl.count(s);
+}
+
+void set_stream_pdl(cudaStream_t s, bool on) {
+  std::lock_guard<std::mutex> lk(g_pdl_mu);
+  if (on) g_no_pdl.erase(s);
+  else g_no_pdl.insert(s);
+}
+
 bool fused_zy_enabled(bool inverse) {
   const char* e = getenv("DDA_NO_FUSED_ZY");
   if (e && *e == '1') return false;
@@ -25,6 +41,24 @@ bool fused_zy_enabled(bool inverse) {
     if (e && *e == '1') return false;
   }
   return true;
+}
+
+bool prefetch_forced() {
+  const char* e = getenv("DDA_PREFETCH");
+  return e && *e == '1';
+}
+
+int resident_ctas(const void* k, int threads, size_t smem) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, std::pair<int, size_t>>, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(k, std::make_pair(threads, smem));
+  auto it = cache.find(key);
+  if (it != cache.end()) return it->second;
+  int n = 0;
+  if (!k || cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, threads, smem) != cudaSuccess || n < 1) n = 1;
+  cache[key] = n;
+  return n;
 }
 
 bool z_pair_forced() {

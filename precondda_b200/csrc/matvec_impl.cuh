@@ -34,6 +34,14 @@ namespace cg = cooperative_groups;
 
 constexpr int kMvMaxThreads = 384;
 
+// L2 prefetch of the input rows of another tile: `rows` row segments of
+// `bytes` each, `stride` elements apart, issued by warp 0 as bulk prefetches.
+template <class C>
+__device__ __forceinline__ void prefetch_rows(const C* base, long long stride, int rows, int bytes) {
+  if (threadIdx.x >= 32) return;
+  for (int r = threadIdx.x; r < rows; r += 32) bulk_prefetch_l2(base + r * stride, (uint32_t)bytes);
+}
+
 // Twiddle tables in shared memory: the transform passes of a precision
 // with the switch on copy their table there at entry (after the pass's
 // exchange area) and read it from there instead of through the read-only
@@ -380,6 +388,14 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   C* col = t2 + ((long long)ky * Lz + kz0) * 3 + w;
   C* sw = s + w;
   const auto twk = pass_tw(tw, s + W * SH::LP, LX);
+  if constexpr (CUBE && (3 * TZC * (int)sizeof(C)) % 16 == 0 && TZC % 2 == 0) {
+    // the input rows of the tile g.pf3 CTAs ahead, into L2
+    const int f = (int)blockIdx.x + g.pf3;
+    if (g.pf3 > 0 && f < (int)gridDim.x) {
+      const int fp = f / NTZC, fk = f - fp * NTZC;
+      prefetch_rows(t2 + ((long long)pencil_ky(fp, Ly) * Lz + fk * TZC) * 3, rs, nx, 3 * TZC * (int)sizeof(C));
+    }
+  }
   auto ld = [&](int, int pos) -> C { return (ok && (ZH || pos < nx)) ? __ldcg(col + pos * rs) : czero<C>(); };
   auto sm = [&](int, int pp) -> C& { return sw[pp * W]; };
   C a[P::E];
@@ -1351,6 +1367,13 @@ bool y_pair_forced();
 bool z_pair_forced();
 // Streaming multiprocessors of the current device (cached per device).
 int device_sms();
+// CTAs of kernel k resident per SM at this block size and shared memory
+// (occupancy query, cached per kernel and shape).
+int resident_ctas(const void* k, int threads, size_t smem);
+// Whether the x / y passes prefetch the input rows of the tiles one
+// resident wave ahead into L2 (DDA_PREFETCH=1 forces it; otherwise
+// DDA_TUNE_PREFETCH in the tuning table).
+bool prefetch_forced();
 
 
 // Launch on clusters of `cl` CTAs along x, with programmatic stream
@@ -1371,7 +1394,7 @@ cudaError_t launch_cluster(void (*k)(KArgs...), int cl, dim3 grid, dim3 block, s
   at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   at[1].val.programmaticStreamSerializationAllowed = 1;
   cfg.attrs = at;
-  cfg.numAttrs = pdl_enabled() ? 2 : 1;
+  cfg.numAttrs = (pdl_enabled() && stream_pdl(s)) ? 2 : 1;
   return cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
 }
 
@@ -1399,6 +1422,11 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
   const bool ypair = k.k2x && (y_pair_forced() || (tf & DDA_TUNE_YPAIR));
   const bool zpair = k.k1x && (z_pair_forced() || (tf & DDA_TUNE_ZPAIR));
+  Geo gq = g;
+  if (prefetch_forced() || (tf & DDA_TUNE_PREFETCH)) {
+    gq.pf3 = resident_ctas((const void*)k.k3, pc.th3, pc.smem3) * device_sms();
+    gq.pf2 = resident_ctas((const void*)k.k2, pc.th2, pc.smem2) * device_sms();
+  }
   if (ff) {
     if ((e = launch_cluster(k.kf, k.cl, dim3((unsigned)k.gridf, nb), dim3(k.thf), k.smemf, s, g, twz, st, act,
                             in_id, cond)))
@@ -1416,7 +1444,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
       if ((e = launch_pdl(k.k2x, dim3((unsigned)k.grid2x, nb), dim3(k.th2x), k.smem2x, s, g, twy, st, act, cond,
                           pc.tz2, pc.ntz2)))
         return e;
-    } else if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond,
+    } else if ((e = launch_pdl(k.k2, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, gq, twy, st, act, cond,
                                pc.tz2, pc.ntz2))) {
       return e;
     }
@@ -1434,7 +1462,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
     if ((e = launch_pdl(k.k3p, dim3((unsigned)gx, nb), dim3(k.th3p), k.smem3p, s, g, twx, st, act, cond, pc.tz3,
                         pc.ntz3, (R)gscale, fz.tensor)))
       return e;
-  } else if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, g, twx, st, act, cond,
+  } else if ((e = launch_pdl(k.k3, dim3((unsigned)pc.grid3, nb), dim3(pc.th3), pc.smem3, s, gq, twx, st, act, cond,
                              pc.tz3, pc.ntz3, (R)gscale, fz.tensor))) {
     return e;
   }
@@ -1447,7 +1475,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
       if ((e = launch_pdl(k.k4x, dim3((unsigned)k.grid2x, nb), dim3(k.th2x), k.smem2x, s, g, twy, st, act, cond,
                           pc.tz2, pc.ntz2)))
         return e;
-    } else if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, g, twy, st, act, cond,
+    } else if ((e = launch_pdl(k.k4, dim3((unsigned)pc.grid2, nb), dim3(pc.th2), pc.smem2, s, gq, twy, st, act, cond,
                                pc.tz2, pc.ntz2))) {
       return e;
     }

@@ -14,6 +14,7 @@
 //              completed slots are reported and become free.
 // Pools on different streams overlap on the device.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -147,6 +148,14 @@ static int slots_create(dda_ctx* ctx, int precision, int nx, int ny, int nz, int
   }
   p->w.astream = p->s;
   p->w128.astream = p->s;
+  // pools run side by side on their own streams: their kernels launch
+  // without programmatic serialization (B200, the 64-geometry batched
+  // workload measured 86-84 solves/s with it, 117 without; DDA_POOL_PDL=1
+  // keeps it)
+  if (p->s) {
+    const char* pe = getenv("DDA_POOL_PDL");
+    if (!(pe && *pe == '1')) set_stream_pdl(p->s, false);
+  }
   if (!rc) rc = p->w.alloc(ctx->c, precision == DDA_PREC_C128 ? DDA_C128 : DDA_C64, g, nslots, true, gp);
   p->w.pscale = pscale;
   if (!rc && precision == DDA_PREC_MIXED) rc = p->w128.alloc(ctx->c, DDA_C128, g, nslots, false);
@@ -213,7 +222,10 @@ void dda_slots_destroy(dda_slots* p) {
   }
   pinned_put(p->h_norm, 2 * p->n * sizeof(double));
   if (p->ev) cudaEventDestroy(p->ev);
-  if (p->s) cudaStreamDestroy(p->s);
+  if (p->s) {
+    set_stream_pdl(p->s, true);
+    cudaStreamDestroy(p->s);
+  }
   cudaGetLastError();
   delete p;
 }

@@ -230,37 +230,38 @@ def test_result_files_match_reference(tmp_path):
 
 def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     """LaunchTuner's selection logic with a fake device timer: the candidate
-    set per bucket, the fastest flags chosen, cached (also in JSON) and not
-    timed twice."""
+    set per bucket, the fastest flags chosen (the default kept within the
+    margin), cached (also in JSON) and not timed twice."""
     import torch
     from precondda_b200 import _lib as L
     from precondda_b200.batch import LaunchTuner, launch_candidates
     c64, c128 = torch.complex64, torch.complex128
-    zy = L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV
-    xs = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PIPE_1SM, L.DDA_TUNE_P3PAIR]
-    ys = (0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR)
-    assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [x | y | z for x in xs for y in ys for z in (0, zy)]
-    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == [
-        x | y | z for x in xs for y in ys for z in (0, L.DDA_TUNE_FUSED)]
+    xs = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PAIR]
+    ys = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
+    ps = [0, L.DDA_TUNE_PREFETCH]
+    nofused = L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV
+    assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [
+        x | y | p | z for x in xs for y in ys for p in ps for z in (0, nofused)]
+    c128k = [x | y | p | z for x in xs for y in ys for p in ps for z in (0, L.DDA_TUNE_FUSED)]
+    assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == c128k
+    assert launch_candidates((64,) * 3, (128,) * 3, c64, 4) == [x | y | p for x in xs for y in ys for p in ps]
     assert launch_candidates((40, 30, 20), (80, 64, 40), c64, 4) == [0]
-    assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0]
+    assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0, L.DDA_TUNE_PREFETCH]
     calls = []
 
     def timer(box, L_, dtype, nb, flags):
         calls.append(flags)
-        base = flags & ~(L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR | L.DDA_TUNE_FUSED)
-        return {0: 3.0, L.DDA_TUNE_P3PIPE_1SM: 2.0, L.DDA_TUNE_P3PIPE: 2.5, L.DDA_TUNE_P3PAIR: 2.2}[base] + \
-            (0.1 if flags & L.DDA_TUNE_YPAIR else 0.0) + (0.05 if flags & L.DDA_TUNE_FUSED else 0.0)
+        return 3.0 - (0.5 if flags == L.DDA_TUNE_PREFETCH else 0.0) - (0.3 if flags == L.DDA_TUNE_P3PAIR else 0.0)
 
     path = str(tmp_path / "launch.json")
     t = LaunchTuner(cache_path=path, timer=timer)
-    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
-    assert sorted(calls) == sorted(x | y | z for x in xs for y in ys for z in (0, L.DDA_TUNE_FUSED))
-    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM
-    assert len(calls) == 16                      # cached
-    assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == 16  # single candidate: no timing
+    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH
+    assert sorted(calls) == sorted(c128k)
+    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH
+    assert len(calls) == len(c128k)                  # cached
+    assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == len(c128k)   # single candidate
     t2 = LaunchTuner(cache_path=path, timer=lambda *a: 1 / 0)
-    assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_P3PIPE_1SM      # from the JSON cache
+    assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH          # from the JSON cache
     # within the margin of the default: the default stays
     t3 = LaunchTuner(timer=lambda box, L_, dt, nb, f: 1.0 - 0.01 * (f == L.DDA_TUNE_P3PAIR))
     assert t3.tune((128,) * 3, (256,) * 3, c64, 16) == 0

@@ -178,6 +178,27 @@ def test_pair_x_pass_matches_one_tile_kernel(n, nb, monkeypatch):
             assert _rel(pa.cpu().numpy(), pb.cpu().numpy()) < 2e-6
 
 
+@pytest.mark.parametrize("dtype", [C64, C128])
+@pytest.mark.parametrize("n,nb", [(64, 2), (128, 1)])
+def test_prefetch_changes_no_result(n, nb, dtype, monkeypatch):
+    """The L2 prefetch of the x and y passes' input (DDA_PREFETCH=1) adds
+    prefetch instructions to the same kernels: results equal bit for bit."""
+    P = _pkg()
+    ops, xs = [], []
+    for j in range(nb):
+        k, d, alpha, x = _rand_problem((n,) * 3, seed=3 * n + j, fill=0.5)
+        ia, _, _, _ = O.prepare_interaction_matrices(alpha, k, d)
+        ops.append(P.DDAOperator(ia, k, d, dtype=dtype))
+        xs.append(torch.as_tensor(x, device="cuda").to(dtype))
+    mv = lambda: P.engine.matvec_batch(ops, xs) if nb > 1 else [ops[0].matvec(xs[0])]
+    monkeypatch.setenv("DDA_PREFETCH", "1")
+    a = mv()
+    monkeypatch.delenv("DDA_PREFETCH", raising=False)
+    b = mv()
+    for u, v in zip(a, b):
+        assert torch.equal(u, v)
+
+
 def test_matvec_dense_tiny():
     P = _pkg()
     k, d, alpha, x = _rand_problem((4, 4, 4), seed=3)
