@@ -144,19 +144,17 @@ def launch_candidates(box, L_, dtype, nb):
     """DDA_TUNE_* flag sets worth timing for one bucket.  Cubic boxes on the
     (2n)^3 grid of 64^3 and 128^3, where the variants are built: for
     complex64 the one-tile, staged or packed-pair x pass, plain or
-    packed-pair y and z passes, with and without the L2 prefetch of the x
-    and y passes' input, and with and without the cluster-fused z/y passes
-    (one-instance 64^3 launches, where they are the default, and any 128^3
-    launch, where they are not); for complex128 the prefetch alone.  Other
-    buckets have the default only."""
+    packed-pair y and z passes, and with and without the cluster-fused z/y
+    passes (one-instance 64^3 launches, where they are the default, and any
+    128^3 launch, where they are not).  Other buckets, and complex128, have
+    the default only.  (The L2 prefetch of DDA_TUNE_PREFETCH measured slower
+    at every size and precision and is not a candidate.)"""
     cube = box[0] == box[1] == box[2] and L_[0] == L_[1] == L_[2] == 2 * box[0]
-    if not (cube and L_[0] in (128, 256)):
+    if not (cube and L_[0] in (128, 256)) or dtype != _C64:
         return [0]
-    if dtype != _C64:
-        return [0, L.DDA_TUNE_PREFETCH]
     x_opts = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PAIR]
     y_opts = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
-    pf_opts = [0, L.DDA_TUNE_PREFETCH]
+    pf_opts = [0]
     zy_opts = [0]
     if L_[0] == 128 and nb == 1:
         zy_opts = [0, L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV]

@@ -1372,7 +1372,9 @@ int device_sms();
 int resident_ctas(const void* k, int threads, size_t smem);
 // Whether the x / y passes prefetch the input rows of the tiles one
 // resident wave ahead into L2 (DDA_PREFETCH=1 forces it; otherwise
-// DDA_TUNE_PREFETCH in the tuning table).
+// DDA_TUNE_PREFETCH in the tuning table).  B200: slower at every size
+// measured (128^3 c64 0.587 against 0.558 ms, c128 1.363 against 1.269;
+// 64^3 c64 0.083 against 0.078), so nothing selects it by default.
 bool prefetch_forced();
 
 

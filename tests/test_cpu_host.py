@@ -238,7 +238,7 @@ def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     c64, c128 = torch.complex64, torch.complex128
     xs = [0, L.DDA_TUNE_P3PIPE, L.DDA_TUNE_P3PAIR]
     ys = [0, L.DDA_TUNE_YPAIR | L.DDA_TUNE_ZPAIR]
-    ps = [0, L.DDA_TUNE_PREFETCH]
+    ps = [0]
     nofused = L.DDA_TUNE_NO_FUSED_ZY | L.DDA_TUNE_NO_FUSED_INV
     assert launch_candidates((64,) * 3, (128,) * 3, c64, 1) == [
         x | y | p | z for x in xs for y in ys for p in ps for z in (0, nofused)]
@@ -246,22 +246,24 @@ def test_launch_tuner_picks_fastest_candidate_and_caches(tmp_path):
     assert launch_candidates((128,) * 3, (256,) * 3, c64, 16) == c128k
     assert launch_candidates((64,) * 3, (128,) * 3, c64, 4) == [x | y | p for x in xs for y in ys for p in ps]
     assert launch_candidates((40, 30, 20), (80, 64, 40), c64, 4) == [0]
-    assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0, L.DDA_TUNE_PREFETCH]
+    assert launch_candidates((64,) * 3, (128,) * 3, c128, 1) == [0]
     calls = []
 
     def timer(box, L_, dtype, nb, flags):
         calls.append(flags)
-        return 3.0 - (0.5 if flags == L.DDA_TUNE_PREFETCH else 0.0) - (0.3 if flags == L.DDA_TUNE_P3PAIR else 0.0)
+        return 3.0 - (0.5 if flags == L.DDA_TUNE_P3PAIR | L.DDA_TUNE_FUSED else 0.0) - \
+            (0.3 if flags == L.DDA_TUNE_P3PAIR else 0.0)
 
     path = str(tmp_path / "launch.json")
     t = LaunchTuner(cache_path=path, timer=timer)
-    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH
+    best = L.DDA_TUNE_P3PAIR | L.DDA_TUNE_FUSED
+    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == best
     assert sorted(calls) == sorted(c128k)
-    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH
+    assert t.tune((128,) * 3, (256,) * 3, c64, 16) == best
     assert len(calls) == len(c128k)                  # cached
     assert t.tune((40, 30, 20), (80, 64, 40), c64, 4) == 0 and len(calls) == len(c128k)   # single candidate
     t2 = LaunchTuner(cache_path=path, timer=lambda *a: 1 / 0)
-    assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == L.DDA_TUNE_PREFETCH          # from the JSON cache
+    assert t2.tune((128,) * 3, (256,) * 3, c64, 16) == best                        # from the JSON cache
     # within the margin of the default: the default stays
     t3 = LaunchTuner(timer=lambda box, L_, dt, nb, f: 1.0 - 0.01 * (f == L.DDA_TUNE_P3PAIR))
     assert t3.tune((128,) * 3, (256,) * 3, c64, 16) == 0
