@@ -66,9 +66,20 @@ template <> struct PlanFor<40> { typedef RPlan<4, 2, 5> type; };
 template <> struct PlanFor<48> { typedef RPlan<4, 4, 3> type; };
 template <> struct PlanFor<64> { typedef RPlan<8, 8> type; };
 template <> struct PlanFor<72> { typedef RPlan<8, 3, 3> type; };
+// DDA_C64_PLAN8=1 (an A/B build option): the radix-8 plans for the
+// power-of-two lengths 128 and 256 too (E = 8: fewer registers per thread,
+// one more exchange)
+#if defined(DDA_C64_PLAN8) && DDA_C64_PLAN8
+template <> struct PlanFor<128> { typedef RPlan<8, 4, 4> type; };
+#else
 template <> struct PlanFor<128> { typedef RPlan<16, 8> type; };
+#endif
 template <> struct PlanFor<144> { typedef RPlan<4, 4, 3, 3> type; };
+#if defined(DDA_C64_PLAN8) && DDA_C64_PLAN8
+template <> struct PlanFor<256> { typedef RPlan<8, 8, 4> type; };
+#else
 template <> struct PlanFor<256> { typedef RPlan<16, 16> type; };
+#endif
 template <> struct PlanFor<512> { typedef RPlan<8, 8, 8> type; };
 template <> struct PlanFor<80> { typedef RPlan<4, 4, 5> type; };
 template <> struct PlanFor<160> { typedef RPlan<4, 4, 2, 5> type; };

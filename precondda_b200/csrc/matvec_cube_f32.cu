@@ -16,6 +16,16 @@ bool mv_cube_set<float>(int L, int p3var, MvSet<float>& o) {
     }
     return false;
   }
+  if (p3var == 2) {
+    // radix-8 plan, tensor product through shared memory (the complex128
+    // default), compiled for the power-of-two lengths
+    switch (L) {
+      case 64: mv_cube_fill<float, 64, 2>(o); return true;
+      case 128: mv_cube_fill<float, 128, 2>(o); return true;
+      case 256: mv_cube_fill<float, 256, 2>(o); return true;
+    }
+    return false;
+  }
   if (p3var != 0) return false;
   switch (L) {
 #define DDA_K(n) case n: mv_cube_fill<float, n, 0>(o); return true;

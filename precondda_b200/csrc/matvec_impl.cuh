@@ -1317,7 +1317,7 @@ void mv_cube_fill(MvSet<R>& o) {
     o.minb3p = MB;
     o.smem3p = PP::smem;
   }
-  if constexpr (sizeof(R) == 4 && (L == 128 || L == 256)) {
+  if constexpr (sizeof(R) == 4 && (L == 128 || (L == 256 && MvShape<R, L>::T <= 16))) {
     // complex64 64^3: both fused buffers fit two CTAs per SM; 128^3: one CTA
     // per SM in clusters of eight (T1, 151 MB and beyond L2, is neither
     // written nor read), for launches of any width, but only where the
