@@ -13,6 +13,7 @@ solves of all ranks over the slowest rank's time.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import math
 import os
@@ -349,6 +350,7 @@ def batch64_block(args, ws, rank, local):
         return None
     a = argparse.Namespace(**vars(args))
     a.geometries, a.warmup, a.steps = 64, 1, 1
+    gc.collect()
     ln = run_batch64(a, ws, rank, local, emit=False)
     return {"workload": ln["config"]["workload"], "solves_per_s": ln["value"], "e2e_solves_per_s": ln["e2e"]["value"],
             "converged": ln["converged"], "rhs": ln["config"]["global_batch"], "iterations": ln["iterations"],
@@ -363,6 +365,7 @@ def serve_block(args, ws, rank, local, rate=3.0, duration=20.0):
         return None
     a = argparse.Namespace(**vars(args))
     a.rates, a.duration = str(rate), duration
+    gc.collect()            # the earlier blocks' operators, before the server sizes its budget
     ln = run_serve(a, ws, rank, local, emit=False)
     c = ln["curve"][-1]
     return {"workload": ln["config"]["workload"], "offered_requests_per_s": rate, "seconds": duration,

@@ -272,6 +272,7 @@ class _Bucket:
     queue: deque = field(default_factory=deque)
     active: dict = field(default_factory=dict)    # slot -> Request
     outstanding: bool = False                     # a chunk of iterations is enqueued and not yet polled
+    nbytes: int = 0                               # HBM the pool holds, charged to the budget
 
 
 class DDAServer:
@@ -282,8 +283,11 @@ class DDAServer:
     precon=True solve, with the engine's circulant preconditioner of its
     padded lattice on the bucket's FFT grid (built when the request is
     admitted).  hbm_budget: bytes the pools may hold (default: 60% of the
-    free device memory at construction; the rest is left to Green builds,
-    the Green cache and the requests' arrays)."""
+    free device memory at construction, after torch's cached blocks are
+    released; the rest is left to Green builds, the Green cache and the
+    requests' arrays).  A new bucket whose pool does not fit what is left
+    closes idle buckets' pools, least recently used first; a request is
+    refused (MemoryError) only when not one slot fits after that."""
 
     def __init__(self, precision="mixed", buckets=DEFAULT_BUCKETS, slots_per_bucket=16, chunk_iters=8,
                  hbm_budget=None, green_budget=8 << 30, inner_tol=1e-4, max_outer=12, ratio=100.0, device=None,
@@ -297,6 +301,10 @@ class DDAServer:
         self.slots_per_bucket = int(slots_per_bucket)
         self.chunk = int(chunk_iters)
         if hbm_budget is None:
+            # the pools allocate outside torch's caching allocator: hand its
+            # cached blocks back first, or they count as used
+            torch.cuda.synchronize(self.device)
+            torch.cuda.empty_cache()
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = int(0.6 * free)      # the rest: Green builds and caches, request arrays
         self.hbm_budget = int(hbm_budget)
@@ -315,13 +323,32 @@ class DDAServer:
     def bucket_for(self, shape) -> int:
         return choose_bucket(shape, self.buckets)
 
+    def _evict_idle(self, need):
+        """Close the pools of idle buckets (nothing queued, running or
+        enqueued), least recently used first, until ``need`` bytes of the
+        budget are free or no idle bucket is left."""
+        for n in list(self._b):
+            if self.hbm_budget - self.hbm_used >= need:
+                return
+            b = self._b[n]
+            if b.queue or b.active or b.outstanding:
+                continue
+            b.pool.close()
+            self.hbm_used -= b.nbytes
+            del self._b[n]
+
     def _bucket(self, n) -> _Bucket:
         if n in self._b:
-            return self._b[n]
+            b = self._b.pop(n)       # most recently used last
+            self._b[n] = b
+            return b
         box = (n, n, n)
         L_ = fft_lengths(box, _C64 if self.precision == "c64" else _C128)
         pre = self.precondition
         per = slot_bytes(box, L_, self.precision, pre) + request_bytes(box, self.precision, L_ if pre else None)
+        want = pool_slots(box, L_, self.precision, self.hbm_budget, self.slots_per_bucket, pre)
+        if want >= 1 and self.hbm_budget - self.hbm_used < want * per:
+            self._evict_idle(want * per)
         room = self.hbm_budget - self.hbm_used
         ns = pool_slots(box, L_, self.precision, room, self.slots_per_bucket, pre)
         if ns < 1:
@@ -331,7 +358,7 @@ class DDAServer:
             self.launch_tuner.tune(box, L_, _C128 if self.precision == "c128" else _C64, ns)
         pool = SlotPool(box, L_, ns, self.precision, 1.0, self.device, precond_L=L_ if pre else None)
         self.hbm_used += ns * per
-        b = _Bucket(n, L_, pool)
+        b = _Bucket(n, L_, pool, nbytes=ns * per)
         self._b[n] = b
         return b
 
@@ -483,3 +510,4 @@ class DDAServer:
         for b in self._b.values():
             b.pool.close()
         self._b.clear()
+        self.hbm_used = 0

@@ -167,3 +167,30 @@ def test_server_budget_of_one_slot_queues_the_rest():
     assert all(r.info.status == "converged" for r in reqs)
     assert len({r.info.iters for r in reqs}) == 1
     srv.close()
+
+
+def test_server_evicts_idle_bucket_for_a_new_one():
+    """A budget that holds one bucket's pool: a request of another bucket
+    closes the idle pool (its memory returns) instead of being refused; a
+    bucket with work in flight is never closed."""
+    import precondda_b200 as P
+    from precondda_b200.serve import DDAServer, Request, slot_bytes, request_bytes
+    k, d, alpha, ia8, E8 = _sphere(8)
+    _, _, _, ia12, E12 = _sphere(12)
+    per12 = slot_bytes((12,) * 3, P.fft_lengths((12,) * 3), "c128") + request_bytes((12,) * 3, "c128")
+    srv = DDAServer(precision="c128", buckets=(8, 12), slots_per_bucket=1, hbm_budget=per12 + per12 // 4)
+    r8 = srv.submit(Request(ia8, E8, k, d, tol=1e-6, max_iter=200))
+    # bucket 8 holds a queued request: bucket 12 does not fit beside it
+    with pytest.raises(MemoryError):
+        srv.submit(Request(ia12, E12, k, d, tol=1e-6, max_iter=200))
+    srv.drain(timeout_s=120)
+    assert r8.info.status == "converged" and list(srv._b) == [8]
+    r12 = srv.submit(Request(ia12, E12, k, d, tol=1e-6, max_iter=200))
+    assert list(srv._b) == [12] and srv.hbm_used == srv._b[12].nbytes
+    srv.drain(timeout_s=120)
+    assert r12.info.status == "converged"
+    # the 12^3 result matches a solve of its own
+    alone = P.DDAOperator(ia12, k, d, dtype=C128).solve(E12, tol=1e-6, max_iter=200, ratio=100)
+    assert r12.info.iters == alone[1].iters
+    srv.close()
+    assert srv.hbm_used == 0
