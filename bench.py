@@ -343,6 +343,18 @@ def north_star_128(dev, seed=3):
             "seconds": {"mixed_batch": t_mix, "plain_one": t_one, "plain_batch": t_pb}}
 
 
+def _extra(fn, *a):
+    """One of the default line's extra workloads; a failure of one (an HBM
+    budget refusal, an out-of-memory error, a time limit) is reported in its
+    key and leaves the headline measurement standing."""
+    import traceback
+    try:
+        return fn(*a)
+    except (MemoryError, TimeoutError, ValueError, RuntimeError) as e:
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(e).__name__}: {e}"}
+
+
 def batch64_block(args, ws, rank, local):
     """The batching configuration (64 geometries x 16 right-hand sides)
     measured inside the default run, summarised (single GPU only)."""
@@ -369,6 +381,7 @@ def serve_block(args, ws, rank, local, rate=3.0, duration=20.0):
     ln = run_serve(a, ws, rank, local, emit=False)
     c = ln["curve"][-1]
     return {"workload": ln["config"]["workload"], "offered_requests_per_s": rate, "seconds": duration,
+            "hbm_budget_GiB": ln["config"]["hbm_budget_GiB"], "pools": ln["config"]["pools"],
             "rhs_per_s": c["rhs_per_s"], "requests_per_s": c["requests_per_s"],
             "request_p50_ms": c["request_p50_ms"], "request_p99_ms": c["request_p99_ms"],
             "rhs_p50_ms": c["rhs_p50_ms"], "rhs_p99_ms": c["rhs_p99_ms"], "converged": c["converged"],
@@ -555,8 +568,9 @@ def run_ours(args, ws, rank, local):
                          "algorithmic_bytes": Bb}
             del opb
         del flush
-        out = {"north_star_128": north_star_128(dev), "config1_plain_32": config1_plain(dev),
-               "batch64": batch64_block(args, ws, rank, local), "serve": serve_block(args, ws, rank, local),
+        out = {"north_star_128": _extra(north_star_128, dev), "config1_plain_32": _extra(config1_plain, dev),
+               "batch64": _extra(batch64_block, args, ws, rank, local),
+               "serve": _extra(serve_block, args, ws, rank, local),
                "launch_tuning": {json.dumps(list(k)): {"flags": v, "seconds": tuner.times.get(k)}
                                  for k, v in tuner.best.items()}}
         out.update({"roofline": roof, "matvec_128": big, "plain_c128_solves_per_s": plain,
@@ -937,6 +951,7 @@ def run_serve(args, ws, rank, local, emit=True):
                               f"boxes 16^3-128^3, m Re U[1.3,2] Im U[0,0.5], lambda U[0.4,0.8] um, 1-16 incidences, "
                               f"mixed precision to 1e-5, continuous batching",
                   "parallelism": "replicas" if ws > 1 else "single", "slots_per_bucket": args.slots,
+                  "hbm_budget_GiB": round(srv.hbm_budget / 2**30, 2),
                   "preconditioner": "none (precon=False)" if args.no_precondition else
                                     "precon=True: occupancy-weighted circulant per request group on its bucket's grid",
                   "pools": {str(k): v for k, v in st.get("pools", {}).items()}},

@@ -32,7 +32,7 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .engine import _C64, _C128, _device, fft_lengths, green_octant_pair, compiled_fft_lengths
+from .engine import _C64, _C128, _device, fft_lengths, green_octant_pair, compiled_fft_lengths, free_device_bytes
 from .engine import Preconditioner
 from .serve import SlotPool, precond_bytes, request_bytes, slot_bytes
 
@@ -301,10 +301,8 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
     groups = defaultdict(list)
     for gi, (box, L_) in enumerate(plan):
         groups[(box, L_)].append(gi)
-    torch.cuda.synchronize(dev)
-    torch.cuda.empty_cache()
+    free = free_device_bytes(dev)
     if hbm_budget is None:
-        free, _ = torch.cuda.mem_get_info(dev)
         hbm_budget = int(0.75 * free)
     # items: buckets, largest first, split so that each fits the budget
     items = deque()

@@ -54,6 +54,20 @@ def stream_handle(device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
 
 
+def free_device_bytes(device=None) -> int:
+    """Device memory that new pools and workspaces can have: torch's cached
+    blocks, the engine context's cached solver workspaces and the freed
+    blocks the engine keeps in the device's stream-ordered pool (the context
+    sets that pool's release threshold to keep them) are handed back first,
+    so none of them counts as used."""
+    dev = _device(device)
+    torch.cuda.synchronize(dev)
+    torch.cuda.empty_cache()
+    L.context(dev.index).trim()
+    free, _ = torch.cuda.mem_get_info(dev)
+    return int(free)
+
+
 _compiled_cache: dict[int, list] = {}
 
 

@@ -35,8 +35,8 @@ import numpy as np
 import torch
 
 from . import _lib as L
-from .engine import (SolveInfo, Preconditioner, _device, _info, as_device, fft_lengths, green_octant_pair,
-                     stream_handle, _C64, _C128)
+from .engine import (SolveInfo, Preconditioner, _device, _info, as_device, fft_lengths, free_device_bytes,
+                     green_octant_pair, stream_handle, _C64, _C128)
 
 PRECISIONS = {"c64": L.DDA_PREC_C64, "c128": L.DDA_PREC_C128, "mixed": L.DDA_PREC_MIXED}
 DEFAULT_BUCKETS = (8, 12, 16, 24, 32, 40, 48, 64, 80, 96, 128, 160, 192, 256)
@@ -301,12 +301,9 @@ class DDAServer:
         self.slots_per_bucket = int(slots_per_bucket)
         self.chunk = int(chunk_iters)
         if hbm_budget is None:
-            # the pools allocate outside torch's caching allocator: hand its
-            # cached blocks back first, or they count as used
-            torch.cuda.synchronize(self.device)
-            torch.cuda.empty_cache()
-            free, _ = torch.cuda.mem_get_info(self.device)
-            hbm_budget = int(0.6 * free)      # the rest: Green builds and caches, request arrays
+            # cached blocks (torch's, the engine's) are handed back first,
+            # or they would count as used
+            hbm_budget = int(0.6 * free_device_bytes(self.device))   # the rest: Green builds, caches, requests
         self.hbm_budget = int(hbm_budget)
         self.hbm_used = 0
         self.green = GreenCache(green_budget, self.device)
