@@ -27,6 +27,17 @@ __device__ __forceinline__ int opaque(int v) {
   asm volatile("mov.b32 %0, %1;" : "=r"(r) : "r"(v));
   return r;
 }
+// DDA_ASSUME_T=1: a kernel tells the compiler that its transform index t
+// is below the plan's thread count (the launch guarantees it), so
+// (t + 16 m) / 16 can fold into immediates of shared-memory addresses.
+#ifndef DDA_ASSUME_T
+#define DDA_ASSUME_T 1
+#endif
+template <int T> __device__ __forceinline__ void assume_t(int t) {
+#if DDA_ASSUME_T
+  __builtin_assume(t >= 0 && t < T);
+#endif
+}
 template <class T> __device__ __forceinline__ T* opaque_ptr(T* p) {
   T* r;
   asm volatile("mov.b64 %0, %1;" : "=l"(r) : "l"(p));

@@ -379,6 +379,7 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   const int nx = CUBE ? NC : g.nx;
   const int W = 3 * tz;
   const int w = threadIdx.x % W, t = threadIdx.x / W;
+  assume_t<SH::T>(t);                   // blockDim.x = W T (make_pass_cfg)
   const int p = blockIdx.x / ntz, kzt = blockIdx.x - p * ntz;
   const int ky = pencil_ky(p, Ly);
   const int kz0 = kzt * tz;
@@ -450,6 +451,7 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   // inverse half: fresh copies of the index and pointers keep the compiler
   // from carrying the forward half's address arithmetic across the kernel
   const int ti = opaque(t);
+  assume_t<SH::T>(ti);
   C* colo = opaque_ptr(col);
   C* swo = opaque_ptr(sw);
   auto smo = [&](int, int pp) -> C& { return swo[pp * W]; };
@@ -954,7 +956,93 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
 //   MV_CONV         y = conv                    (E_field_solver)
 //   MV_CONV_MASKED  y = mask*conv               (fft_matvec)
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
+// In the cubic complex64 kernels of power-of-two length (64^3 boxes and up)
+// the combine's operands are loaded
+// DDA_P5_EB outputs at a time, before those outputs' stores.  B200, 128^3
+// complex64 matvec: 0.560 ms one at a time, 0.538 ms by two, 0.544 by four,
+// 0.554 by eight (more registers, spills under the z passes' cap).
+// Complex128 by two took 1.283 against 1.271 ms (the 256-point pass went
+// from 80 to 102 registers), so the other kernels load at each output.
 // ---------------------------------------------------------------------------
+#ifndef DDA_P5_EB
+#define DDA_P5_EB 2
+#endif
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+// ia x - v with a fixed rounding (explicit fused multiply-adds), so every
+// kernel that forms the combine gives the same bits
+template <class C> __device__ __forceinline__ C combine_ax(C ia, C x, C v) {
+  C r;
+  r.x = fma_rn(ia.x, x.x, fma_rn(-ia.y, x.y, -v.x));
+  r.y = fma_rn(ia.x, x.y, fma_rn(ia.y, x.x, -v.y));
+  return r;
+}
+
+// The combine of pass 5 on one thread's inverse-z outputs: a[] holds the
+// last stage of plan P (swapped: the inverse runs as swap(FFT(swap(.)))),
+// thread ti; outputs at positions >= nz (or all beyond L/2 with DH) and
+// empty sites of occupied-site vectors are not stored.  The operands of a
+// batch of EB outputs (inv_alpha, x) are loaded before the batch's first
+// store: a cache-hinted store is a compiler memory barrier and the hinted
+// loads keep their order, so loads written between the stores would each
+// wait for the store before them, one memory latency per output.
+// post(e, r) runs after the store of element e (fused dot products).
+template <class P, bool DH, int EB0, typename R, class C, class POST>
+__device__ __forceinline__ void mv_combine_out(const C* a, int ti, bool ok, int nz, long long site0, int c,
+                                               const int* __restrict__ cid, const C* __restrict__ iag,
+                                               const C* __restrict__ xg, const C* __restrict__ bg,
+                                               C* __restrict__ yg, int mode, const POST& post) {
+  constexpr int RL = P::r[P::S - 1];
+  constexpr int NQ = DH ? RL / 2 : RL;
+  constexpr int NB = P::E / RL;
+  constexpr int K = NQ * NB;
+  constexpr int EB = K < EB0 ? K : EB0;
+  const bool need_ia = mode != MV_CONV;
+  const bool need_x = mode == MV_AX || mode == MV_RESIDUAL;
+#pragma unroll
+  for (int k0 = 0; k0 < K; k0 += EB) {
+    int ee[EB];             // element index in the instance's vectors (< 2^31: n^3 <= 512^3)
+    C iav[EB], xv[EB];
+#pragma unroll
+    for (int j = 0; j < EB; ++j) {
+      const int q = (k0 + j) / NB, b = (k0 + j) % NB;
+      const int pos = rout_pos<P, P::S - 1>(ti, b, q);
+      int e = -1;
+      if (k0 + j < K && ok && (DH || pos < nz)) {
+        e = (int)((site0 + pos) * 3 + c);
+        if (cid) {
+          const int kk = cid[pos];
+          e = kk < 0 ? -1 : 3 * kk + c;
+        }
+      }
+      ee[j] = e;
+      iav[j] = (need_ia && e >= 0) ? __ldg(iag + pos) : czero<C>();   // shared by the 3 component lanes
+      xv[j] = (need_x && e >= 0) ? __ldcg(xg + e) : czero<C>();
+    }
+#pragma unroll
+    for (int j = 0; j < EB; ++j) {
+      const int q = (k0 + j) / NB, b = (k0 + j) % NB;
+      const int e = ee[j];
+      if (e < 0) continue;
+      C v = cswap(a[b * RL + q]);
+      C r;
+      if (mode == MV_CONV) {
+        r = v;
+      } else {
+        const C ia = iav[j];
+        if (ia.x == (R)0 && ia.y == (R)0) v = czero<C>();
+        if (mode == MV_CONV_MASKED) {
+          r = v;
+        } else {
+          r = combine_ax(ia, xv[j], v);
+          if (mode == MV_RESIDUAL) r = csub(__ldcg(bg + e), r);
+        }
+      }
+      __stcg(yg + e, r);
+      post(e, r);
+    }
+  }
+}
 template <typename R, int LZ, int NC>
 __global__ void __launch_bounds__(kMvMaxThreads)
     k_mv_pass5(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int in_id,
@@ -1129,31 +1217,12 @@ __global__ void __launch_bounds__(FusedZY<R, L>::TH, FusedZY<R, L>::MINB) k_mv_i
     C* sl = xs + l * 3 * LP + c;
     auto sm = [&](int, int pp) -> C& { return sl[pp * 3]; };
     // the combine of pass 5 (y = ia x - mask conv and its variants)
-    auto stf = [&](int, int pos, C v) {
-      long long e = (site0 + pos) * 3 + c;
-      if (cid) {
-        const int k = cid[pos];
-        if (k < 0) return;
-        e = 3LL * k + c;
-      }
-      C o;
-      if (mode == MV_CONV) {
-        o = v;
-      } else {
-        const C a_ = __ldg(iag + pos);
-        const bool msk = (a_.x != (R)0) || (a_.y != (R)0);
-        if (!msk) v = czero<C>();
-        if (mode == MV_CONV_MASKED) {
-          o = v;
-        } else {
-          o = csub(cmul(a_, __ldcg(xg + e)), v);
-          if (mode == MV_RESIDUAL) o = csub(__ldcg(bg + e), o);
-        }
-      }
-      __stcg(yg + e, o);
-    };
     C a[P::E];
-    rfft<P, 1, true, false, true>(a, t, ld, sm, stf, tw);
+    rload<P, 1, false>(a, t, [&](int, int pos) -> C { return cswap(ld(0, pos)); });
+    rstage<P, 0, false>(a, t, tw);
+    rrest<P, 1, 0>(a, t, sm, tw);
+    mv_combine_out<P, true, DDA_P5_EB, R>(a, opaque(t), true, NC, site0, c, cid, iag, xg, bg, yg, mode,
+                                          [](int, C) {});
   }
 }
 
