@@ -638,15 +638,16 @@ def run_profile_matvec(args, local):
     ia = np.where(occ, 1.0 / (0.01 + 0.001j), 0).astype(np.complex128)
     op = P.DDAOperator(ia, k, d, dtype=dt, device=dev)
     x = torch.randn(n, n, n, 3, dtype=dt, device=dev)
+    nr = max(1, args.profile_rhs)
     for _ in range(args.reps):
-        y = op.matvec(x)
+        y = op.matvec(x) if nr == 1 else P.engine.matvec_batch([op] * nr, [x] * nr)[0]
     torch.cuda.synchronize()
-    out = {"profile_matvec": n, "dtype": args.dtype, "reps": args.reps, "L": op.L,
+    out = {"profile_matvec": n, "dtype": args.dtype, "reps": args.reps, "L": op.L, "rhs": nr,
            "p3_variant": os.environ.get("DDA_P3_VARIANT", "default"), "checksum": float(y.abs().sum())}
     if args.time:
         flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
-        t = time_matvec(op, 20, flush)
-        B = matvec_bytes(op.shape, 8 if dt == torch.complex64 else 16)
+        t = time_matvec(op, 20, flush) if nr == 1 else time_matvec_batch([op] * nr, 20, flush)
+        B = nr * matvec_bytes(op.shape, 8 if dt == torch.complex64 else 16)
         peak, _ = measured_peak()
         out.update({"ms": t * 1e3, "GBps": B / t / 1e9, "frac": B / t / 1e9 / peak})
     print(json.dumps(out))
@@ -979,6 +980,8 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="default workload: only the timed solves and e2e (no extra blocks; for launch-list captures)")
     ap.add_argument("--profile-matvec", type=int, default=0, help="only run matvecs on an n^3 box (for ncu)")
+    ap.add_argument("--profile-rhs", type=int, default=1,
+                    help="with --profile-matvec: right-hand sides per launch (gridDim.y)")
     ap.add_argument("--dtype", default="c64", choices=["c64", "c128"])
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--time", action="store_true", help="with --profile-matvec: time 20 launches (L2 flushed)")

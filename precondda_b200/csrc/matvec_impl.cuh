@@ -161,12 +161,13 @@ template <int NC> constexpr bool mixed_radix_mid() { return NC >= 20 && NC <= 96
 #ifndef DDA_GEN_P3_MINB
 #define DDA_GEN_P3_MINB 2
 #endif
-// Complex128 z passes of power-of-two cubic lengths >= 128: plain.  At 56
-// registers (three CTAs per SM) the 128^3 matvec took 1.403 against 1.428 ms
-// and the one-RHS 64^3 one 0.1556 against 0.1536 ms, within noise; the x
-// pass dominates.  DDA_ZD_REGS sets a cap.
+// Complex128 z passes of power-of-two cubic lengths >= 128: at most 80
+// registers (two CTAs of 384 threads per SM), the cap under which pass 5
+// holds its batched combine operands (uncapped: 102).  At 56 registers
+// (three CTAs) the 128^3 matvec took 1.403 against 1.428 ms plain, within
+// noise.  DDA_ZD_REGS=0 leaves them uncapped.
 #ifndef DDA_ZD_REGS
-#define DDA_ZD_REGS 0
+#define DDA_ZD_REGS 80
 #endif
 // Register cap of a z pass (0 = the plain kernel).
 template <typename R, int NC, int CAP>
@@ -956,13 +957,14 @@ __global__ void __launch_bounds__(PZPair<LZ>::TH, MINB)
 //   MV_CONV         y = conv                    (E_field_solver)
 //   MV_CONV_MASKED  y = mask*conv               (fft_matvec)
 // mask = (inv_alpha != 0), the reference's alpha != 0 (ddaforgit.py:1108).
-// In the cubic complex64 kernels of power-of-two length (64^3 boxes and up)
-// the combine's operands are loaded
-// DDA_P5_EB outputs at a time, before those outputs' stores.  B200, 128^3
-// complex64 matvec: 0.560 ms one at a time, 0.538 ms by two, 0.544 by four,
-// 0.554 by eight (more registers, spills under the z passes' cap).
-// Complex128 by two took 1.283 against 1.271 ms (the 256-point pass went
-// from 80 to 102 registers), so the other kernels load at each output.
+// In the cubic kernels of power-of-two length (64^3 boxes and up) the
+// combine's operands are loaded DDA_P5_EB outputs at a time, before those
+// outputs' stores.  B200, 128^3 complex64 matvec: 0.560 ms one at a time,
+// 0.538 ms by two, 0.544 by four, 0.554 by eight (more registers, spills
+// under the z passes' cap).  Complex128 by two under an 80-register cap:
+// 128^3 1.259 -> 1.225 ms, 64^3 0.1485 -> 0.1444 ms (uncapped it took 102
+// registers and was slower, 1.283 ms).  The other kernels load at each
+// output (batched, they take 10-30 more registers).
 // ---------------------------------------------------------------------------
 #ifndef DDA_P5_EB
 #define DDA_P5_EB 2
