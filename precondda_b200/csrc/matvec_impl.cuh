@@ -319,10 +319,11 @@ __global__ void __launch_bounds__(kMvMaxThreads) k_mv_pass3r(Geo g, const typena
 // variant with one component per thread and the tensor product through
 // shared memory: thread = (w fastest, t)
 // Cubic complex64 kernels of power-of-two length (E <= 16 per thread): three
-// CTAs of 384 threads per SM (56 registers), except L = 128 (64^3 boxes),
-// where two CTAs without spills measured faster (B200, two-RHS 64^3 matvec
-// 0.1362 -> 0.1321 ms; at L = 256 two CTAs were slower).  DDA_P3_MINB
-// overrides all lengths.
+// CTAs of 384 threads per SM (56 registers).  L = 128 (64^3 boxes) ran at
+// two CTAs while its 56-register build spilled; with the transform-index
+// range known to the compiler it no longer does, and three CTAs measured
+// faster (B200, two-RHS 64^3 matvec 0.1270 -> 0.1208 ms, one RHS 0.0728 ->
+// 0.0706 ms).  DDA_P3_MINB overrides all lengths.
 // Complex128 cubic x passes of power-of-two length: at most 85 registers (two
 // 384-thread CTAs; the 192-thread launches then fit four per SM).  ptxas
 // settles at 80 without spills, against 100-108 uncapped: 64^3 two-RHS
@@ -347,7 +348,7 @@ constexpr int p3_min_blocks() {
 #ifdef DDA_P3_MINB
   return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? DDA_P3_MINB : 1;
 #else
-  return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? (LX == 128 ? 2 : 3) : 1;
+  return (NC > 0 && sizeof(R) == 4 && LX >= 64 && (LX & (LX - 1)) == 0) ? 3 : 1;
 #endif
 }
 template <typename R, int LX, int V, int NC>
