@@ -177,8 +177,19 @@ constexpr int z_regs() {
   if (mixed_radix_mid<NC>()) return DDA_ZMR_REGS;
   return NC == 0 ? DDA_GEN_REGS : 0;
 }
+// Cubic complex64 y passes of power-of-two length: DDA_Y_REGS caps the
+// forward (zero-half) pass, DDA_YI_REGS the inverse (0: plain kernels).
+#ifndef DDA_Y_REGS
+#define DDA_Y_REGS 0
+#endif
+#ifndef DDA_YI_REGS
+#define DDA_YI_REGS 0
+#endif
 // Register cap of a y pass (0 = the plain kernel).
-template <typename R, int NC> constexpr int y_regs() { return (sizeof(R) == 4 && NC == 0) ? DDA_GEN_Y_REGS : 0; }
+template <typename R, int NC, bool INV = false> constexpr int y_regs() {
+  if (sizeof(R) == 4 && NC >= 64 && ((2 * NC) & (2 * NC - 1)) == 0) return INV ? DDA_YI_REGS : DDA_Y_REGS;
+  return (sizeof(R) == 4 && NC == 0) ? DDA_GEN_Y_REGS : 0;
+}
 
 // ---------------------------------------------------------------------------
 // pass 1: forward z on nl lines x 3 components; input zero beyond nz
@@ -206,7 +217,7 @@ __global__ void __launch_bounds__(kMvMaxThreads)
                 int tz_, int ntz_)
 #include "mv_pass_y.inc"
 template <typename R, bool INV, int LY, int NC>
-__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((y_regs<R, NC>()))
+__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((y_regs<R, NC, INV>()))
     k_mv_pass_y_cap(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int cond,
                     int tz_, int ntz_)
 #include "mv_pass_y.inc"
@@ -1294,7 +1305,7 @@ auto pick_pass5() {
 }
 template <typename R, bool INV, int L, int NC>
 auto pick_pass_y() {
-  if constexpr (y_regs<R, NC>() > 0) return k_mv_pass_y_cap<R, INV, L, NC>;
+  if constexpr (y_regs<R, NC, INV>() > 0) return k_mv_pass_y_cap<R, INV, L, NC>;
   else return k_mv_pass_y<R, INV, L, NC>;
 }
 
