@@ -91,10 +91,29 @@ int dda_ctx_create(int device, dda_ctx** out) {
       (e = cudaMalloc((void**)&c->c.xcnt, sizeof(unsigned))) != cudaSuccess ||
       (e = cudaMalloc((void**)&c->c.xout, 4 * sizeof(double))) != cudaSuccess ||
       (e = cudaMallocHost((void**)&c->c.xout_h, 4 * sizeof(double))) != cudaSuccess ||
-      (e = cudaMemset(c->c.xcnt, 0, sizeof(unsigned))) != cudaSuccess) {
+      (e = cudaMemset(c->c.xcnt, 0, sizeof(unsigned))) != cudaSuccess ||
+      (e = cudaEventCreateWithFlags(&c->c.ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+      (e = cudaMalloc((void**)&c->c.iota, Ctx::kIota * sizeof(int))) != cudaSuccess) {
     set_error(cudaGetErrorString(e));
     delete c;
     return DDA_ERR_CUDA;
+  }
+  for (int j = 0; j < Ctx::kMaxSplit - 1; ++j) {
+    if ((e = cudaStreamCreateWithFlags(&c->c.aux[j], cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->c.ev_join[j], cudaEventDisableTiming)) != cudaSuccess) {
+      set_error(cudaGetErrorString(e));
+      delete c;
+      return DDA_ERR_CUDA;
+    }
+  }
+  {
+    std::vector<int> h(Ctx::kIota);
+    for (int j = 0; j < Ctx::kIota; ++j) h[j] = j;
+    if ((e = cudaMemcpy(c->c.iota, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
+      set_error(cudaGetErrorString(e));
+      delete c;
+      return DDA_ERR_CUDA;
+    }
   }
   // transient buffers (Green-build transforms, voxeliser shape lists) come
   // from the device's stream-ordered pool; keep freed blocks in the pool
@@ -118,6 +137,12 @@ void dda_ctx_destroy(dda_ctx* ctx) {
   cudaEventDestroy(ctx->c.ev[0]); cudaEventDestroy(ctx->c.ev[1]);
   cudaEventDestroy(ctx->c.ev_user); cudaEventDestroy(ctx->c.ev_done);
   cudaStreamDestroy(ctx->c.stream);
+  for (int j = 0; j < Ctx::kMaxSplit - 1; ++j) {
+    if (ctx->c.aux[j]) { cudaStreamSynchronize(ctx->c.aux[j]); cudaStreamDestroy(ctx->c.aux[j]); }
+    if (ctx->c.ev_join[j]) cudaEventDestroy(ctx->c.ev_join[j]);
+  }
+  if (ctx->c.ev_fork) cudaEventDestroy(ctx->c.ev_fork);
+  cudaFree(ctx->c.iota);
   cudaFree(ctx->c.xred); cudaFree(ctx->c.xcnt); cudaFree(ctx->c.xout); cudaFreeHost(ctx->c.xout_h);
   delete ctx;
 }

@@ -21,6 +21,9 @@ void set_error(const std::string& msg);
 // streams at once, and a kernel launched early holds SM resources while it
 // waits for its predecessor, which other streams' work could use.
 bool pdl_enabled();
+// Branches a batched matvec launch sequence of nb instances is split into
+// (DDA_MV_SPLIT; 1 = one launch sequence over all instances).
+int mv_split_ways(int nb);
 bool stream_pdl(cudaStream_t s);
 void set_stream_pdl(cudaStream_t s, bool on);
 template <typename... KArgs, typename... Args>
@@ -80,6 +83,17 @@ struct Ctx {
   double* xout = nullptr;      // [4] device
   double* xout_h = nullptr;    // [4] pinned
   int xrb = 1;
+  // Concurrent branches of one batched launch sequence (mv_split): auxiliary
+  // streams, fork / join events and instance indices 0..kIota-1 for launches
+  // without an active list.  Made at context creation, so a fork needs no
+  // allocation (it may be recorded into a graph).
+  static constexpr int kMaxSplit = 4;
+  static constexpr int kIota = 4096;
+  cudaStream_t aux[kMaxSplit - 1] = {};
+  cudaEvent_t ev_fork = nullptr;
+  cudaEvent_t ev_join[kMaxSplit - 1] = {};
+  int* iota = nullptr;
+  std::mutex fork_mu;
   // returns device twiddles for length L (builds on first use)
   const void* twiddles(int L, bool dbl);
   // cached solver workspace for (dtype, geometry, batch size)

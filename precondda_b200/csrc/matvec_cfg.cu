@@ -17,6 +17,15 @@ bool pdl_enabled() {
   return on;
 }
 
+int mv_split_ways(int nb) {
+  static const int k = [] {
+    const char* e = getenv("DDA_MV_SPLIT");
+    const int v = e ? atoi(e) : 1;
+    return v < 1 ? 1 : (v > Ctx::kMaxSplit ? Ctx::kMaxSplit : v);
+  }();
+  return nb < k ? nb : k;
+}
+
 namespace {
 std::mutex g_pdl_mu;
 std::set<cudaStream_t> g_no_pdl;

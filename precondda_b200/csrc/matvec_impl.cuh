@@ -1589,7 +1589,32 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
   const C* twy = (const C*)ctx.twiddles(g.Ly, dbl);
   const C* twz = (const C*)ctx.twiddles(g.Lz, dbl);
   if (!twx || !twy || !twz) return cudaErrorMemoryAllocation;
-  return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, out_id, mode, cond, gscale, s, fz);
+  const int K = mv_split_ways(nb);
+  if (K <= 1 || (!act && nb > Ctx::kIota))
+    return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, out_id, mode, cond, gscale, s, fz);
+  // K concurrent branches, each a launch sequence over nb/K instances: the
+  // first on s, the others on the context's auxiliary streams, forked from
+  // and joined back into s by events (graph branches under capture), so one
+  // branch's passes fill the SMs another's wave tails leave idle
+  std::lock_guard<std::mutex> lk(ctx.fork_mu);
+  cudaError_t e = cudaEventRecord(ctx.ev_fork, s);
+  if (e != cudaSuccess) return e;
+  for (int j = 1; j < K; ++j)
+    if ((e = cudaStreamWaitEvent(ctx.aux[j - 1], ctx.ev_fork, 0)) != cudaSuccess) return e;
+  cudaError_t first = cudaSuccess;
+  for (int j = 0; j < K; ++j) {
+    const int o = j * nb / K, n = (j + 1) * nb / K - o;
+    const int* a = (act ? act : ctx.iota) + o;
+    e = launch_mv_set<R>(k, g, pc, st, a, n, twx, twy, twz, in_id, out_id, mode, cond, gscale,
+                         j ? ctx.aux[j - 1] : s, fz);
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  }
+  for (int j = 1; j < K; ++j) {
+    if ((e = cudaEventRecord(ctx.ev_join[j - 1], ctx.aux[j - 1])) == cudaSuccess)
+      e = cudaStreamWaitEvent(s, ctx.ev_join[j - 1], 0);
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  }
+  return first;
 }
 
 // Same five launches with caller-provided twiddle tables (used by the
