@@ -40,11 +40,11 @@ TOL, INNER_TOL, MAX_ITER, RATIO = 1e-6, 1e-4, 2000, 100.0
 # CPU per-iteration time to a whole solve for the CPU arms (oracle run: 123
 # iterations, relative residual 7.0e-7).
 REF_ITERS_64 = 123
-# DRAM bytes (read + write) of one complex64 64^3 matvec (five passes), from
-# an ncu capture of the same launch; the passes' intermediates stay in L2, so
-# this is below the algorithmic bytes.  The bench's two-RHS launch moves twice
-# this (each RHS has its own T1/T2).
-MATVEC64_C64_DRAM_BYTES = 103.9e6
+# DRAM bytes (read + write) of the complex64 64^3 two-RHS matvec (five
+# passes, both right-hand sides in one launch), from an ncu capture of that
+# launch (bench.py --profile-matvec 64 --profile-rhs 2); the passes'
+# intermediates stay in L2, so this is below the algorithmic bytes.
+MATVEC64_C64_RHS2_DRAM_BYTES = 181.9e6
 
 
 def problem(n=N_BOX, m=M_REF):
@@ -552,7 +552,7 @@ def run_ours(args, ws, rank, local):
         B = matvec_bytes(op.shape, 8)
         ach = 2 * B / t_mv / 1e9
         roof = {"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "traffic": 2 * MATVEC64_C64_DRAM_BYTES, "traffic_from": "ncu capture of this launch (profile)",
+                "traffic": MATVEC64_C64_RHS2_DRAM_BYTES, "traffic_from": "ncu capture of this launch (profile)",
                 "kernel": "5-pass matvec, complex64, 64^3 box (FFT 128^3), both right-hand sides in one launch",
                 "algorithmic_bytes": 2 * B, "ms": t_mv * 1e3, "peak_kind": peak_kind,
                 "single_rhs": {"ms": t_mv1 * 1e3, "GBps": B / t_mv1 / 1e9, "frac": B / t_mv1 / 1e9 / peak}}
