@@ -303,6 +303,11 @@ int dda_slots_admit_pre(dda_slots* pool, int slot, const dda_instance* lo, const
                         double tol, double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
 /* Enqueue `niter` GPBiCGSTAB iterations of every occupied slot. */
 int dda_slots_run(dda_slots* pool, int niter);
+/* 1 when the pool's stream has finished all enqueued work (dda_slots_poll
+ * would not wait), 0 while it is busy, a negative DDA_ERR_* code on error.
+ * A host loop over several pools polls the ready ones first, so a pool
+ * whose chunk ended is refilled while the others still run. */
+int dda_slots_ready(const dda_slots* pool);
 /* Wait for the pool's stream, then report the slots that finished since the
  * last poll (finished[0..*nfinished), results in the same order; arrays of
  * capacity length) and free them.  Mixed pools refine here: a finished

@@ -42,7 +42,8 @@ EXPORTS = (
     "dda_fft_length_ok", "dda_green_build", "dda_ghat_to_engine", "dda_op_create", "dda_op_destroy", "dda_matvec",
     "dda_matvec_noalloc", "dda_gpbicgstab", "dda_solve_batch", "dda_solve_mixed_batch", "dda_cross_sections",
     "dda_voxelize", "dda_incident_field", "dda_slots_create", "dda_slots_destroy", "dda_slots_capacity",
-    "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_poll", "dda_slots_release",
+    "dda_slots_free_slot", "dda_slots_admit", "dda_slots_run", "dda_slots_ready", "dda_slots_poll",
+    "dda_slots_release",
     "dda_far_field", "dda_matvec_batch", "dda_precond_build", "dda_precond_op_create", "dda_gpbicgstab_pre",
     "dda_solve_batch_pre", "dda_solve_mixed_batch_pre", "dda_slots_create_pre", "dda_slots_admit_pre",
     "dda_tuning_set", "dda_tuning_get",
@@ -117,6 +118,7 @@ def _declare(lib):
     lib.dda_slots_free_slot.argtypes = [vp]
     lib.dda_slots_admit.argtypes = [vp, i, C.POINTER(dda_instance), C.POINTER(dda_instance), d, d, i, i, d, vp]
     lib.dda_slots_run.argtypes = [vp, i]
+    lib.dda_slots_ready.argtypes = [vp]
     lib.dda_slots_poll.argtypes = [vp, C.POINTER(i), C.POINTER(dda_result), C.POINTER(i), C.POINTER(i)]
     lib.dda_slots_release.argtypes = [vp, i]
     lib.dda_slots_create_pre.argtypes = [vp, i, i, i, i, i, i, i, d, i, i, i, d, i, C.POINTER(vp)]

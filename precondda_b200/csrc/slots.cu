@@ -333,6 +333,16 @@ int dda_slots_run(dda_slots* p, int niter) {
   return DDA_OK;
 }
 
+int dda_slots_ready(const dda_slots* p) {
+  if (!p) { set_error("null pool"); return -DDA_ERR_ARG; }
+  cudaSetDevice(p->ctx->c.device);
+  const cudaError_t e = cudaStreamQuery(p->s);
+  if (e == cudaSuccess) return 1;
+  if (e == cudaErrorNotReady) { cudaGetLastError(); return 0; }
+  set_error(cudaGetErrorString(e));
+  return -DDA_ERR_CUDA;
+}
+
 int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinished, int* nrunning) {
   if (!p || !finished || !nfinished) { set_error("bad arguments"); return DDA_ERR_ARG; }
   cudaSetDevice(p->ctx->c.device);

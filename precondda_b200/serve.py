@@ -184,6 +184,15 @@ class SlotPool:
         with torch.cuda.device(self.device):
             L.check(L.lib().dda_slots_run(self._h, int(niter)))
 
+    def ready(self) -> bool:
+        """Whether the pool's enqueued iterations have all finished (a poll
+        would not wait)."""
+        with torch.cuda.device(self.device):
+            r = L.lib().dda_slots_ready(self._h)
+        if r < 0:
+            L.check(-r)
+        return r == 1
+
     def poll(self):
         """[(slot, SolveInfo, P)] of the slots that finished; they become free."""
         nf, nr = C.c_int(0), C.c_int(0)
@@ -273,6 +282,7 @@ class _Bucket:
     active: dict = field(default_factory=dict)    # slot -> Request
     outstanding: bool = False                     # a chunk of iterations is enqueued and not yet polled
     nbytes: int = 0                               # HBM the pool holds, charged to the budget
+    seq: int = 0                                  # order in which the outstanding chunk was enqueued
 
 
 class DDAServer:
@@ -310,6 +320,7 @@ class DDAServer:
         self.inner_tol, self.max_outer, self.ratio = float(inner_tol), int(max_outer), float(ratio)
         self._b: dict[int, _Bucket] = {}
         self._next = 0
+        self._seq = 0
         self.done: list[Request] = []
         self._pre: dict = {}       # pre_key -> [Preconditioner or None, requests not yet finished]
         # optional batch.LaunchTuner: each new bucket's matvec launch variant
@@ -435,12 +446,20 @@ class DDAServer:
         return sum(len(b.queue) + len(b.active) for b in self._b.values())
 
     def step(self) -> list:
-        """For every bucket: collect the requests its last chunk finished
-        (waiting for that pool only), admit waiting requests into the freed
-        slots and enqueue the next ``chunk_iters`` iterations at once, so a
-        pool never waits for the others.  Returns the finished requests."""
+        """For every bucket whose pool is idle: collect the requests its last
+        chunk finished, admit waiting requests into the freed slots and
+        enqueue the next ``chunk_iters`` iterations at once.  Pools still
+        running their chunk are left alone, so a pool of short iterations is
+        refilled as often as it finishes instead of once per chunk of the
+        slowest pool; when no idle pool has work, the step waits for the
+        chunk that was enqueued first.  Returns the finished requests."""
         out = []
+        todo, busy = [], []
         for b in self._b.values():
+            (busy if b.outstanding and not b.pool.ready() else todo).append(b)
+        if busy and not any(b.outstanding or b.queue for b in todo):
+            todo = [min(busy, key=lambda b: b.seq)]
+        for b in todo:
             if b.outstanding:
                 for s, info, P in b.pool.poll():
                     req = b.active.pop(s)
@@ -455,6 +474,8 @@ class DDAServer:
             if b.active:
                 b.pool.run(self.chunk)
                 b.outstanding = True
+                self._seq += 1
+                b.seq = self._seq
         self.done.extend(out)
         return out
 
