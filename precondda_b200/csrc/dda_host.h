@@ -190,6 +190,7 @@ struct MvFuse {
   double* red = nullptr;      // >= nb * grid1 * KRED doubles
   unsigned* cnt = nullptr;    // per-instance tickets
   int tensor = 0;             // octant of the x pass: 0 InstState::ghat, 1 InstState::pghat
+  int skip = 0;               // 1: no pass 1 (T1 already holds it), 2: no pass 5 (T1 left for the next product)
 };
 
 // Enqueue the 5-pass matvec for a batch of instances that share Geo.
@@ -198,6 +199,16 @@ template <typename R>
 cudaError_t launch_matvec(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
                           int in_id, int out_id, int mode, int cond, double gscale, cudaStream_t s,
                           const MvFuse& fz = MvFuse());
+
+// out = A M in over a preconditioner grid equal to the operator's, M in
+// stored in mid_id, with M's last pass and A's first fused (launch_amul_impl
+// in matvec_impl.cuh).
+template <typename R>
+cudaError_t launch_amul(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
+                        int in_id, int mid_id, int out_id, int mode, int cond, double gscale, double pscale,
+                        cudaStream_t s, const MvFuse& fz = MvFuse());
+// Whether products A M use launch_amul (DDA_NO_MA_FUSE=1 turns it off).
+bool ma_fuse_enabled();
 
 // One matvec with explicit twiddle tables (allocation-free entry point).
 template <typename R>

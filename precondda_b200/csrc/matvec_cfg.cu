@@ -17,6 +17,11 @@ bool pdl_enabled() {
   return on;
 }
 
+bool ma_fuse_enabled() {
+  const char* e = getenv("DDA_NO_MA_FUSE");   // read per call: tests switch it between captures
+  return !(e && *e == '1');
+}
+
 int mv_split_ways(int nb) {
   static const int k = [] {
     const char* e = getenv("DDA_MV_SPLIT");

@@ -1069,6 +1069,30 @@ __global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_
 #include "mv_pass5.inc"
 
 // ---------------------------------------------------------------------------
+// pass 5 of M (MV_CONV_MASKED) + pass 1 of A on the same z lines, for the
+// product A M of a preconditioned solve whose preconditioner grid is the
+// operator's (mv_pass51.inc).  Plain kernels (DDA_Z51_REGS sets a cap where
+// the z passes have one): under the z passes' 56-register cap the L = 128
+// kernel spilled 88 bytes; uncapped it takes 77 registers (L = 256: 56, no
+// spill).  B200, preconditioned mixed solves: 64^3 x 2 RHS 108.3 solves/s
+// with the separate passes, 110.4 capped, 111.9 uncapped; 128^3 x 2 RHS
+// 14.72, 15.04, 15.06.
+// ---------------------------------------------------------------------------
+#ifndef DDA_Z51_REGS
+#define DDA_Z51_REGS 0
+#endif
+template <typename R, int LZ, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads)
+    k_mv_pass51(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int mid_id,
+                int cond, int nl_)
+#include "mv_pass51.inc"
+template <typename R, int LZ, int NC>
+__global__ void __launch_bounds__(kMvMaxThreads) __maxnreg__((z_regs<R, NC, DDA_Z51_REGS>()))
+    k_mv_pass51_cap(Geo g, const typename CT<R>::T* __restrict__ tw, InstState* st, const int* act, int mid_id,
+                    int cond, int nl_)
+#include "mv_pass51.inc"
+
+// ---------------------------------------------------------------------------
 // Passes 1+2 and 4+5 fused over a thread-block cluster (cubic boxes; the
 // z/y transforms keep T1 on chip).  The CL CTAs of a cluster share one x
 // slab ix:
@@ -1251,7 +1275,9 @@ template <typename R> struct MvSet {
   typedef void (*P5)(Geo, const C*, InstState*, const int*, int, int, int, int, int, int, double*, unsigned*);
   typedef void (*PF)(Geo, const C*, InstState*, const int*, int, int);
   typedef void (*PI)(Geo, const C*, InstState*, const int*, int, int, int, int);
+  typedef void (*P51)(Geo, const C*, InstState*, const int*, int, int, int);
   P1 k1 = nullptr; PY k2 = nullptr; P3 k3 = nullptr; PY k4 = nullptr; P5 k5 = nullptr;
+  P51 k51 = nullptr;   // pass 5 of M + pass 1 of A (launch_amul_impl)
   // tile sizes the kernels were compiled for (cubic set only; 0 = any)
   int nl = 0, tz2 = 0, tz3 = 0;
   // cluster-fused passes 1+2 (kf) and 4+5 (ki), cubic sets only: cluster
@@ -1303,6 +1329,11 @@ auto pick_pass5() {
   if constexpr (z_regs<R, NC, DDA_Z_REGS>() > 0) return k_mv_pass5_cap<R, L, NC>;
   else return k_mv_pass5<R, L, NC>;
 }
+template <typename R, int L, int NC>
+auto pick_pass51() {
+  if constexpr (z_regs<R, NC, DDA_Z51_REGS>() > 0) return k_mv_pass51_cap<R, L, NC>;
+  else return k_mv_pass51<R, L, NC>;
+}
 template <typename R, bool INV, int L, int NC>
 auto pick_pass_y() {
   if constexpr (y_regs<R, NC, INV>() > 0) return k_mv_pass_y_cap<R, INV, L, NC>;
@@ -1313,7 +1344,7 @@ template <typename R>
 bool mv_general_set_impl(int Lx, int Ly, int Lz, int p3var, MvSet<R>& o) {
   typedef MvSet<R> M;
   switch (Lz) {
-#define DDA_K(n) case n: o.k1 = pick_pass1<R, n, 0>(); o.k5 = pick_pass5<R, n, 0>(); break;
+#define DDA_K(n) case n: o.k1 = pick_pass1<R, n, 0>(); o.k5 = pick_pass5<R, n, 0>(); o.k51 = pick_pass51<R, n, 0>(); break;
     DDA_FFT_SIZES(DDA_K)
 #undef DDA_K
     default: return false;
@@ -1352,6 +1383,7 @@ void mv_cube_fill(MvSet<R>& o) {
   else o.k3 = (typename M::P3)k_mv_pass3s<R, L, V, NC>;
   o.k4 = (typename M::PY)pick_pass_y<R, true, L, NC>();
   o.k5 = pick_pass5<R, L, NC>();
+  o.k51 = pick_pass51<R, L, NC>();
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
   o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
   o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
@@ -1503,8 +1535,11 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
   // passes.
   const int tf = tune_flags(sizeof(R) == 8 ? DDA_C128 : DDA_C64, g, nb);
   const bool one = k.fused_any ? (tf & DDA_TUNE_FUSED) != 0 : nb == 1;
-  const bool ff = one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) && !(tf & DDA_TUNE_NO_FUSED_ZY);
-  const bool fi = one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) && !(tf & DDA_TUNE_NO_FUSED_INV);
+  const bool skip1 = (fz.skip & 1) != 0, skip5 = (fz.skip & 2) != 0;
+  const bool ff = !skip1 && one && k.kf && fz.pre == MV_PRE_NONE && fused_zy_enabled(false) &&
+                  !(tf & DDA_TUNE_NO_FUSED_ZY);
+  const bool fi = !skip5 && one && k.ki && fz.post == MV_POST_NONE && fused_zy_enabled(true) &&
+                  !(tf & DDA_TUNE_NO_FUSED_INV);
   const bool ypair = k.k2x && (y_pair_forced() || (tf & DDA_TUNE_YPAIR));
   const bool zpair = k.k1x && (z_pair_forced() || (tf & DDA_TUNE_ZPAIR));
   Geo gq = g;
@@ -1517,7 +1552,9 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                             in_id, cond)))
       return e;
   } else {
-    if (zpair && fz.pre == MV_PRE_NONE) {
+    if (skip1) {
+      // T1 already holds the forward z transform (k_mv_pass51)
+    } else if (zpair && fz.pre == MV_PRE_NONE) {
       if ((e = launch_pdl(k.k1x, dim3((unsigned)k.grid1x, nb), dim3(k.th1x), k.smem1x, s, g, twz, st, act, in_id,
                           cond, pc.nl, fz.pre)))
         return e;
@@ -1564,7 +1601,9 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
                                pc.tz2, pc.ntz2))) {
       return e;
     }
-    if (zpair && fz.post == MV_POST_NONE) {
+    if (skip5) {
+      // T1 is left for the next product's first pass (k_mv_pass51)
+    } else if (zpair && fz.post == MV_POST_NONE) {
       if ((e = launch_pdl(k.k5x, dim3((unsigned)k.grid1x, nb), dim3(k.th1x), k.smem1x, s, g, twz, st, act, in_id,
                           out_id, mode, cond, pc.nl, fz.post, fz.red, fz.cnt)))
         return e;
@@ -1573,7 +1612,7 @@ cudaError_t launch_mv_set(const MvSet<R>& k, const Geo& g, const PassCfg& pc, In
       return e;
     }
   }
-  note_launch(s, 5 - (ff ? 1 : 0) - (fi ? 1 : 0));
+  note_launch(s, 5 - (ff ? 1 : 0) - (fi ? 1 : 0) - (skip1 ? 1 : 0) - (skip5 ? 1 : 0));
   return cudaGetLastError();
 }
 
@@ -1615,6 +1654,45 @@ cudaError_t launch_matvec_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstSt
     if (e != cudaSuccess && first == cudaSuccess) first = e;
   }
   return first;
+}
+
+// out = A M in for a preconditioned product whose preconditioner grid is the
+// operator's (gp = g): M's passes 1-4 (octant pghat), k_mv_pass51 (M's pass 5
+// with its mask into mid_id, then A's pass 1 from shared memory), A's passes
+// 2-5 (its combine reads mid_id).  A's first pass reads no vector.  fz: M's pass 1 takes fz.pre, A's pass 5
+// fz.post (fused Krylov steps).
+template <typename R>
+cudaError_t launch_amul_impl(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st, const int* act, int nb,
+                             int in_id, int mid_id, int out_id, int mode, int cond, double gscale, double pscale,
+                             cudaStream_t s, const MvFuse& fz) {
+  typedef typename CT<R>::T C;
+  constexpr bool dbl = sizeof(R) == 8;
+  MvSet<R> k;
+  if (!mv_select<R>(g, pc, k) || !k.k51) return cudaErrorInvalidValue;
+  const C* twx = (const C*)ctx.twiddles(g.Lx, dbl);
+  const C* twy = (const C*)ctx.twiddles(g.Ly, dbl);
+  const C* twz = (const C*)ctx.twiddles(g.Lz, dbl);
+  if (!twx || !twy || !twz) return cudaErrorMemoryAllocation;
+  const void* ks[1] = {(const void*)k.k51};
+  cudaError_t e = mv_prepare(ks, 1);
+  if (e != cudaSuccess) return e;
+  MvFuse fm;
+  fm.tensor = 1;
+  fm.pre = fz.pre;
+  fm.skip = 2;
+  if ((e = launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, in_id, mid_id, MV_CONV_MASKED, cond, pscale, s,
+                            fm)))
+    return e;
+  if ((e = launch_pdl(k.k51, dim3((unsigned)pc.grid1, nb), dim3(pc.th1), pc.smem1, s, g, twz, st, act, mid_id,
+                      cond, pc.nl)))
+    return e;
+  note_launch(s, 1);
+  MvFuse fa = fz;
+  fa.pre = MV_PRE_NONE;
+  fa.tensor = 0;
+  fa.skip = 1;
+  // A's combine reads its x (the M vector) from mid_id
+  return launch_mv_set<R>(k, g, pc, st, act, nb, twx, twy, twz, mid_id, out_id, mode, cond, gscale, s, fa);
 }
 
 // Same five launches with caller-provided twiddle tables (used by the

@@ -238,6 +238,11 @@ template <typename R>
 static cudaError_t amul(Ctx& c, BatchWs& w, int in, int out, int mode, int cond, double gscale, cudaStream_t s,
                         const MvFuse& fz = MvFuse()) {
   MvFuse fa = fz;
+  if (w.pre && ma_fuse_enabled() && w.gp.nx == w.g.nx && w.gp.ny == w.g.ny && w.gp.nz == w.g.nz &&
+      w.gp.Lx == w.g.Lx && w.gp.Ly == w.g.Ly && w.gp.Lz == w.g.Lz) {
+    // M's last pass and A's first in one kernel: A's first pass reads no vector
+    return launch_amul<R>(c, w.g, w.pc, w.d_st, nullptr, w.nb, in, V_MH, out, mode, cond, gscale, w.pscale, s, fz);
+  }
   if (w.pre) {
     MvFuse fm;
     fm.tensor = 1;

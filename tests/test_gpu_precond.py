@@ -204,3 +204,38 @@ def test_precond_edge_cases_and_errors():
                                       iac.data_ptr(), C.byref(h)) == L.DDA_ERR_BAD_SHAPE  # 14: not compiled
     with pytest.raises(ValueError):
         P.Preconditioner(inv_alpha=ia, k=k, d=d, L_=(4, 16, 16))                          # grid < box
+
+
+@pytest.mark.parametrize("case", ["cube64", "blob"])
+def test_fused_preconditioner_handoff_equals_separate_passes(monkeypatch, case):
+    """A M with M's last pass and A's first in one kernel (the M vector
+    handed over in shared memory, never in HBM) gives the separate passes'
+    iterates bit for bit: c64, c128 and mixed preconditioned solves, on a
+    cubic box (compile-time kernels) and an irregular scatterer in a ragged
+    box (runtime-size kernels), two right-hand sides in one batch."""
+    import precondda_b200 as P
+    if case == "cube64":
+        k, d, ia, E = _sphere(64, 1.7 + 0.1j)
+        E2 = O.incident_field((64,) * 3, d, k, (0, 0, 1), (0, 1, 0))
+    else:
+        k, d, ia, E = _blob((20, 24, 28), 5, 2.2 + 0.1j)
+        E2 = O.incident_field((20, 24, 28), d, k, (0, 1, 0), (1, 0, 0))
+    op = P.DDAOperator(ia, k, d, dtype=C128, with_twin=True)
+    pre = op.preconditioner()
+
+    def run():
+        op._ctx.trim()                      # cached iteration graphs hold the kernels of their capture
+        out = []
+        for prec, tol in (("c64", 1e-5), ("c128", 1e-7), ("mixed", 1e-7)):
+            Ps, infos = P.solve_many([op, op], [E, E2], tol=tol, max_iter=400, precision=prec, preconditioner=pre)
+            out.append(([p.clone() for p in Ps], [(i.iters, i.outer, i.status) for i in infos]))
+        return out
+
+    fused = run()
+    monkeypatch.setenv("DDA_NO_MA_FUSE", "1")
+    separate = run()
+    for (Pf, inf), (Ps, ins) in zip(fused, separate):
+        assert inf == ins
+        assert all(st == "converged" for _, _, st in inf)
+        for a, b in zip(Pf, Ps):
+            assert torch.equal(a, b)
