@@ -220,11 +220,12 @@ void Ctx::trim() {
 // DDA_FUSE_KRYLOV=1 lets the Krylov steps alpha (<rhat, v>), s / y and
 // zeta / eta ride on the two matvecs (dot products in the last pass, s and y
 // formed in the first -- M's first pass in a preconditioned solve) instead of
-// three separate kernels.  Measured on B200 with the current passes it is
-// no faster overall (preconditioned 64^3 x 2 RHS: mixed 108.7 against 108.4
-// solves/s, c128 60.8 against 61.6; 128^3 ellipsoid x 16 RHS mixed 15.76
-// against 15.66; 128^3 x 2 RHS mixed 14.7 against 14.0; plain c128 32^3
-// 197.6 against 189.0), so the separate kernels are the default.
+// three separate kernels.  Measured on B200 it is no faster overall: with
+// the preconditioner's last pass fused into A's first (launch_amul),
+// preconditioned 64^3 x 2 RHS mixed 112.3 against 111.7 solves/s and 128^3
+// x 2 RHS 14.05 against 15.22; before that fusion, 64^3 108.7 against
+// 108.4, c128 60.8 against 61.6, 128^3 x 16 RHS 15.76 against 15.66, plain
+// c128 32^3 197.6 against 189.0.  The separate kernels are the default.
 static bool fuse_krylov() {
   const char* e = getenv("DDA_FUSE_KRYLOV");
   return e && *e == '1';
