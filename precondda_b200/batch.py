@@ -21,6 +21,7 @@ same way and records it in the engine's tuning table.
 """
 from __future__ import annotations
 
+import itertools
 import json
 import math
 import os
@@ -353,6 +354,7 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     active, fresh, used = [], [], 0
+    seq, chunk_seq = itertools.count(), {}     # order in which each pool's current chunk was enqueued
     while items or active or fresh:
         while items:
             key, gl = items[0]
@@ -369,12 +371,20 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
                 break
             items.popleft()
             entry[0].run(chunk)             # a new pool starts iterating at once
+            chunk_seq[id(entry[0])] = next(seq)
             fresh.append(entry)
             used += entry[2]
-        # each pool is polled (waiting for its own last chunk only) and given
-        # its next chunk right away, so no pool waits for the slowest one
+        # pools whose last chunk has finished are polled and given their next
+        # chunk right away, so no pool waits for the slowest one; when none
+        # has finished, the loop waits for the chunk enqueued first
+        ready = [e[0].ready() for e in active]
+        if active and not any(ready):
+            ready[min(range(len(active)), key=lambda i: chunk_seq[id(active[i][0])])] = True
         still = []
-        for pool, where, est in active:
+        for (pool, where, est), rdy in zip(active, ready):
+            if not rdy:
+                still.append((pool, where, est))
+                continue
             for s, info, P in pool.poll():
                 g, j = where[s]
                 nx, ny, nz = geoms[g].shape
@@ -386,6 +396,7 @@ def solve_geometries(geoms, tol=1e-5, precision="mixed", inner_tol=1e-4, max_ite
                     Ps[g][j] = Pc
             if pool.running:
                 pool.run(chunk)
+                chunk_seq[id(pool)] = next(seq)
                 still.append((pool, where, est))
             else:
                 pool.close()
