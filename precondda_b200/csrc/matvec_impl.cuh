@@ -109,6 +109,14 @@ template <typename R> constexpr int mv_lanes_t(int T) {
 }
 constexpr int cmin_i(int a, int b) { return a < b ? a : b; }
 template <typename R, int T> constexpr int mv_tiles() { return mv_lanes_t<R>(T) / T > 1 ? mv_lanes_t<R>(T) / T : 1; }
+// kz columns per CTA of the one-component x pass (k_mv_pass3s);
+// DDA_P3_TZ128 > 0 sets it for complex64 L = 128 (an A/B build option)
+#ifndef DDA_P3_TZ128
+#define DDA_P3_TZ128 0
+#endif
+template <typename R, int LX, int T> constexpr int p3s_tiles() {
+  return (sizeof(R) == 4 && LX == 128 && DDA_P3_TZ128 > 0) ? DDA_P3_TZ128 : mv_tiles<R, T>();
+}
 
 // NC > 0 selects the cubic specialisation of a pass: box NC^3 on the FFT
 // grid (2 NC)^3, every size a compile-time constant, so shared-memory and
@@ -373,7 +381,7 @@ __global__ void __launch_bounds__(kMvMaxThreads, p3_min_blocks<R, LX, NC>()) k_m
   typedef RevPlan<P> Q;
   constexpr bool CUBE = NC > 0;
   static_assert(!CUBE || LX == 2 * NC, "cubic kernels need L = 2n");
-  constexpr int TZC = CUBE ? cmin_i(mv_tiles<R, SH::T>(), LX) : 1;
+  constexpr int TZC = CUBE ? cmin_i(p3s_tiles<R, LX, SH::T>(), LX) : 1;
   constexpr int NTZC = (LX + TZC - 1) / TZC;
   constexpr bool ZH = CUBE && P::r[0] % 2 == 0;
   constexpr bool DH = CUBE && half_store_ok<Q>();
@@ -1386,7 +1394,7 @@ void mv_cube_fill(MvSet<R>& o) {
   o.k51 = pick_pass51<R, L, NC>();
   o.nl = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), NC * NC);
   o.tz2 = cmin_i(mv_tiles<R, MvShape<R, L>::T>(), L);
-  o.tz3 = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
+  o.tz3 = cmin_i(V == 1 ? mv_tiles<R, P3Shape<R, L, V>::T>() : p3s_tiles<R, L, P3Shape<R, L, V>::T>(), L);
   if constexpr (sizeof(R) == 4 && V == 0 && (L == 128 || L == 256)) {
     // complex64 64^3 / 128^3: the staged persistent x pass, same tile shape
     constexpr int TZ = cmin_i(mv_tiles<R, P3Shape<R, L, V>::T>(), L);
@@ -1766,6 +1774,7 @@ PassCfg make_pass_cfg_impl(const Geo& g) {
   tile_dims3<R>(g.Lx, c.p3var, T, LP);
   c.p3reg = c.p3var == 1;
   c.tz3 = std::min(std::max(1, mv_lanes_t<R>(T) / T), g.Lz);
+  if (sizeof(R) == 4 && g.Lx == 128 && DDA_P3_TZ128 > 0 && !c.p3reg) c.tz3 = std::min(DDA_P3_TZ128, g.Lz);
   c.th3 = (c.p3reg ? 1 : 3) * c.tz3 * T;
   c.smem3 = (size_t)3 * c.tz3 * LP * esz + (smem_tw((int)esz) ? (size_t)g.Lx * esz : 0);
   c.ntz3 = (g.Lz + c.tz3 - 1) / c.tz3;
