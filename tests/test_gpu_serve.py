@@ -58,6 +58,34 @@ def test_slot_pool_c128_matches_oracle():
     pool.close()
 
 
+def test_slot_pool_ready_reports_idle_stream():
+    """dda_slots_ready: idle after the stream drains, and a pool that was
+    reported ready polls without waiting (the result is the same as a
+    blocking poll's)."""
+    import precondda_b200 as P
+    from precondda_b200.serve import SlotPool
+    n = 8
+    k, d, alpha, E = _sphere(n, 1.5 + 0.01j)
+    ia, mask, G, _ = O.prepare_interaction_matrices(alpha, k, d)
+    L = (2 * n,) * 3
+    ghat = P.green_octant((n, n, n), k, d, L, 1.0 / (L[0] * L[1] * L[2]), C128, layout="engine")
+    pool = SlotPool((n, n, n), L, 2, "c128")
+    assert pool.ready()
+    pool.admit(0, ghat, torch.tensor(ia, device="cuda"), torch.tensor(E, device="cuda"), tol=1e-6, max_iter=500)
+    done = {}
+    for _ in range(500):
+        pool.run(4)
+        torch.cuda.synchronize()
+        assert pool.ready()
+        for s, info, Pout in pool.poll():
+            done[s] = info
+        if pool.running == 0:
+            break
+    assert done[0].status == "converged"
+    assert pool.ready()
+    pool.close()
+
+
 def _requests(P, specs):
     reqs = []
     for (n, m, kdir, pol, tol) in specs:
