@@ -279,8 +279,8 @@ def time_matvec_batch(ops, reps, flush):
     return statistics.median(ts)
 
 
-def north_star_128(dev, seed=3):
-    """The 128^3 target as the driver runs it: the seeded rotated ellipsoid
+def ellipsoid128_16rhs(dev, seed=3):
+    """The 128^3 mixed-over-plain measurement: the seeded rotated ellipsoid
     (semi-axes (64, 48, 40) d, |m|kd = 0.6) with 2 polarisations x 8
     incidence directions (16 right-hand sides), all solved in one batched
     mixed-precision launch (complex64 sweeps to 1e-4, FP64 refinement to
@@ -388,7 +388,7 @@ def serve_block(args, ws, rank, local, rate=3.0, duration=20.0):
             "rhs": c["rhs"], "green_hits": c["green_hits"], "green_misses": c["green_misses"]}
 
 
-def config1_plain(dev):
+def sphere32_plain(dev):
     """The plain-method configuration on the GPU: 32^3 sphere (17,256
     dipoles, m = 1.5+0.01i, |m|kd = 0.5), complex128 GPBiCGSTAB from P0 = 0,
     tol 1e-6, maxiter 2000, ratio 100, precon=False, x polarisation."""
@@ -568,7 +568,7 @@ def run_ours(args, ws, rank, local):
                          "algorithmic_bytes": Bb}
             del opb
         del flush
-        out = {"north_star_128": _extra(north_star_128, dev), "config1_plain_32": _extra(config1_plain, dev),
+        out = {"ellipsoid128_16rhs": _extra(ellipsoid128_16rhs, dev), "sphere32_plain_c128": _extra(sphere32_plain, dev),
                "batch64": _extra(batch64_block, args, ws, rank, local),
                "serve": _extra(serve_block, args, ws, rank, local),
                "launch_tuning": {json.dumps(list(k)): {"flags": v, "seconds": tuner.times.get(k)}

@@ -57,7 +57,7 @@ def _xsec_err(got, ref):
     return max(abs(g - r) / abs(r) for g, r in zip(got, ref))
 
 
-def test_config1_plain_c128_solve_matches_oracle_and_reference(fx):
+def test_sphere32_plain_c128_solve_matches_oracle_and_reference(fx):
     import precondda_b200 as P
     n, m = 32, 1.5 + 0.01j
     k, d, alpha, E = _sphere(n, m, (1, 0, 0))
@@ -81,7 +81,7 @@ def test_config1_plain_c128_solve_matches_oracle_and_reference(fx):
     assert abs(np.linalg.norm(Pn) - float(fx["c1_ref_Pnorm"])) / float(fx["c1_ref_Pnorm"]) < 1e-5
 
 
-def test_config1_reference_api_solve_matches_reference(fx):
+def test_sphere32_reference_api_solve_matches_reference(fx):
     """The drop-in solve_gpbicgstab (complex64 like the reference's) on the
     32^3 sphere: the reference's iteration count and outputs."""
     import precondda_b200 as P
