@@ -209,6 +209,13 @@ cudaError_t launch_amul(Ctx& ctx, const Geo& g, const PassCfg& pc, InstState* st
                         cudaStream_t s, const MvFuse& fz = MvFuse());
 // Whether products A M use launch_amul (DDA_NO_MA_FUSE=1 turns it off).
 bool ma_fuse_enabled();
+// Inner (complex64) target of a mixed solve's later sweeps: what the FP64
+// tolerance still needs from the current true relative residual, times a
+// safety factor (0.8; DDA_SWEEP_SAFETY overrides), within [inner_tol, 0.5].
+// B200, preconditioned mixed solves to 1e-6, factor 0.3 / 0.6 / 0.8 / 0.9:
+// 64^3 sphere 29 / 28 / 26 / 26 inner iterations, 128^3 ellipsoid 26 / 25 /
+// - / 24, every solve in two sweeps with true residual <= 1e-6.
+double mixed_sweep_target(double inner_tol, double tol, double relres);
 
 // One matvec with explicit twiddle tables (allocation-free entry point).
 template <typename R>

@@ -1,6 +1,7 @@
 // Tile shapes of the five matvec passes (see matvec_impl.cuh).
 #include "matvec_impl.cuh"
 
+#include <algorithm>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -15,6 +16,16 @@ bool pdl_enabled() {
     return !(e && *e == '1');
   }();
   return on;
+}
+
+double mixed_sweep_target(double inner_tol, double tol, double relres) {
+  static const double f = [] {
+    const char* e = getenv("DDA_SWEEP_SAFETY");
+    const double v = e ? atof(e) : 0.0;
+    return (v > 0.0 && v < 1.0) ? v : 0.8;
+  }();
+  if (!(relres > 0.0)) return inner_tol;
+  return std::max(inner_tol, std::min(0.5, f * tol / relres));
 }
 
 bool ma_fuse_enabled() {

@@ -445,7 +445,7 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
       for (int j : rearm) {
         SlotInfo& I = p->info[j];
         const InstState& S = p->w.h_st[1][j];
-        const double tj = std::max(I.inner_tol, std::min(0.5, 0.3 * I.tol / I.relres));
+        const double tj = mixed_sweep_target(I.inner_tol, I.tol, I.relres);
         if ((rc = arm_solver(p, j, S.ghat, S.pghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false, nullptr)))
           return rc;
       }

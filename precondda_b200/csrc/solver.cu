@@ -603,9 +603,8 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
       H64[j].pghat = pre ? pre->phat[j] : nullptr;
       H64[j].inva = i64[j].inv_alpha;
       // inner target: inner_tol, relaxed on later sweeps to what the FP64
-      // target still needs (with a safety factor), never above 0.5
-      double tj = inner_tol;
-      if (sweep > 0 && relres[j] > 0) tj = std::max(inner_tol, std::min(0.5, 0.3 * tol / relres[j]));
+      // target still needs (mixed_sweep_target)
+      const double tj = sweep > 0 ? mixed_sweep_target(inner_tol, tol, relres[j]) : inner_tol;
       H64[j].target = tj;
       H64[j].ratio = ratio;
       H64[j].max_iter = max_iter;
