@@ -216,6 +216,18 @@ bool ma_fuse_enabled();
 // 64^3 sphere 29 / 28 / 26 / 26 inner iterations, 128^3 ellipsoid 26 / 25 /
 // - / 24, every solve in two sweeps with true residual <= 1e-6.
 double mixed_sweep_target(double inner_tol, double tol, double relres);
+// Reset ratio of a mixed solve's complex64 sweeps.  The plain solves keep
+// the reference's rule (reset at the third iteration and whenever the
+// residual fell by `ratio` since the last reset, Gpbicgstab.py:1125-1158);
+// the sweeps keep it with the ratio raised to at least 1000 (0 still
+// means no resets; DDA_INNER_RATIO overrides): a reset restarts the
+// recurrence, and the FP64 refinement around the sweeps is what guards the
+// accuracy.  B200, preconditioned mixed solves to 1e-6, ratio 100 / 1000 /
+// 0: 64^3 m = 1.7+0.1i 26 / 21 / 21 inner iterations (19.3 / 15.5 / 14.6
+// ms for two RHS), m = 2.5+0.1i 57 / 54 / 49, m = 3.5+0.05i 829 / 777 / 909,
+// 48^3 m = 3.5+0.5i 58 / 58 / 47, 96^3 m = 2+0.3i 21 / 19 / 16; all in two
+// sweeps to true residual <= 1e-6.
+double mixed_inner_ratio(double ratio);
 
 // One matvec with explicit twiddle tables (allocation-free entry point).
 template <typename R>

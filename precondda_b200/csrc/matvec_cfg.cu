@@ -28,6 +28,15 @@ double mixed_sweep_target(double inner_tol, double tol, double relres) {
   return std::max(inner_tol, std::min(0.5, f * tol / relres));
 }
 
+double mixed_inner_ratio(double ratio) {
+  static const double r = [] {
+    const char* e = getenv("DDA_INNER_RATIO");
+    return e ? atof(e) : -1.0;
+  }();
+  if (r >= 0.0) return r;
+  return ratio == 0.0 ? 0.0 : std::max(ratio, 1000.0);
+}
+
 bool ma_fuse_enabled() {
   const char* e = getenv("DDA_NO_MA_FUSE");   // read per call: tests switch it between captures
   return !(e && *e == '1');

@@ -308,8 +308,8 @@ static int slots_admit(dda_slots* p, int slot, const dda_instance* lo, const dda
     launch_norm2<double>(p->w128.d_st, V_B, 1, (long long)p->w128.n3, p->w128.red, p->w128.cnt, p->w128.RB,
                          p->d_bnorm, p->s, act);
     cudaMemcpyAsync(H.vec[V_R], H.vec[V_B], bytes, cudaMemcpyDeviceToDevice, p->s);
-    if ((rc = arm_solver(p, slot, lo->ghat, phat, lo->inv_alpha, nullptr, inner_tol, max_iter, ratio, false,
-                         nullptr)))
+    if ((rc = arm_solver(p, slot, lo->ghat, phat, lo->inv_alpha, nullptr, inner_tol, max_iter,
+                         mixed_inner_ratio(ratio), false, nullptr)))
       return rc;
     if (compress_sites()) launch_site_map<float>(p->w.d_st, 1, p->g.nsite, p->w.bcount, p->s, act);
     launch_down(p->w.d_st, V_B, p->w128.d_st, V_R, 1, (long long)p->w.n3, c.num_sms, p->s, act);
@@ -446,7 +446,8 @@ int dda_slots_poll(dda_slots* p, int* finished, dda_result* results, int* nfinis
         SlotInfo& I = p->info[j];
         const InstState& S = p->w.h_st[1][j];
         const double tj = mixed_sweep_target(I.inner_tol, I.tol, I.relres);
-        if ((rc = arm_solver(p, j, S.ghat, S.pghat, S.inva, nullptr, tj, I.max_iter, I.ratio, false, nullptr)))
+        if ((rc = arm_solver(p, j, S.ghat, S.pghat, S.inva, nullptr, tj, I.max_iter, mixed_inner_ratio(I.ratio),
+                             false, nullptr)))
           return rc;
       }
       if ((rc = set_act(p, 1, rearm))) return rc;

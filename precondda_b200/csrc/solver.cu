@@ -606,7 +606,7 @@ int solve_mixed(Ctx& c, const Geo& g, double gscale, const dda_instance* i64, co
       // target still needs (mixed_sweep_target)
       const double tj = sweep > 0 ? mixed_sweep_target(inner_tol, tol, relres[j]) : inner_tol;
       H64[j].target = tj;
-      H64[j].ratio = ratio;
+      H64[j].ratio = mixed_inner_ratio(ratio);
       H64[j].max_iter = max_iter;
       H64[j].active = active[j];
       H[j].active = active[j];
