@@ -201,9 +201,11 @@ int dda_solve_batch(dda_ctx* ctx, int dtype, int nx, int ny, int nz, int Lx, int
                     const dda_instance* inst, int nb, double target, int max_iter, double ratio, dda_result* res,
                     void* stream);
 
-/* Mixed precision: complex64 GPBiCGSTAB sweeps (relative target inner_tol)
- * inside an FP64 iterative-refinement loop whose true residual
- * E_inc*mask - A.P is an FP64 matvec; stops when it is <= tol * ||E_inc*mask||.
+/* Mixed precision: complex64 GPBiCGSTAB sweeps (relative target inner_tol
+ * for the first; later sweeps aim at 0.8 x what tol still needs) inside an
+ * FP64 iterative-refinement loop whose true residual E_inc*mask - A.P is an
+ * FP64 matvec; stops when it is <= tol * ||E_inc*mask||.  The sweeps apply
+ * the reference's restart rule with max(ratio, 1000) (0: no restarts).
  * inst64 / inst128 describe the same instances in both precisions
  * (inst64[j].p_out and inst64[j].e_inc are scratch the engine may overwrite;
  * inst128[j].p_out receives the FP64 solution). */
@@ -289,7 +291,8 @@ int dda_slots_free_slot(const dda_slots* pool);
  * DDA_PREC_C128 reads `hi`, DDA_PREC_MIXED reads both (lo: complex64 ghat and
  * inv_alpha; hi: complex128 ghat, inv_alpha, e_inc and p_out).  tol is the
  * solver target (the FP64 target for mixed pools); inner_tol, max_outer only
- * matter for mixed pools.  The result lands in p_out when the slot finishes. */
+ * matter for mixed pools, whose sweeps follow dda_solve_mixed_batch.  The
+ * result lands in p_out when the slot finishes. */
 int dda_slots_admit(dda_slots* pool, int slot, const dda_instance* lo, const dda_instance* hi, double tol,
                     double inner_tol, int max_iter, int max_outer, double ratio, void* stream);
 /* Preconditioned pools (the precon=True solve of dda_solve_batch_pre for
